@@ -1,0 +1,373 @@
+"""MLS-MPM baking simulator (the reference's ``physics/mpm.py:17-340``) on one B200.
+
+Same constructor, attributes and methods as the reference ``MpmSimulator``
+(``Step``, ``Advance``, ``Reset``, ``CheckState``, ``UpdateMesh``,
+``CaptureSnapshot``/``SaveSnapshot``, the settling state machine), with state in
+CUDA tensors and every kernel on the device. Two ping-pong particle states are
+allocated once; no array is allocated per substep.
+
+Error flags. ``Step()`` reads the device flags after the transport solve and
+after the return map, exactly where the reference synchronises, and raises
+before the new state is committed. ``Advance(n)`` runs its substeps without a
+host round trip and checks the flags once at the end; a failure then names the
+first substep whose flags were set.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import fields, replace
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from .. import _lib, arrays
+from ..geometry import ComputeSignedVolumes
+from ..geometry.mesh_tracking import ParticleMeshBinding
+from .grid import GridState, UpdateGrid
+from .materials.ding import DingMaterial
+from .materials.elastic import ElasticMaterial
+from .state import AllocateState, CreateParticleState
+from .thermal_water import AllocateTransportState, ThermalWaterTransport
+from .transfer import GridToParticle, ParticleToGrid
+
+
+class MpmSimulator:
+    def __init__(self, tet_mesh, particle_samples, simulation_config, material_config,
+                 initial_velocity=(0.0, 0.0, 0.0), retain_history=False, ding_config=None, transport_config=None):
+        simulation_config.Validate(material_config)
+        self.device = _lib.require_cuda(simulation_config.device_name)
+        self.device_name = str(self.device)
+        _lib.load()
+        self.tet_mesh = tet_mesh
+        self.particle_samples = particle_samples
+        self.simulation_config = simulation_config
+        self.material = ElasticMaterial(material_config)
+        if material_config.model == "ding2019":
+            from ..config import DingConfig
+            self.material = DingMaterial(material_config, ding_config or DingConfig(), self.device, retain_history)
+        if isinstance(self.material, DingMaterial):
+            self.material.simulation_config = simulation_config
+        if (isinstance(self.material, DingMaterial) and self.material.ding_config.gas_enabled
+                and not (transport_config and transport_config.enabled)):
+            raise ValueError("Ding gas simulation requires transport.enabled=true; prescribed temperature "
+                             "schedules were removed")
+        self.initial_velocity = initial_velocity
+        self.retain_history = retain_history
+        self.ValidateInitialDomain()
+        self.mesh_binding = ParticleMeshBinding(tet_mesh, particle_samples, self.device)
+        self.transport = None
+        self.error_flags = torch.zeros(2, dtype=torch.int32, device=self.device)
+        if transport_config is not None and transport_config.enabled:
+            transport_config.Validate(material_config)
+            self.material.initial_temperature_k = transport_config.initial_temperature_k
+            self.transport = ThermalWaterTransport(self, transport_config)
+        self._buffers = {}
+        self.Reset()
+
+    # ------------------------------------------------------------ settling
+    @property
+    def settling_steps(self):
+        if self.transport is None:
+            return 0
+        if self._baking_start_step is not None and self._baking_start_step > 0:
+            return self._baking_start_step
+        return int(math.ceil(self.transport.config.settling_duration_s / self.simulation_config.time_step - 1e-10))
+
+    @property
+    def IsSettling(self):
+        return (self.transport is not None and self.transport.config.settling_duration_s > 0
+                and self._baking_start_step is None)
+
+    @property
+    def baking_steps(self):
+        return 0 if self.IsSettling else max(0, self.step_count - self.settling_steps)
+
+    @property
+    def baking_time(self):
+        return self.baking_steps * self.simulation_config.time_step
+
+    def UpdateSettling(self, old_state):
+        from .quasistatic import SettlingMetrics
+        config = self.transport.config
+        dt = self.simulation_config.time_step
+        if not config.settling_auto:
+            if self.step_count >= self.settling_steps:
+                self._baking_start_step = self.step_count
+                self.settling_reason = "fixed_duration"
+            return
+        self.settling_metrics.zero_()
+        SettlingMetrics(self.current_state.particle_velocities, self.current_state.affine_velocities,
+                        self.settling_reference_plastic, self.current_state.material_state.plastic_gradients,
+                        self.settling_metrics, (self.step_count - self.settling_reference_step) * dt)
+        values = self.settling_metrics.tolist()
+        if (self.step_count - self.settling_reference_step) * dt + 1e-12 >= min(.01, config.settling_hold_duration_s):
+            self.settling_plastic_rate = float(values[2])
+            self.settling_reference_plastic.copy_(self.current_state.material_state.plastic_gradients)
+            self.settling_reference_step = self.step_count
+        values[2] = self.settling_plastic_rate
+        self.settling_diagnostics = dict(max_speed_m_s=float(values[0]), max_strain_rate_per_s=float(values[1]),
+                                         max_plastic_rate_per_s=float(values[2]))
+        eligible = (self.step_count - 1) * dt + 1e-12 >= config.settling_min_duration_s
+        small = values[0] <= config.settling_speed_tolerance and max(values[1:]) <= config.settling_rate_tolerance
+        self.settling_quiet_steps = self.settling_quiet_steps + 1 if eligible and small else 0
+        if self.settling_quiet_steps * dt + 1e-12 >= config.settling_hold_duration_s:
+            self._baking_start_step = self.step_count
+            self.settling_reason = "quasi_static"
+        elif self.step_count >= self.settling_steps:
+            self.settling_reason = "timeout"
+            raise RuntimeError("Settling did not reach quasi-static tolerances before settling_duration_s; "
+                               "baking was not started. Increase the maximum duration or review tolerances/material.")
+
+    # -------------------------------------------------------------- set-up
+    def Masses(self, state=None):
+        state = self.current_state if state is None else state
+        return state.transport_state.particle_masses if state.transport_state is not None else \
+            self.particle_data.particle_masses
+
+    def ValidateInitialDomain(self):
+        s = self.simulation_config
+        origin = np.asarray(s.grid_origin)
+        lower = origin + (s.boundary_cells - 1) * s.grid_spacing
+        upper = origin + (s.grid_resolution - s.boundary_cells) * s.grid_spacing
+        points = np.concatenate([self.tet_mesh.vertex_positions, self.particle_samples.particle_positions])
+        if np.any(points < lower) or np.any(points > upper):
+            raise ValueError(f"model must initially fit inside {lower} .. {upper}; adjust [mesh] mesh_scale/"
+                             "mesh_translation or [simulation] grid settings in the config file")
+
+    def surface_vertices_buffer(self):
+        if "vertices" not in self._buffers:
+            self._buffers["vertices"] = arrays.vec3s(len(self.tet_mesh.vertex_positions), device=self.device)
+        return self._buffers["vertices"]
+
+    def transport_particle_workspace(self):
+        if "transport" not in self._buffers:
+            n = self.particle_data.particle_count
+            self._buffers["transport"] = {name: arrays.scalars(n, torch.float64, self.device)
+                                          for name in ("exposed", "contact", "particle_heat", "particle_loss")}
+        return self._buffers["transport"]
+
+    def _allocate_like_current(self):
+        n = self.particle_data.particle_count
+        state = AllocateState(n, self.device)
+        if isinstance(self.material, DingMaterial):
+            self.material.InitializeState(state)
+        if self.transport is not None:
+            state.transport_state = AllocateTransportState(n, self.device)
+        return state
+
+    def Reset(self):
+        if isinstance(self.material, DingMaterial):
+            self.material.Reset()
+        self.current_state, self.particle_data = CreateParticleState(self.particle_samples, self.device,
+                                                                     self.initial_velocity, self.retain_history)
+        if isinstance(self.material, DingMaterial):
+            self.material.InitializeState(self.current_state)
+        if self.transport is not None:
+            self.transport.InitializeState(self.current_state)
+        self.next_state = self._allocate_like_current()
+        n = self.particle_data.particle_count
+        self.grid_state = GridState(self.simulation_config, self.device)
+        self.kirchhoff_stresses = arrays.mat33s(n, device=self.device)
+        self._stress_water = arrays.mat33s(n, device=self.device)
+        self._prepared = dict(temperatures=arrays.scalars(n, torch.float32, self.device),
+                              reference_densities=arrays.scalars(n, torch.float32, self.device),
+                              saturations=arrays.scalars(n, torch.float64, self.device),
+                              gas_moles=arrays.scalars(n, torch.float64, self.device),
+                              gas_pressures=arrays.scalars(n, torch.float64, self.device))
+        self.vertex_positions = arrays.from_numpy(self.tet_mesh.vertex_positions.astype(np.float32), "f4",
+                                                  self.device)
+        self.error_flags.zero_()
+        if self.transport is not None:
+            self.transport.error_flags.zero_()
+        self.state_history = [self.current_state] if self.retain_history else []
+        self.workspace_history = []
+        self.transport_workspace_history = []
+        self.step_count = 0
+        self._baking_start_step = None if (self.transport is not None
+                                           and self.transport.config.settling_duration_s > 0) else 0
+        self.settling_quiet_steps = 0
+        self.settling_reference_step = 0
+        self.settling_plastic_rate = 0.0
+        self.settling_reference_plastic = (self.current_state.material_state.plastic_gradients.clone()
+                                           if isinstance(self.material, DingMaterial) else None)
+        self.settling_reason = "pending" if self._baking_start_step is None else "disabled"
+        self.settling_diagnostics = dict(max_speed_m_s=0.0, max_strain_rate_per_s=0.0, max_plastic_rate_per_s=0.0)
+        self.settling_metrics = torch.zeros(3, dtype=torch.float32, device=self.device)
+        self.mesh_step_count = 0
+        self._first_failed_step = None
+        if getattr(self, "result_recorder", None) is not None:
+            self.result_recorder.Reset()
+
+    # ---------------------------------------------------------------- step
+    def _substep(self, check):
+        sim = self.simulation_config
+        was_settling = self.IsSettling
+        original = self.current_state
+        state = original
+        if self.retain_history:
+            output = self._allocate_like_current()
+        else:
+            output = self.next_state
+        if self.transport is not None:
+            state = self.transport.Advance(state, sim.time_step, settling=was_settling,
+                                           output=output.transport_state, prepared_material=self._prepared,
+                                           check=check)
+        grid = self.grid_state
+        grid.Clear()
+        stress = self.kirchhoff_stresses
+        if isinstance(self.material, DingMaterial) and self.material.ding_config.gas_enabled:
+            self.material.LaunchGasStress(state, stress)
+            if check:
+                self.material.CheckState()
+        else:
+            self.material.ComputeStress(state, stress, self.error_flags)
+        if self.transport is not None:
+            stress = self.transport.AddWaterStress(state, stress, output=self._stress_water)
+        R = sim.grid_resolution
+        ParticleToGrid(state.particle_positions, state.particle_velocities, state.affine_velocities, stress,
+                       self.Masses(state), self.particle_data.reference_volumes, grid, sim.grid_origin,
+                       sim.grid_spacing, R, sim.time_step, self.error_flags)
+        UpdateGrid(grid, sim)
+        GridToParticle(state.particle_positions, state.deformation_gradients, grid, output.particle_positions,
+                       output.particle_velocities, output.affine_velocities, output.deformation_gradients,
+                       sim.grid_origin, sim.grid_spacing, R, sim.time_step, self.error_flags)
+        self.material.AdvanceState(state, output, sim.time_step)
+        if isinstance(self.material, DingMaterial) and check:
+            self.material.CheckState()
+        if self.transport is not None:
+            self.transport.FinishStep(state, output)
+        if self.retain_history:
+            self.state_history.append(output)
+        self.current_state = output
+        self.next_state = original
+        self.step_count += 1
+        if was_settling:
+            self.UpdateSettling(original)
+        if getattr(self, "result_recorder", None) is not None:
+            self.result_recorder.Record()
+
+    def Step(self):
+        self._substep(check=True)
+
+    def _device_flag_messages(self):
+        messages = []
+        if isinstance(self.material, DingMaterial):
+            m = self.material.FlagMessage(self.material.error_flags.tolist())
+            if m:
+                messages.append(m)
+        if self.transport is not None:
+            m = self.transport.FlagMessage(self.transport.error_flags.tolist())
+            if m:
+                messages.append(m)
+        return messages
+
+    def Advance(self, step_count):
+        if step_count < 1:
+            raise ValueError("step_count must be positive")
+        start = self.step_count
+        for _ in range(step_count):
+            self._substep(check=self.IsSettling)
+        messages = self._device_flag_messages()
+        if messages:
+            raise RuntimeError(messages[0] + f" (flag raised within substeps {start + 1}..{self.step_count})")
+        return self.CheckState()
+
+    def UpdateMesh(self, force_update=False):
+        if force_update or self.mesh_step_count != self.step_count:
+            self.mesh_binding.Reconstruct(self.current_state, self.vertex_positions)
+            self.mesh_step_count = self.step_count
+
+    def CheckState(self):
+        flags = self.error_flags.tolist()
+        if flags[0]:
+            raise RuntimeError("nonpositive/nonfinite J; reduce dt or inspect loading and sampling")
+        if flags[1]:
+            raise RuntimeError("particle stencil left the grid; enlarge the domain or reduce dt")
+        st = self.current_state
+        x = st.particle_positions.double()
+        v = st.particle_velocities.double()
+        F = st.deformation_gradients.double()
+        Cm = st.affine_velocities
+        if not all(bool(torch.isfinite(a).all()) for a in (x, v, F, Cm)):
+            raise RuntimeError("nonfinite particle state; simulation stopped")
+        J = torch.linalg.det(F)
+        if float(J.min()) <= 0.0:
+            raise RuntimeError("inverted particle deformation; reduce dt or loading")
+        sim = self.simulation_config
+        gpos = (x - torch.tensor(sim.grid_origin, device=x.device, dtype=x.dtype)) / sim.grid_spacing
+        if bool((gpos < 0.5).any()) or bool((gpos >= sim.grid_resolution - 1.5).any()):
+            raise RuntimeError("particle outside valid grid stencil")
+        masses = self.Masses().double()
+        vmax = float(torch.linalg.norm(st.particle_velocities.double(), dim=1).max())
+        wave = self.material.material_config.wave_speed
+        if isinstance(self.material, DingMaterial) and self.material.ding_config.gas_enabled:
+            wave = max(wave, self.material.GasWaveSpeed(st))
+        if self.transport is not None and self.transport.config.water_enabled:
+            ww = (self.transport.config.water_stress * st.transport_state.saturations * J
+                  / st.material_state.reference_densities.double())
+            wave = float(math.sqrt(wave * wave + float(ww.max())))
+        cfl = (vmax + wave) * sim.time_step / sim.grid_spacing
+        if cfl > sim.cfl_limit:
+            raise RuntimeError(f"estimated CFL={cfl:.3f} > {sim.cfl_limit}; reduce dt")
+        if isinstance(self.material, DingMaterial):
+            self.material.CheckState()
+            ms = st.material_state
+            if not bool(torch.isfinite(ms.elastic_gradients).all()) or not bool(torch.isfinite(ms.plastic_gradients).all()):
+                raise RuntimeError("nonfinite Ding internal state")
+            if float(ms.return_residuals.max()) > 1e-4:
+                raise RuntimeError("Ding local return mapping did not converge")
+        self.UpdateMesh()
+        vertices = arrays.to_numpy(self.vertex_positions)
+        if not np.isfinite(vertices).all():
+            raise RuntimeError("nonfinite reconstructed mesh vertices")
+        volumes = torch.as_tensor(self.particle_samples.reference_volumes, device=J.device, dtype=torch.float64)
+        return {
+            "step_count": self.step_count,
+            "simulation_time": self.step_count * sim.time_step,
+            "particle_count": self.particle_data.particle_count,
+            "particle_volume_m3": float(torch.dot(volumes, J)),
+            "total_mass": float(masses.sum()),
+            "grid_mass": float(self.grid_state.node_masses.double().sum()),
+            "minimum_j": float(J.min()),
+            "maximum_j": float(J.max()),
+            "maximum_speed": vmax,
+            "kinetic_energy": float(0.5 * torch.sum(masses * torch.sum(v * v, dim=1))),
+            "estimated_cfl": cfl,
+            "unmapped_mesh_vertices": self.mesh_binding.unmapped_vertex_count,
+            "inverted_mesh_tets": int(np.count_nonzero(ComputeSignedVolumes(vertices.astype(np.float64),
+                                                                            self.tet_mesh.tet_indices) <= 0.0)),
+        }
+
+    # ------------------------------------------------------------ snapshots
+    def CaptureSnapshot(self):
+        self.UpdateMesh()
+        st = self.current_state
+        snap = dict(
+            particle_positions=arrays.to_numpy(st.particle_positions).copy(),
+            particle_velocities=arrays.to_numpy(st.particle_velocities).copy(),
+            deformation_gradients=arrays.to_numpy(st.deformation_gradients).copy(),
+            affine_velocities=arrays.to_numpy(st.affine_velocities).copy(),
+            particle_masses=arrays.to_numpy(self.Masses()).copy(),
+            reference_volumes=arrays.to_numpy(self.particle_data.reference_volumes).copy(),
+            vertices=arrays.to_numpy(self.vertex_positions).copy(), tetrahedra=self.tet_mesh.tet_indices.copy(),
+            reference_vertices=self.tet_mesh.vertex_positions.copy(),
+            source_tets=np.asarray(self.particle_samples.source_tets).copy(),
+            simulation_time=self.step_count * self.simulation_config.time_step,
+            baking_time_s=self.baking_time, settling_steps=self.settling_steps)
+        if isinstance(self.material, DingMaterial):
+            for name in ("elastic_gradients", "plastic_gradients", "kirchhoff_stresses", "return_residuals",
+                         "porosities", "temperatures", "gelled", "yield_stresses", "viscosities", "gas_moles",
+                         "gas_pressures", "porosity_residuals", "reference_densities"):
+                snap["ding_" + name] = arrays.to_numpy(getattr(st.material_state, name)).copy()
+        if st.transport_state is not None:
+            for field in fields(st.transport_state):
+                snap["transport_" + field.name] = arrays.to_numpy(getattr(st.transport_state, field.name)).copy()
+        return snap
+
+    def SaveSnapshot(self, output_path):
+        self.UpdateMesh()
+        output_path = Path(output_path)
+        output_path.parent.mkdir(parents=True, exist_ok=True)
+        np.savez_compressed(output_path, **self.CaptureSnapshot())

@@ -1,0 +1,185 @@
+/*
+ * baking_b200 -- C ABI of the B200 (sm_100a) MLS-MPM baking substep.
+ *
+ * One entry point per reference Warp kernel (same argument order as the kernel,
+ * arrays passed as device pointers), plus the fused whole-substep entry points
+ * the simulator uses. Conventions shared by every call:
+ *
+ *  - Device memory is owned by the caller; nothing here allocates or frees it.
+ *  - Per-particle arrays are structure-of-arrays "planes": a vec3 is 3 planes and
+ *    a mat33 is 9 planes (row-major component order), each plane `pitch`
+ *    elements long, so component c of particle i lives at base[c * pitch + i].
+ *    Scalars are one plane. Every particle array in one call shares `pitch`.
+ *  - Grid nodes are indexed (i * R + j) * R + k like the reference
+ *    (physics/transfer.py:31-33). Mechanics nodes are packed float4:
+ *    node_pm = {px, py, pz, m} (momentum, mass), node_v = {vx, vy, vz, 0}.
+ *  - `stream` is a cudaStream_t passed as void*; every call is asynchronous on it.
+ *  - Return value: 0 on success, BK_ERR_* (< 0) on an invalid argument or a
+ *    launch failure; bk_last_error() describes the most recent failure of the
+ *    calling thread. No call aborts the process.
+ *  - Physical failures (inverted J, stencil outside the grid, porosity domain,
+ *    gas CFL, transport stability) are reported exactly as in the reference:
+ *    int flags on the device set to 1, read by the host afterwards.
+ */
+#ifndef BAKING_B200_H
+#define BAKING_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BK_API __attribute__((visibility("default")))
+#else
+#define BK_API
+#endif
+
+#define BK_OK 0
+#define BK_ERR_ARGUMENT (-1)
+#define BK_ERR_LAUNCH (-2)
+#define BK_ERR_UNSUPPORTED (-3)
+
+typedef struct BkDingParams {
+    int32_t coupled_porosity;    /* gas mode: end-state porosity solve */
+    int32_t temperature_enabled;
+    float shear_modulus, lame_lambda, yield_stress, initial_porosity, time_step;
+    float temperature_knots[4], yield_factors[4], viscosity_factors[4];
+} BkDingParams;
+
+typedef struct BkScalarParams {
+    float oven_temperature, tray_temperature, tray_transfer, surface_loss, water_density, latent_heat;
+    int32_t water_enabled;
+    float origin[3];
+    float spacing;
+    int32_t resolution;
+} BkScalarParams;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+BK_API int bk_version(void);
+/* Message of the last failed call on this thread ("" if none). */
+BK_API const char *bk_last_error(void);
+
+/* ---- mechanics: physics/transfer.py, physics/grid.py ------------------- */
+
+/* ParticleToGrid, physics/transfer.py:36-70. Adds w*m and w*(m v + A (x_i - x_p)) into node_pm. */
+BK_API int bk_particle_to_grid(int64_t n, int64_t pitch, const float *x, const float *v, const float *C,
+                        const float *tau, const float *mass, const float *V0, float *node_pm,
+                        const float *origin, float spacing, int32_t resolution, float time_step,
+                        int32_t *flags, void *stream);
+
+/* UpdateGrid, physics/grid.py:20-38. v = p/m + dt g with unilateral walls, where m > 0. */
+BK_API int bk_update_grid(int32_t resolution, const float *node_pm, float *node_v, int32_t boundary_cells,
+                   const float *gravity, float time_step, void *stream);
+
+/* GridToParticle, physics/transfer.py:73-109. */
+BK_API int bk_grid_to_particle(int64_t n, int64_t pitch, const float *x_in, const float *F_in, const float *node_v,
+                        float *x_out, float *v_out, float *C_out, float *F_out, const float *origin,
+                        float spacing, int32_t resolution, float time_step, int32_t *flags, void *stream);
+
+/* ---- materials: physics/materials/{elastic,ding,gas}.py ------------------ */
+
+/* ComputeElasticStress, physics/materials/elastic.py:13-26. */
+BK_API int bk_compute_elastic_stress(int64_t n, int64_t pitch, const float *F, float *tau, float shear_modulus,
+                              float lame_lambda, int32_t *flags, void *stream);
+
+/* UpdateDing, physics/materials/ding.py:140-221 (ding_return :103-137, solve_porosity
+   physics/materials/porous_return.py:43-61). flags has 3 entries (ding.py:232). */
+BK_API int bk_update_ding(int64_t n, int64_t pitch, const float *Fe_old, const float *porosity_old,
+                   const int32_t *gelled_old, const float *F_total, const float *C_new, float *Fe_new,
+                   float *Fp_new, float *tau_new, float *residuals, float *porosity_new, float *temperature_out,
+                   int32_t *gelled_new, float *yield_out, float *viscosity_out, const float *viscosity_parameter,
+                   int32_t *flags, float *porosity_residuals, const BkDingParams *params,
+                   const float *temperature_local, void *stream);
+
+/* CombineGasStress, physics/materials/gas.py:16-35. */
+BK_API int bk_combine_gas_stress(int64_t n, int64_t pitch, const float *tau_solid, const float *F, const float *porosity,
+                          const double *moles, const float *temperature, float *tau_total, int32_t *flags,
+                          float ambient_pressure, float initial_porosity, const float *density,
+                          float elastic_modulus, float time_step, float spacing, float cfl_limit, void *stream);
+
+/* RefreshGas, physics/materials/gas.py:38-45. */
+BK_API int bk_refresh_gas(int64_t n, int64_t pitch, const double *old_moles, double *new_moles, const float *F,
+                   const float *porosity, double *pressures, const float *temperature, void *stream);
+
+/* ---- transport: physics/thermal_water.py, geometry/mesh_tracking.py ---- */
+
+/* ReconstructMeshVertices, geometry/mesh_tracking.py:13-38. Vertex arrays use `vertex_pitch`;
+   reference_offsets are 3 planes of `binding_pitch` (one entry per binding). */
+BK_API int bk_reconstruct_mesh_vertices(int64_t vertex_count, int64_t pitch, const float *x, const float *F,
+                                 int64_t vertex_pitch, const float *reference_vertices, const int32_t *offsets,
+                                 const int32_t *particles, const float *weights, int64_t binding_pitch,
+                                 const float *reference_offsets, float *out_vertices, void *stream);
+
+/* SurfaceAreas, physics/thermal_water.py:77-92. faces: face_count x 3 int32 (row-major). */
+BK_API int bk_surface_areas(int64_t face_count, int64_t vertex_pitch, const float *vertices, const int32_t *faces,
+                     const int32_t *owners, double *exposed, double *contact, float floor_height,
+                     float contact_distance, void *stream);
+
+/* ScalarToGrid, physics/thermal_water.py:95-137. node_fields: 7 arrays of R^3 doubles in the order
+   volumes, capacities, energy, water, heat, loss, exchange. */
+BK_API int bk_scalar_to_grid(int64_t n, int64_t pitch, const float *x, const float *F, const float *V0,
+                      const double *capacities, const double *temperatures, const double *water,
+                      const double *exposed, const double *contact, const float *heat_parameter,
+                      const BkScalarParams *params, double *const *node_fields, double *particle_heat,
+                      double *particle_loss, int32_t *flags, void *stream);
+
+/* GridFields, physics/thermal_water.py:140-147. */
+BK_API int bk_grid_fields(int64_t node_count, const double *volumes, const double *capacities, const double *energy,
+                   const double *water, double *temperatures, double *saturations, float water_density,
+                   void *stream);
+
+/* DiffuseGrid, physics/thermal_water.py:150-190 (7-point finite-volume stencil). */
+BK_API int bk_diffuse_grid(int64_t node_count, const double *volumes, const double *capacities,
+                    const double *temperatures, const double *saturations, const double *water,
+                    const double *boundary_heat, const double *boundary_loss, const double *boundary_exchange,
+                    double *temperature_changes, double *water_changes, int32_t *errors, float conductivity,
+                    float diffusivity, float water_density, int32_t water_enabled, float spacing,
+                    int32_t resolution, float time_step, void *stream);
+
+/* ScalarToParticles, physics/thermal_water.py:193-229. */
+BK_API int bk_scalar_to_particles(int64_t n, int64_t pitch, const float *x, const double *T_old, const double *W_old,
+                           const double *loss_old, const double *exchange_old, const double *dry_masses,
+                           const float *V0, const float *F, const double *node_water, const double *node_dT,
+                           const double *node_dW, const double *particle_heat, const double *particle_loss,
+                           double *T_new, float *T_material, double *W_new, double *loss_new, double *exchange_new,
+                           float *mass_new, float *density_new, double *saturation_new, float water_density,
+                           const float *origin, float spacing, int32_t resolution, float time_step,
+                           int32_t *flags, void *stream);
+
+/* LocalGas, physics/thermal_water.py:232-245. parameter has n entries when per_particle != 0
+   (per-particle source rate), else 1. */
+BK_API int bk_local_gas(int64_t n, int64_t pitch, const double *old_moles, const double *T_old, const double *T_new,
+                 double *new_moles, double *pressures, const float *F, const float *porosity,
+                 const float *parameter, int32_t per_particle, float density, float peak, float width,
+                 float time_step, int32_t produce, void *stream);
+
+/* WaterStress, physics/thermal_water.py:248-253. */
+BK_API int bk_water_stress(int64_t n, int64_t pitch, const float *F, const double *saturations, const float *tau_old,
+                    float *tau_new, float initial_saturation, float stiffness, void *stream);
+
+/* Saturations, physics/thermal_water.py:256-260. */
+BK_API int bk_saturations(int64_t n, int64_t pitch, const double *water, const float *V0, const float *F,
+                   double *saturations, float density, void *stream);
+
+/* SettlingMetrics, physics/quasistatic.py:11-21. metrics: 3 floats, max-reduced. */
+BK_API int bk_settling_metrics(int64_t n, int64_t pitch, const float *v, const float *C, const float *Fp_old,
+                        const float *Fp_new, float *metrics, float time_step, void *stream);
+
+
+/* Device evaluation of the float64 end-state porosity solve, one problem per entry:
+   solve_porosity (physics/materials/porous_return.py:43-61) into porosity[i] and
+   porosity_prediction (:34-40) of that result into prediction[i]. */
+BK_API int bk_solve_porosity(int64_t n, const float *q, const float *p, const float *dev_factor,
+                             const float *mean_scale, const float *exponent, const double *plastic_volume,
+                             float initial_porosity, float *porosity, double *prediction, void *stream);
+
+/* Device evaluation of porosity_coefficient (physics/materials/ding.py:68-74) per entry. */
+BK_API int bk_porosity_coefficient(int64_t n, const float *porosity, float *coefficient, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BAKING_B200_H */
