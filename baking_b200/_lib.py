@@ -53,6 +53,9 @@ SIGNATURES = {
     "bk_settling_metrics": [I64, I64, P, P, P, P, P, F32, P],
     "bk_solve_porosity": [I64, P, P, P, P, P, P, F32, P, P, P],
     "bk_porosity_coefficient": [I64, P, P, P],
+    "bk_profile_start": [],
+    "bk_profile_stop": [],
+    "bk_profile_report": [I32, P, I32, P, P, P],
 }
 
 _lib = None
@@ -95,13 +98,79 @@ def require_cuda(device=None):
     return torch.device(device if device not in (None, "auto", "cuda") else "cuda:0")
 
 
+class KernelTimer:
+    """Per-kernel CUDA-event timing while active: the library's own events around every launch
+    inside the fused entry points, plus host-side events around each other C-ABI call."""
+
+    active = None
+
+    def __enter__(self):
+        self.events = {}
+        lib = load()
+        lib.bk_profile_start()
+        KernelTimer.active = self
+        return self
+
+    def __exit__(self, *exc):
+        KernelTimer.active = None
+        load().bk_profile_stop()
+
+    def add(self, name, start, end):
+        if name.startswith("bk_substep"):
+            return  # timed kernel by kernel inside the library
+        self.events.setdefault(name, []).append((start, end))
+
+    def summary(self):
+        torch.cuda.synchronize()
+        out = {}
+        for name, pairs in self.events.items():
+            times = [a.elapsed_time(b) / 1e3 for a, b in pairs]
+            out[name] = {"count": len(times), "total_s": sum(times), "mean_s": sum(times) / len(times)}
+        lib = load()
+        cap, kmax = 64, 64
+        names = C.create_string_buffer(cap * kmax)
+        totals = (C.c_double * kmax)()
+        counts = (C.c_int32 * kmax)()
+        got = C.c_int32(0)
+        if lib.bk_profile_report(kmax, names, cap, totals, counts, C.byref(got)) != 0:
+            raise RuntimeError(lib.bk_last_error().decode(errors="replace"))
+        for k in range(got.value):
+            name = names.raw[k * cap:(k + 1) * cap].split(b"\0", 1)[0].decode()
+            if counts[k]:
+                out[name] = {"count": int(counts[k]), "total_s": totals[k] / 1e3, "mean_s": totals[k] / 1e3 / counts[k]}
+        return out
+
+
 def call(name, *args):
     """Call one C-ABI entry point; raise RuntimeError on a nonzero status."""
     lib = load()
-    rc = getattr(lib, name)(*args)
+    timer = KernelTimer.active
+    if timer is not None:
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        rc = getattr(lib, name)(*args)
+        end.record()
+        timer.add(name, start, end)
+    else:
+        rc = getattr(lib, name)(*args)
     if rc != 0:
         message = lib.bk_last_error().decode(errors="replace")
         raise RuntimeError(f"{name} failed ({rc}): {message}")
+
+
+def call_raw(fn, name, *args):
+    """Call an already-declared C-ABI function object (timed like ``call``); raise on failure."""
+    timer = KernelTimer.active
+    if timer is not None:
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        rc = fn(*args)
+        end.record()
+        timer.add(name, start, end)
+    else:
+        rc = fn(*args)
+    if rc != 0:
+        raise RuntimeError(f"{name} failed ({rc}): {load().bk_last_error().decode(errors='replace')}")
 
 
 def stream_handle(device=None):

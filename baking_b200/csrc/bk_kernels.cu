@@ -7,20 +7,21 @@
 #include <cstring>
 
 #include "baking_b200.h"
+#include "bk_common.h"
 #include "bk_device.cuh"
 
 using namespace bk;
 
 namespace {
-
 thread_local char g_error[512] = "";
+}
 
-int fail(int code, const char* msg) {
+int bk::fail(int code, const char* msg) {
     snprintf(g_error, sizeof g_error, "%s", msg);
     return code;
 }
 
-int check_launch(const char* name) {
+int bk::check_launch(const char* name) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         snprintf(g_error, sizeof g_error, "%s: %s", name, cudaGetErrorString(e));
@@ -28,6 +29,8 @@ int check_launch(const char* name) {
     }
     return BK_OK;
 }
+
+namespace {
 
 constexpr int kBlock = 256;
 

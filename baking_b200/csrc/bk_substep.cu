@@ -1,0 +1,832 @@
+// Fused MLS-MPM baking substep for sm_100a (the simulator's hot path).
+//
+// The reference runs ~16 Warp launches per substep (physics/mpm.py:163-225,
+// physics/thermal_water.py:296-367) with three host synchronisations and fresh
+// dense-grid allocations. Here one substep is seven launches:
+//
+//   surface_vertices   rebuild only the boundary-face vertices (warp per vertex)
+//   surface_owners     face areas -> boundary heat/loss/exchange of face-owning particles, scattered
+//   transport_scatter  scalar P2G (volume, capacity, energy, water), warp-cooperative per stencil base
+//   diffuse            7-point finite-volume heat/water flux over the active node box only
+//   p2g                scalar G2P + gas source + gas/water stress + momentum P2G, fused per particle
+//   grid_update        momentum -> velocity with walls over the active box; zeroes the scatter fields
+//   g2p_return         G2P (v, C, x, F) fused with the Ding return map (float64 SVD in registers)
+//
+// Scatter scheme ("warp-cooperative stencil runs"): a warp loads 32 consecutive
+// particles; consecutive lanes whose particles share a stencil base form a run;
+// for each run, lane j < 27 owns stencil node j, sums the run's contributions in
+// registers (particle data broadcast from shared memory) and issues one atomic
+// per field. With particles ordered by cell this turns 27 atomics per particle
+// into 27 per run of ~tens of particles, and any order stays correct.
+//
+// The active node box (min/max stencil node of the current particles) bounds
+// every dense grid pass; the grid passes leave the scatter fields zeroed behind
+// them, so no dense memset is needed between substeps.
+#include <cfloat>
+#include <climits>
+#include <cstdio>
+
+#include "baking_b200.h"
+#include "bk_common.h"
+#include "bk_device.cuh"
+#include "bk_profile.h"
+
+using namespace bk;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr unsigned kFull = 0xffffffffu;
+
+inline cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Kernel-side copy of the parameters (plain values only).
+struct Params {
+    int64_t n, pitch;
+    int R, bc;
+    float origin[3], dx, dt, gravity[3];
+    int material;
+    DingParamsDev ding;
+    int transport, gas, settling;
+    float oven, tray, tray_transfer, surface_loss, water_density, latent;
+    int water_enabled;
+    float conductivity, diffusivity, s0, water_stress;
+    float ambient, density, elastic_modulus, cfl, peak, width;
+};
+
+Params to_params(const BkSubstepParams& p) {
+    Params k;
+    k.n = p.n; k.pitch = p.pitch; k.R = p.resolution; k.bc = p.boundary_cells;
+    for (int a = 0; a < 3; ++a) { k.origin[a] = p.origin[a]; k.gravity[a] = p.gravity[a]; }
+    k.dx = p.spacing; k.dt = p.time_step;
+    k.material = p.material;
+    const BkDingParams& d = p.ding;
+    k.ding.coupled_porosity = d.coupled_porosity; k.ding.temperature_enabled = d.temperature_enabled;
+    k.ding.mu = d.shear_modulus; k.ding.lam = d.lame_lambda; k.ding.yield_stress = d.yield_stress;
+    k.ding.initial_porosity = d.initial_porosity; k.ding.dt = d.time_step;
+    for (int i = 0; i < 4; ++i) {
+        k.ding.knots[i] = d.temperature_knots[i];
+        k.ding.yield_factors[i] = d.yield_factors[i];
+        k.ding.viscosity_factors[i] = d.viscosity_factors[i];
+    }
+    k.transport = p.transport; k.gas = p.gas; k.settling = p.settling;
+    k.oven = p.scalar.oven_temperature; k.tray = p.scalar.tray_temperature;
+    k.tray_transfer = p.scalar.tray_transfer; k.surface_loss = p.scalar.surface_loss;
+    k.water_density = p.scalar.water_density; k.latent = p.scalar.latent_heat;
+    k.water_enabled = p.scalar.water_enabled;
+    k.conductivity = p.conductivity; k.diffusivity = p.diffusivity; k.s0 = p.initial_saturation;
+    k.water_stress = p.water_stress;
+    k.ambient = p.gas_ambient_pressure; k.density = p.density; k.elastic_modulus = p.elastic_modulus;
+    k.cfl = p.cfl_limit; k.peak = p.gas_peak; k.width = p.gas_width;
+    return k;
+}
+
+struct GridPtrs {
+    float4* pm;
+    float4* v;
+    double* f[7];
+    double2* dTr;
+    int* bounds;
+};
+
+GridPtrs grid_ptrs(const BkGrid& g) {
+    GridPtrs r;
+    r.pm = reinterpret_cast<float4*>(g.node_pm);
+    r.v = reinterpret_cast<float4*>(g.node_v);
+    for (int k = 0; k < 7; ++k) r.f[k] = g.fields[k];
+    r.dTr = reinterpret_cast<double2*>(g.node_dT_ratio);
+    r.bounds = g.bounds;
+    return r;
+}
+
+// Stencil node j in 0..26 -> offsets (j / 9, (j / 3) % 3, j % 3), the reference's loop order.
+__device__ __forceinline__ void node_offset(int j, int& ox, int& oy, int& oz) {
+    ox = j / 9;
+    oy = (j / 3) % 3;
+    oz = j - 9 * ox - 3 * oy;
+}
+
+__device__ __forceinline__ long long pack_base(const int* b) {
+    return ((long long)b[0] << 42) | ((long long)b[1] << 21) | (long long)b[2];
+}
+
+// Block-level min/max of valid stencil nodes into the active node box (bounds[0..2] lo, [3..5] hi).
+// Every thread of the block must call this (it synchronises the block).
+__device__ void update_bounds(int* bounds, bool valid, const int* b) {
+    __shared__ int s_box[6];
+    if (threadIdx.x < 6) s_box[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int lo = __reduce_min_sync(kFull, valid ? b[a] : INT_MAX);
+        int hi = __reduce_max_sync(kFull, valid ? b[a] + 2 : INT_MIN);
+        if ((threadIdx.x & 31) == 0 && lo != INT_MAX) {
+            atomicMin(&s_box[a], lo);
+            atomicMax(&s_box[3 + a], hi);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3 && s_box[threadIdx.x] != INT_MAX) {
+        atomicMin(bounds + threadIdx.x, s_box[threadIdx.x]);
+        atomicMax(bounds + 3 + threadIdx.x, s_box[3 + threadIdx.x]);
+    }
+}
+
+// ------------------------------------------------------------------ surface
+// geometry/mesh_tracking.py:13-38 restricted to the vertices of boundary faces; one warp per vertex.
+__global__ void k_surface_vertices(Params P, const float* __restrict__ x, const float* __restrict__ F,
+                                   BkSurface sf) {
+    int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (w >= sf.vertex_count) return;
+    int vid = sf.vertex_ids[w];
+    int b0 = sf.binding_offsets[vid], b1 = sf.binding_offsets[vid + 1];
+    const int64_t vp = sf.vertex_pitch, bp = sf.binding_pitch, pitch = P.pitch;
+    if (b0 == b1) {
+        if (lane < 3) sf.vertices[lane * vp + vid] = sf.reference_vertices[lane * vp + vid];
+        return;
+    }
+    auto predict = [&](int b, float* r) {
+        int p = sf.binding_particles[b];
+        M3 f = load_m3(F, p, pitch);
+        V3 xp = load_v3(x, p, pitch);
+        float o[3] = {sf.reference_offsets[b], sf.reference_offsets[bp + b], sf.reference_offsets[2 * bp + b]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) r[a] = xp.v[a] + (f.m[3 * a] * o[0] + f.m[3 * a + 1] * o[1] + f.m[3 * a + 2] * o[2]);
+    };
+    float anchor[3];
+    predict(b0, anchor);
+    float disp[3] = {0.f, 0.f, 0.f};
+    for (int b = b0 + lane; b < b1; b += 32) {
+        float pr[3];
+        predict(b, pr);
+        float wgt = sf.binding_weights[b];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) disp[a] += wgt * (pr[a] - anchor[a]);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) disp[a] += __shfl_xor_sync(kFull, disp[a], o);
+    if (lane < 3) sf.vertices[lane * vp + vid] = anchor[lane] + disp[lane];
+}
+
+// physics/thermal_water.py:77-92 (face areas, tray contact) and the surface terms of :108-122,
+// per face-owning particle, scattered into the heat/loss/exchange node fields.
+__global__ void k_surface_owners(Params P, BkState in, BkConstants cst, BkSurface sf, GridPtrs g, int32_t* sim_flags) {
+    int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (o >= sf.owner_count) return;
+    const int64_t vp = sf.vertex_pitch, pitch = P.pitch;
+    int p = sf.owners[o];
+    double exposed = 0.0, contact = 0.0;
+    for (int f = sf.owner_face_offsets[o]; f < sf.owner_face_offsets[o + 1]; ++f) {
+        double q[3][3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            int vid = sf.faces[3 * f + k];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) q[k][a] = (double)sf.vertices[a * vp + vid];
+        }
+        double e1[3] = {q[1][0] - q[0][0], q[1][1] - q[0][1], q[1][2] - q[0][2]};
+        double e2[3] = {q[2][0] - q[0][0], q[2][1] - q[0][1], q[2][2] - q[0][2]};
+        double nr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        double len = sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]);
+        double area = 0.5 * len;
+        double cy = (q[0][1] + q[1][1] + q[2][1]) / 3.0;
+        if (cy <= (double)(sf.floor_height + sf.contact_distance) && nr[1] < -0.2 * len) contact += area;
+        else exposed += area;
+    }
+    double vol = (double)cst.volume[p] * (double)det3(load_m3(in.F, p, pitch));
+    double T = in.temperature[p], W = in.water[p];
+    double sat = W / ((double)P.water_density * vol);
+    double loss = 0.0;
+    if (P.water_enabled) loss = (double)P.surface_loss * T * sat * exposed;
+    double h = (double)cst.heat_parameter[0];
+    double heat = h * exposed * ((double)P.oven - T) + (double)P.tray_transfer * contact * ((double)P.tray - T)
+                - (double)P.latent * loss;
+    double exch = h * exposed + (double)P.tray_transfer * contact;
+    if (P.water_enabled) exch += (double)(P.latent * P.surface_loss) * sat * exposed;
+    sf.owner_heat[o] = heat;
+    sf.owner_loss[o] = loss;
+    Stencil st = make_stencil(load_v3(in.x, p, pitch), P.origin, P.dx, P.R);
+    if (!st.valid) { set_flag(sim_flags, 1); return; }
+#pragma unroll 1
+    for (int j = 0; j < 27; ++j) {
+        int ox, oy, oz;
+        node_offset(j, ox, oy, oz);
+        double w = (double)(st.w[0][ox] * st.w[1][oy] * st.w[2][oz]);
+        int64_t node = node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R);
+        atomicAdd(g.f[4] + node, w * heat);
+        atomicAdd(g.f[5] + node, w * loss);
+        atomicAdd(g.f[6] + node, w * exch);
+    }
+}
+
+// ---------------------------------------------------------- transport P2G
+// physics/thermal_water.py:108-137 (volume, capacity, energy, water), warp-cooperative per stencil run.
+struct TransportSmem {
+    float w[kThreads][9];
+    double val[kThreads][4];
+};
+
+__global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkState in, BkConstants cst, GridPtrs g,
+                                                               int32_t* sim_flags) {
+    __shared__ TransportSmem sm;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int64_t i = blockIdx.x * (int64_t)kThreads + tid;
+    const int64_t pitch = P.pitch;
+    bool valid = false;
+    Stencil st;
+    st.b[0] = st.b[1] = st.b[2] = 0;
+    if (i < P.n) {
+        st = make_stencil(load_v3(in.x, i, pitch), P.origin, P.dx, P.R);
+        valid = st.valid;
+        if (!valid) set_flag(sim_flags, 1);
+    }
+    if (valid) {
+        double vol = (double)cst.volume[i] * (double)det3(load_m3(in.F, i, pitch));
+        double cap = cst.capacity[i], T = in.temperature[i];
+        sm.val[tid][0] = vol;
+        sm.val[tid][1] = cap;
+        sm.val[tid][2] = cap * T;
+        sm.val[tid][3] = in.water[i];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int o = 0; o < 3; ++o) sm.w[tid][3 * a + o] = st.w[a][o];
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) sm.val[tid][k] = 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) sm.w[tid][k] = 0.f;
+    }
+    update_bounds(g.bounds, valid, st.b);  // contains __syncthreads
+    long long key = valid ? pack_base(st.b) : -1;
+    long long prev = __shfl_up_sync(kFull, key, 1);
+    unsigned starts = __ballot_sync(kFull, valid && (lane == 0 || prev != key));
+    const int warp_base = tid & ~31;
+    int ox, oy, oz;
+    node_offset(lane < 27 ? lane : 0, ox, oy, oz);
+    while (starts) {
+        int s = __ffs(starts) - 1;
+        starts &= starts - 1;
+        int e = starts ? __ffs(starts) - 1 : 32;
+        int b0 = __shfl_sync(kFull, st.b[0], s), b1 = __shfl_sync(kFull, st.b[1], s), b2 = __shfl_sync(kFull, st.b[2], s);
+        if (lane < 27) {
+            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int k = warp_base + s; k < warp_base + e; ++k) {
+                double w = (double)(sm.w[k][ox] * sm.w[k][3 + oy] * sm.w[k][6 + oz]);
+#pragma unroll
+                for (int f = 0; f < 4; ++f) acc[f] += w * sm.val[k][f];
+            }
+            int64_t node = node_index(b0 + ox, b1 + oy, b2 + oz, P.R);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) atomicAdd(g.f[f] + node, acc[f]);
+        }
+    }
+}
+
+// ------------------------------------------------------------ grid passes
+// Node box [lo, hi] of `bounds` clipped to the grid; false when it is empty. The empty box is
+// stored as lo = INT_MAX, hi = INT_MIN, so emptiness is tested before any subtraction.
+__device__ __forceinline__ bool box_of(const int* bounds, int R, int lo[3], int ext[3], int64_t& count) {
+    count = 1;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int l = bounds[a], h = bounds[3 + a];
+        if (l > h) return false;
+        l = max(l, 0);
+        h = min(h, R - 1);
+        if (l > h) return false;
+        lo[a] = l;
+        ext[a] = h - l + 1;
+        count *= ext[a];
+    }
+    return true;
+}
+
+// physics/thermal_water.py:140-190: node temperature/saturation and the 7-point flux, over the active box.
+__global__ void k_diffuse(Params P, GridPtrs g, int32_t* errors) {
+    int lo[3], ext[3];
+    int64_t count;
+    if (!box_of(g.bounds, P.R, lo, ext, count)) return;
+    const int R = P.R;
+    const double rho_w = (double)P.water_density;
+    const double cell = (double)(P.dx * P.dx * P.dx);
+    const double kc = (double)(P.conductivity * P.dx);
+    const double kw = (double)(P.diffusivity * P.water_density * P.dx);
+    const double dt = (double)P.dt;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+        int c[3];
+        c[2] = lo[2] + (int)(t % ext[2]);
+        c[1] = lo[1] + (int)((t / ext[2]) % ext[1]);
+        c[0] = lo[0] + (int)(t / ((int64_t)ext[2] * ext[1]));
+        int64_t i = node_index(c[0], c[1], c[2], R);
+        double ci = g.f[1][i];
+        if (!(ci > 0.0)) {
+            g.dTr[i] = make_double2(0.0, 0.0);
+            continue;
+        }
+        double vi = g.f[0][i], Wi = g.f[3][i];
+        double Ti = g.f[2][i] / ci, si = Wi / (rho_w * vi);
+        double heat_rate = g.f[4][i], water_rate = -g.f[5][i], heat_diag = g.f[6][i], water_diag = 0.0;
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis)
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                int o[3] = {c[0], c[1], c[2]};
+                o[axis] += 2 * side - 1;
+                if (o[axis] < 0 || o[axis] >= R) continue;
+                int64_t j = node_index(o[0], o[1], o[2], R);
+                double cj = g.f[1][j];
+                if (!(cj > 0.0)) continue;
+                double vj = g.f[0][j];
+                double Tj = g.f[2][j] / cj;
+                double fill = 2.0 * vi * vj / (vi + vj) / cell;
+                double hc = kc * fill;
+                heat_rate += hc * (Tj - Ti);
+                heat_diag += hc;
+                if (P.water_enabled) {
+                    double sj = g.f[3][j] / (rho_w * vj);
+                    double mob = kw * fill * 0.5 * (Ti + Tj) * 0.5 * (si + sj);
+                    water_rate += mob * (sj - si);
+                    water_diag += mob / (rho_w * vi);
+                }
+            }
+        if (dt * heat_diag > ci) set_flag(errors, 0);
+        double change = dt * water_rate;
+        if (Wi + change < 0.0 || dt * water_diag > 1.0) set_flag(errors, 1);
+        double dT = dt * heat_rate / ci;
+        g.dTr[i] = make_double2(dT, Wi > 0.0 ? change / Wi : 0.0);
+    }
+}
+
+// GridState.Clear (physics/grid.py:14-17) restricted to the previous substep's active box, the only
+// nodes holding nonzero momentum, mass or velocity; the grid of the last substep stays readable
+// until the next one starts.
+__global__ void k_clear_previous(Params P, GridPtrs g) {
+    int lo[3], ext[3];
+    int64_t count;
+    if (!box_of(g.bounds + 6, P.R, lo, ext, count)) return;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+        int c2 = lo[2] + (int)(t % ext[2]);
+        int c1 = lo[1] + (int)((t / ext[2]) % ext[1]);
+        int c0 = lo[0] + (int)(t / ((int64_t)ext[2] * ext[1]));
+        int64_t i = node_index(c0, c1, c2, P.R);
+        g.pm[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        g.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+}
+
+// physics/grid.py:20-38 over the active box; clears the transport scatter fields behind it.
+__global__ void k_grid_update(Params P, GridPtrs g) {
+    int lo[3], ext[3];
+    int64_t count;
+    if (!box_of(g.bounds, P.R, lo, ext, count)) return;
+    const int R = P.R, bc = P.bc;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+        int c[3];
+        c[2] = lo[2] + (int)(t % ext[2]);
+        c[1] = lo[1] + (int)((t / ext[2]) % ext[1]);
+        c[0] = lo[0] + (int)(t / ((int64_t)ext[2] * ext[1]));
+        int64_t i = node_index(c[0], c[1], c[2], R);
+        float4 pm = g.pm[i];
+        float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (pm.w > 0.0f) {
+            float vel[3] = {pm.x / pm.w + P.dt * P.gravity[0], pm.y / pm.w + P.dt * P.gravity[1],
+                            pm.z / pm.w + P.dt * P.gravity[2]};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (c[a] < bc && vel[a] < 0.0f) vel[a] = 0.0f;
+                if (c[a] >= R - bc && vel[a] > 0.0f) vel[a] = 0.0f;
+            }
+            out = make_float4(vel[0], vel[1], vel[2], 0.f);
+        }
+        g.v[i] = out;
+        if (P.transport) {
+#pragma unroll
+            for (int k = 0; k < 7; ++k) g.f[k][i] = 0.0;
+        }
+    }
+}
+
+// ------------------------------------------------------------- fused P2G
+// Scalar G2P (thermal_water.py:206-229), local gas source (:238-245), gas stress (gas.py:16-35),
+// water stress (thermal_water.py:248-253) and momentum P2G (transfer.py:47-70) for one particle
+// per thread, then the warp-cooperative momentum scatter.
+struct P2GSmem {
+    float w[kThreads][9];
+    float m[kThreads];
+    float q[kThreads][3];
+    float A[kThreads][9];
+};
+
+__global__ void __launch_bounds__(kThreads) k_p2g(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
+                                                 BkFlags flags, float* max_residuals) {
+    __shared__ P2GSmem sm;
+    if (blockIdx.x == 0 && threadIdx.x < 2) max_residuals[threadIdx.x] = 0.0f;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int64_t i = blockIdx.x * (int64_t)kThreads + tid;
+    const int64_t pitch = P.pitch;
+    bool valid = false;
+    Stencil st;
+    st.b[0] = st.b[1] = st.b[2] = 0;
+    float mass = 0.f, q[3] = {0.f, 0.f, 0.f}, A[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (i < P.n) {
+        V3 x = load_v3(in.x, i, pitch);
+        st = make_stencil(x, P.origin, P.dx, P.R);
+        valid = st.valid;
+        if (!valid) set_flag(flags.simulation, 1);
+    }
+    if (valid) {
+        M3 F = load_m3(in.F, i, pitch);
+        float J = det3(F);
+        M3 tau;
+        float T_mat = 0.f;
+        float rho_ref = P.density;
+        double sat = 0.0;
+        if (P.transport) {
+            double dTp = 0.0, ratio = 0.0;
+#pragma unroll
+            for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+                for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                    for (int oz = 0; oz < 3; ++oz) {
+                        double w = (double)(st.w[0][ox] * st.w[1][oy] * st.w[2][oz]);
+                        double2 d = __ldg(g.dTr + node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R));
+                        dTp += w * d.x;
+                        ratio += w * d.y;
+                    }
+            double T_old = in.temperature[i];
+            double Tn = T_old + dTp;
+            double Wn = in.water[i] * (1.0 + ratio);
+            double dry = cst.dry_mass[i];
+            float V0 = cst.volume[i];
+            out.temperature[i] = Tn;
+            out.water[i] = Wn;
+            mass = (float)(dry + Wn);
+            rho_ref = (float)((dry + Wn) / (double)V0);
+            sat = Wn / ((double)P.water_density * (double)V0 * (double)J);
+            T_mat = (float)Tn;
+            if (P.gas) {
+                double N = in.gas_moles[i];
+                if (!P.settling) {
+                    double Tm = 0.5 * (T_old + Tn);
+                    double z = (Tm - (double)P.peak) / (double)P.width;
+                    N += (double)(P.dt * P.density) * (double)cst.gas_rate[cst.gas_rate_per_particle ? i : 0] *
+                         exp(-(z * z));
+                }
+                out.gas_moles[i] = N;
+            }
+        } else {
+            mass = cst.mass[i];
+            if (P.material == 1) T_mat = in.material_temperature[i];
+        }
+        if (P.material == 1) {
+            tau = load_m3(in.tau, i, pitch);
+            if (P.gas) {
+                float n = in.porosity[i];
+                if (n <= 0.0f || n >= 1.0f || !isfinite(n) || J <= 0.0f) {
+                    set_flag(flags.ding, 0);
+                } else {
+                    float p = (float)gas_pressure(out.gas_moles[i], T_mat, J, n);
+                    float iso = J * (P.ambient - p);
+#pragma unroll
+                    for (int e = 0; e < 9; ++e) tau.m[e] += (e % 4) == 0 ? iso : iso * 0.0f;
+                    float bulk = p * (1.0f + (1.0f - P.ding.initial_porosity + n) / n);
+                    float wave = sqrtf((P.elastic_modulus + bulk) * J / rho_ref);
+                    if (!isfinite(p) || wave * P.dt / P.dx > P.cfl) set_flag(flags.ding, 2);
+                }
+            }
+        } else {
+            if (!isfinite(J) || J <= 0.0f) {
+                set_flag(flags.simulation, 0);
+#pragma unroll
+                for (int e = 0; e < 9; ++e) tau.m[e] = 0.0f;
+            } else {
+                float lj = logf(J);
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        float ffT = F.m[3 * r] * F.m[3 * c] + F.m[3 * r + 1] * F.m[3 * c + 1] + F.m[3 * r + 2] * F.m[3 * c + 2];
+                        float id = r == c ? 1.0f : 0.0f;
+                        tau.m[3 * r + c] = P.ding.mu * (ffT - id) + P.ding.lam * lj * id;
+                    }
+            }
+        }
+        if (P.transport) {
+            float iso = J * P.water_stress * ((float)sat - P.s0);
+#pragma unroll
+            for (int e = 0; e < 9; ++e) tau.m[e] -= (e % 4) == 0 ? iso : iso * 0.0f;
+        }
+        float scale = P.dt * cst.volume[i] * 4.0f / (P.dx * P.dx);
+        M3 Cm = load_m3(in.C, i, pitch);
+        V3 vel = load_v3(in.v, i, pitch);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) A[e] = mass * Cm.m[e] - scale * tau.m[e];
+        // w (m v + A (o - l) dx) = w (q + A dx o) with q = m v - A l dx.
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+            q[r] = mass * vel.v[r] - (A[3 * r] * st.l[0] + A[3 * r + 1] * st.l[1] + A[3 * r + 2] * st.l[2]) * P.dx;
+#pragma unroll
+        for (int e = 0; e < 9; ++e) A[e] *= P.dx;
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int o = 0; o < 3; ++o) sm.w[tid][3 * a + o] = valid ? st.w[a][o] : 0.f;
+    sm.m[tid] = mass;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) sm.q[tid][r] = q[r];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) sm.A[tid][e] = A[e];
+    update_bounds(g.bounds, valid, st.b);  // contains __syncthreads
+    long long key = valid ? pack_base(st.b) : -1;
+    long long prev = __shfl_up_sync(kFull, key, 1);
+    unsigned starts = __ballot_sync(kFull, valid && (lane == 0 || prev != key));
+    const int warp_base = tid & ~31;
+    int ox, oy, oz;
+    node_offset(lane < 27 ? lane : 0, ox, oy, oz);
+    const float fo[3] = {(float)ox, (float)oy, (float)oz};
+    while (starts) {
+        int s = __ffs(starts) - 1;
+        starts &= starts - 1;
+        int e = starts ? __ffs(starts) - 1 : 32;
+        int b0 = __shfl_sync(kFull, st.b[0], s), b1 = __shfl_sync(kFull, st.b[1], s), b2 = __shfl_sync(kFull, st.b[2], s);
+        if (lane < 27) {
+            float am = 0.f, ap[3] = {0.f, 0.f, 0.f};
+            for (int k = warp_base + s; k < warp_base + e; ++k) {
+                float w = sm.w[k][ox] * sm.w[k][3 + oy] * sm.w[k][6 + oz];
+                am += w * sm.m[k];
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                    ap[r] += w * (sm.q[k][r] + (sm.A[k][3 * r] * fo[0] + sm.A[k][3 * r + 1] * fo[1] + sm.A[k][3 * r + 2] * fo[2]));
+            }
+            atomicAdd(g.pm + node_index(b0 + ox, b1 + oy, b2 + oz, P.R), make_float4(ap[0], ap[1], ap[2], am));
+        }
+    }
+}
+
+// ------------------------------------------------------ fused G2P + return
+__device__ __forceinline__ void atomic_max_nonneg(float* addr, float value) {
+    if (value > 0.0f) atomicMax(reinterpret_cast<int*>(addr), __float_as_int(value));
+}
+
+__global__ void __launch_bounds__(128) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
+                                                   BkDiagnostics diag, BkFlags flags) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (blockIdx.x == 0 && threadIdx.x < 6) {
+        // This substep's box becomes the box the next substep clears; the active box restarts empty.
+        g.bounds[6 + threadIdx.x] = g.bounds[threadIdx.x];
+        g.bounds[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
+    }
+    if (i >= P.n) return;
+    const int64_t pitch = P.pitch;
+    V3 xi = load_v3(in.x, i, pitch);
+    Stencil st = make_stencil(xi, P.origin, P.dx, P.R);
+    if (!st.valid) { set_flag(flags.simulation, 1); return; }
+    float nv[3] = {0.f, 0.f, 0.f}, nc[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float k = 4.0f / (P.dx * P.dx);
+#pragma unroll
+    for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+        for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+            for (int oz = 0; oz < 3; ++oz) {
+                float w = st.w[0][ox] * st.w[1][oy] * st.w[2][oz];
+                float d[3] = {((float)ox - st.l[0]) * P.dx, ((float)oy - st.l[1]) * P.dx, ((float)oz - st.l[2]) * P.dx};
+                float4 u = __ldg(g.v + node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R));
+                float uu[3] = {u.x, u.y, u.z};
+                float kw = k * w;
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    nv[r] += w * uu[r];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) nc[3 * r + c] += kw * (uu[r] * d[c]);
+                }
+            }
+    M3 F = load_m3(in.F, i, pitch);
+    M3 G, Cn;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+        Cn.m[e] = nc[e];
+        G.m[e] = P.dt * nc[e] + ((e % 4) == 0 ? 1.0f : 0.0f);
+    }
+    M3 Fn = matmul(G, F);
+    V3 vo{{nv[0], nv[1], nv[2]}}, xo{{xi.v[0] + P.dt * nv[0], xi.v[1] + P.dt * nv[1], xi.v[2] + P.dt * nv[2]}};
+    store_v3(out.v, i, pitch, vo);
+    store_m3(out.C, i, pitch, Cn);
+    store_v3(out.x, i, pitch, xo);
+    store_m3(out.F, i, pitch, Fn);
+    if (P.material != 1) return;
+    float T = P.transport ? (float)out.temperature[i] : in.material_temperature[i];
+    DingParticleOut o;
+    if (!update_ding_particle(P.ding, load_m3(in.Fe, i, pitch), in.porosity[i], in.gelled[i], Fn, Cn, T,
+                              __ldg(cst.viscosity_parameter), flags.ding, o))
+        return;
+    store_m3(out.Fe, i, pitch, o.Fe);
+    store_m3(out.tau, i, pitch, o.tau);
+    out.porosity[i] = o.porosity;
+    out.gelled[i] = o.gelled;
+    if (!P.transport) out.material_temperature[i] = T;
+    if (diag.plastic_gradients) store_m3(diag.plastic_gradients, i, pitch, o.Fp);
+    if (diag.return_residuals) diag.return_residuals[i] = o.residual;
+    if (diag.porosity_residuals) diag.porosity_residuals[i] = o.porosity_residual;
+    atomic_max_nonneg(diag.max_residuals, o.residual);
+    atomic_max_nonneg(diag.max_residuals + 1, o.porosity_residual);
+}
+
+// ------------------------------------------------------------ materialize
+__global__ void k_materialize(Params P, BkState s, BkConstants cst, float* Fp, float* T_mat, float* rho,
+                              float* yield, float* visc, double* gas_p, double* sat, float* mass) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const int64_t pitch = P.pitch;
+    M3 F = load_m3(s.F, i, pitch);
+    float J = det3(F);
+    float T = 0.f;
+    if (P.transport) {
+        double W = s.water[i], dry = cst.dry_mass[i];
+        double V0 = (double)cst.volume[i];
+        T = (float)s.temperature[i];
+        if (rho) rho[i] = (float)((dry + W) / V0);
+        if (sat) sat[i] = W / ((double)P.water_density * V0 * (double)J);
+        if (mass) mass[i] = (float)(dry + W);
+    } else if (P.material == 1) {
+        T = s.material_temperature[i];
+        if (rho) rho[i] = P.density;
+    }
+    if (P.material != 1) return;
+    if (T_mat) T_mat[i] = T;
+    if (Fp) store_m3(Fp, i, pitch, matmul(inverse3(load_m3(s.Fe, i, pitch)), F));
+    const DingParamsDev& D = P.ding;
+    float ty = D.yield_stress, eta = __ldg(cst.viscosity_parameter);
+    if (D.temperature_enabled) {
+        float Teff = s.gelled[i] ? D.knots[3] : T;
+        ty = D.yield_stress * temperature_factor(Teff, D.knots, D.yield_factors);
+        eta = eta * temperature_factor(Teff, D.knots, D.viscosity_factors);
+    }
+    if (yield) yield[i] = ty;
+    if (visc) visc[i] = eta;
+    if (gas_p && P.gas) {
+        float n = s.porosity[i];
+        if (n > 0.0f && n < 1.0f) gas_p[i] = gas_pressure(s.gas_moles[i], T, J, n);
+    }
+}
+
+// physics/thermal_water.py:225-226 for the face-owning particles (the only ones whose loss or
+// exchange changes): accumulators += dt * per-owner rate.
+__global__ void k_surface_accumulate(int64_t owners_n, const int32_t* __restrict__ owners,
+                                     const double* __restrict__ heat, const double* __restrict__ loss, double dt,
+                                     double* __restrict__ water_losses, double* __restrict__ heat_exchanges) {
+    int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (o >= owners_n) return;
+    int p = owners[o];
+    water_losses[p] += dt * loss[o];
+    heat_exchanges[p] += dt * heat[o];
+}
+
+unsigned blocks_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
+
+}  // namespace
+
+extern "C" {
+
+#define BK_REQUIRE(cond, msg) do { if (!(cond)) return fail(BK_ERR_ARGUMENT, msg); } while (0)
+
+int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, const BkConstants* constants,
+               BkGrid* grid, BkSurface* surface, BkDiagnostics* diagnostics, BkFlags* flags, int32_t phases,
+               void* stream) {
+    BK_REQUIRE(params && in && out && constants && grid && diagnostics && flags, "bk_substep: null argument");
+    const BkSubstepParams& p = *params;
+    BK_REQUIRE(p.n >= 0 && p.pitch >= p.n, "bk_substep: bad particle count/pitch");
+    BK_REQUIRE(p.resolution >= 4 && p.resolution < (1 << 20) && p.spacing > 0.0f, "bk_substep: bad grid");
+    BK_REQUIRE(grid->node_pm && grid->node_v && grid->bounds, "bk_substep: missing grid arrays");
+    BK_REQUIRE((((uintptr_t)grid->node_pm | (uintptr_t)grid->node_v) & 15) == 0, "bk_substep: grid not 16-byte aligned");
+    BK_REQUIRE(in->x && in->v && in->C && in->F && out->x && out->v && out->C && out->F, "bk_substep: missing state");
+    BK_REQUIRE(flags->simulation && flags->ding && flags->transport && diagnostics->max_residuals,
+               "bk_substep: missing flags");
+    if (p.material == 1)
+        BK_REQUIRE(in->Fe && in->tau && in->porosity && in->gelled && out->Fe && out->tau && out->porosity &&
+                   out->gelled && constants->viscosity_parameter, "bk_substep: missing Ding state");
+    if (p.material == 1 && !p.transport)
+        BK_REQUIRE(in->material_temperature && out->material_temperature, "bk_substep: missing Ding temperature");
+    if (p.transport) {
+        BK_REQUIRE(surface && in->temperature && in->water && out->temperature && out->water && constants->capacity &&
+                   constants->dry_mass && constants->heat_parameter && grid->node_dT_ratio,
+                   "bk_substep: missing transport arrays");
+        for (int k = 0; k < 7; ++k) BK_REQUIRE(grid->fields[k] != nullptr, "bk_substep: missing node field");
+        BK_REQUIRE(((uintptr_t)grid->node_dT_ratio & 15) == 0, "bk_substep: node_dT_ratio not 16-byte aligned");
+    } else {
+        BK_REQUIRE(constants->mass != nullptr, "bk_substep: missing particle masses");
+    }
+    if (p.gas)
+        BK_REQUIRE(p.transport && p.material == 1 && in->gas_moles && out->gas_moles && constants->gas_rate,
+                   "bk_substep: gas mode needs transport, the Ding model and gas arrays");
+    if (p.n == 0) return BK_OK;
+    Params P = to_params(p);
+    GridPtrs g = grid_ptrs(*grid);
+    cudaStream_t s = S(stream);
+    const unsigned particle_blocks = blocks_for(p.n, kThreads);
+    int device = 0, sms = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const unsigned box_blocks = (unsigned)sms * 4;
+    if ((phases & BK_PHASE_TRANSPORT) && p.transport) {
+        if (surface->vertex_count > 0) {
+            {
+                int rec = profile_begin("surface_vertices", s);
+                k_surface_vertices<<<blocks_for(surface->vertex_count * 32, kThreads), kThreads, 0, s>>>(P, in->x, in->F,
+                                                                                                   *surface);
+                profile_end(rec, s);
+            }
+            if (int rc = check_launch("bk_substep/surface_vertices")) return rc;
+        }
+        if (surface->owner_count > 0) {
+            {
+                int rec = profile_begin("surface_owners", s);
+                k_surface_owners<<<blocks_for(surface->owner_count, 128), 128, 0, s>>>(P, *in, *constants, *surface, g,
+                                                                                  flags->simulation);
+                profile_end(rec, s);
+            }
+            if (int rc = check_launch("bk_substep/surface_owners")) return rc;
+        }
+        {
+            int rec = profile_begin("transport_scatter", s);
+            k_transport_scatter<<<particle_blocks, kThreads, 0, s>>>(P, *in, *constants, g, flags->simulation);
+            profile_end(rec, s);
+        }
+        if (int rc = check_launch("bk_substep/transport_scatter")) return rc;
+        {
+            int rec = profile_begin("diffuse", s);
+            k_diffuse<<<box_blocks, kThreads, 0, s>>>(P, g, flags->transport);
+            profile_end(rec, s);
+        }
+        if (int rc = check_launch("bk_substep/diffuse")) return rc;
+    }
+    if (phases & BK_PHASE_MECHANICS) {
+        {
+            int rec = profile_begin("clear_previous", s);
+            k_clear_previous<<<box_blocks, kThreads, 0, s>>>(P, g);
+            profile_end(rec, s);
+        }
+        if (int rc = check_launch("bk_substep/clear_previous")) return rc;
+        {
+            int rec = profile_begin("p2g", s);
+            k_p2g<<<particle_blocks, kThreads, 0, s>>>(P, *in, *out, *constants, g, *flags,
+                                                   diagnostics->max_residuals);
+            profile_end(rec, s);
+        }
+        if (int rc = check_launch("bk_substep/p2g")) return rc;
+        {
+            int rec = profile_begin("grid_update", s);
+            k_grid_update<<<box_blocks, kThreads, 0, s>>>(P, g);
+            profile_end(rec, s);
+        }
+        if (int rc = check_launch("bk_substep/grid_update")) return rc;
+        {
+            int rec = profile_begin("g2p_return", s);
+            k_g2p_return<<<blocks_for(p.n, 128), 128, 0, s>>>(P, *in, *out, *constants, g, *diagnostics, *flags);
+            profile_end(rec, s);
+        }
+        if (int rc = check_launch("bk_substep/g2p_return")) return rc;
+    }
+    return BK_OK;
+}
+
+int bk_surface_accumulate(const BkSurface* surface, float time_step, double* water_losses, double* heat_exchanges,
+                          void* stream) {
+    BK_REQUIRE(surface && water_losses && heat_exchanges, "bk_surface_accumulate: null argument");
+    if (surface->owner_count == 0) return BK_OK;
+    BK_REQUIRE(surface->owners && surface->owner_heat && surface->owner_loss, "bk_surface_accumulate: missing owners");
+    k_surface_accumulate<<<blocks_for(surface->owner_count, kThreads), kThreads, 0, S(stream)>>>(
+        surface->owner_count, surface->owners, surface->owner_heat, surface->owner_loss, (double)time_step,
+        water_losses, heat_exchanges);
+    return check_launch("bk_surface_accumulate");
+}
+
+int bk_materialize(const BkSubstepParams* params, const BkState* state, const BkConstants* constants,
+                   float* plastic_gradients, float* material_temperature, float* reference_density,
+                   float* yield_stress, float* viscosity, double* gas_pressure, double* saturation,
+                   float* particle_mass, void* stream) {
+    BK_REQUIRE(params && state && constants, "bk_materialize: null argument");
+    const BkSubstepParams& p = *params;
+    BK_REQUIRE(p.n >= 0 && p.pitch >= p.n, "bk_materialize: bad particle count/pitch");
+    if (p.n == 0) return BK_OK;
+    BK_REQUIRE(state->F != nullptr, "bk_materialize: missing F");
+    if (p.transport)
+        BK_REQUIRE(state->temperature && state->water && constants->dry_mass && constants->volume,
+                   "bk_materialize: missing transport arrays");
+    if (p.material == 1)
+        BK_REQUIRE(state->Fe && state->gelled && state->porosity && constants->viscosity_parameter &&
+                   (p.transport || state->material_temperature), "bk_materialize: missing Ding arrays");
+    if (p.gas && gas_pressure) BK_REQUIRE(state->gas_moles != nullptr, "bk_materialize: missing gas moles");
+    k_materialize<<<blocks_for(p.n, kThreads), kThreads, 0, S(stream)>>>(
+        to_params(p), *state, *constants, plastic_gradients, material_temperature, reference_density, yield_stress,
+        viscosity, gas_pressure, saturation, particle_mass);
+    return check_launch("bk_materialize");
+}
+
+}  // extern "C"

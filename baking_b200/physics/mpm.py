@@ -25,17 +25,26 @@ import torch
 from .. import _lib, arrays
 from ..geometry import ComputeSignedVolumes
 from ..geometry.mesh_tracking import ParticleMeshBinding
-from .grid import GridState, UpdateGrid
+from .grid import GridState
 from .materials.ding import DingMaterial
 from .materials.elastic import ElasticMaterial
 from .state import AllocateState, CreateParticleState
 from .thermal_water import AllocateTransportState, ThermalWaterTransport
-from .transfer import GridToParticle, ParticleToGrid
+
 
 
 class MpmSimulator:
     def __init__(self, tet_mesh, particle_samples, simulation_config, material_config,
-                 initial_velocity=(0.0, 0.0, 0.0), retain_history=False, ding_config=None, transport_config=None):
+                 initial_velocity=(0.0, 0.0, 0.0), retain_history=False, ding_config=None, transport_config=None,
+                 diagnostics="full"):
+        """``diagnostics="full"`` keeps every reference output array current after each substep;
+        ``"lean"`` writes only the primary state per substep and fills the derivable arrays
+        (plastic gradients, material temperature, density, yield stress, viscosity, gas pressure,
+        saturation, particle mass) when ``current_state`` is read. Per-particle return residuals
+        are kept only in "full" mode; both modes keep their per-substep maximum."""
+        if diagnostics not in ("full", "lean"):
+            raise ValueError("diagnostics must be 'full' or 'lean'")
+        self.diagnostics = diagnostics
         simulation_config.Validate(material_config)
         self.device = _lib.require_cuda(simulation_config.device_name)
         self.device_name = str(self.device)
@@ -59,12 +68,28 @@ class MpmSimulator:
         self.mesh_binding = ParticleMeshBinding(tet_mesh, particle_samples, self.device)
         self.transport = None
         self.error_flags = torch.zeros(2, dtype=torch.int32, device=self.device)
+        self.error_flags_ding_unused = torch.zeros(3, dtype=torch.int32, device=self.device)
+        self.error_flags_transport_unused = torch.zeros(2, dtype=torch.int32, device=self.device)
         if transport_config is not None and transport_config.enabled:
             transport_config.Validate(material_config)
             self.material.initial_temperature_k = transport_config.initial_temperature_k
             self.transport = ThermalWaterTransport(self, transport_config)
         self._buffers = {}
         self.Reset()
+
+    # --------------------------------------------------------------- state
+    @property
+    def current_state(self):
+        """The accepted state; its derivable reference fields are filled before it is returned."""
+        if self._stale:
+            self._engine.materialize(self._current, plastic=self.diagnostics == "lean")
+            self._stale = False
+        return self._current
+
+    @current_state.setter
+    def current_state(self, state):
+        self._current = state
+        self._stale = False
 
     # ------------------------------------------------------------ settling
     @property
@@ -121,6 +146,13 @@ class MpmSimulator:
                                "baking was not started. Increase the maximum duration or review tolerances/material.")
 
     # -------------------------------------------------------------- set-up
+    def SetGasSourceRates(self, rates):
+        """Per-particle gas source rate alpha_i (mol/(kg s)) in place of the scalar production parameter."""
+        rates = torch.as_tensor(np.asarray(rates, dtype=np.float32), device=self.device).reshape(-1)
+        if rates.shape[0] not in (1, self.particle_data.particle_count):
+            raise ValueError("gas source rates need one value or one per particle")
+        self.material.production_parameter = rates.contiguous()
+
     def Masses(self, state=None):
         state = self.current_state if state is None else state
         return state.transport_state.particle_masses if state.transport_state is not None else \
@@ -148,24 +180,33 @@ class MpmSimulator:
                                           for name in ("exposed", "contact", "particle_heat", "particle_loss")}
         return self._buffers["transport"]
 
-    def _allocate_like_current(self):
+    def _allocate_like_current(self, share_accumulators=True):
         n = self.particle_data.particle_count
         state = AllocateState(n, self.device)
         if isinstance(self.material, DingMaterial):
             self.material.InitializeState(state)
         if self.transport is not None:
             state.transport_state = AllocateTransportState(n, self.device)
+            current = self._current.transport_state
+            if share_accumulators:
+                # Loss/exchange only change for face-owning particles; both ping-pong states share them.
+                state.transport_state.water_losses = current.water_losses
+                state.transport_state.heat_exchanges = current.heat_exchanges
+            else:
+                state.transport_state.water_losses = current.water_losses.clone()
+                state.transport_state.heat_exchanges = current.heat_exchanges.clone()
         return state
 
     def Reset(self):
         if isinstance(self.material, DingMaterial):
             self.material.Reset()
-        self.current_state, self.particle_data = CreateParticleState(self.particle_samples, self.device,
-                                                                     self.initial_velocity, self.retain_history)
+        self._stale = False
+        self._current, self.particle_data = CreateParticleState(self.particle_samples, self.device,
+                                                                self.initial_velocity, self.retain_history)
         if isinstance(self.material, DingMaterial):
-            self.material.InitializeState(self.current_state)
+            self.material.InitializeState(self._current)
         if self.transport is not None:
-            self.transport.InitializeState(self.current_state)
+            self.transport.InitializeState(self._current)
         self.next_state = self._allocate_like_current()
         n = self.particle_data.particle_count
         self.grid_state = GridState(self.simulation_config, self.device)
@@ -196,57 +237,47 @@ class MpmSimulator:
         self.settling_diagnostics = dict(max_speed_m_s=0.0, max_strain_rate_per_s=0.0, max_plastic_rate_per_s=0.0)
         self.settling_metrics = torch.zeros(3, dtype=torch.float32, device=self.device)
         self.mesh_step_count = 0
-        self._first_failed_step = None
+        from .substep import SubstepEngine
+        self._engine = SubstepEngine(self)
         if getattr(self, "result_recorder", None) is not None:
             self.result_recorder.Reset()
 
     # ---------------------------------------------------------------- step
     def _substep(self, check):
-        sim = self.simulation_config
+        """One substep through the fused kernels; with ``check`` the device flags are read where the
+        reference synchronises (after the transport solve and after the return map)."""
+        from .substep import PHASE_MECHANICS, PHASE_TRANSPORT
         was_settling = self.IsSettling
-        original = self.current_state
-        state = original
-        if self.retain_history:
-            output = self._allocate_like_current()
+        original = self._current
+        output = self._allocate_like_current(share_accumulators=False) if self.retain_history else self.next_state
+        full = self.diagnostics == "full"
+        if check and self.transport is not None:
+            self._engine.run(original, output, was_settling, PHASE_TRANSPORT, full)
+            self.transport.CheckState()
+            self._engine.run(original, output, was_settling, PHASE_MECHANICS, full)
         else:
-            output = self.next_state
-        if self.transport is not None:
-            state = self.transport.Advance(state, sim.time_step, settling=was_settling,
-                                           output=output.transport_state, prepared_material=self._prepared,
-                                           check=check)
-        grid = self.grid_state
-        grid.Clear()
-        stress = self.kirchhoff_stresses
-        if isinstance(self.material, DingMaterial) and self.material.ding_config.gas_enabled:
-            self.material.LaunchGasStress(state, stress)
-            if check:
-                self.material.CheckState()
-        else:
-            self.material.ComputeStress(state, stress, self.error_flags)
-        if self.transport is not None:
-            stress = self.transport.AddWaterStress(state, stress, output=self._stress_water)
-        R = sim.grid_resolution
-        ParticleToGrid(state.particle_positions, state.particle_velocities, state.affine_velocities, stress,
-                       self.Masses(state), self.particle_data.reference_volumes, grid, sim.grid_origin,
-                       sim.grid_spacing, R, sim.time_step, self.error_flags)
-        UpdateGrid(grid, sim)
-        GridToParticle(state.particle_positions, state.deformation_gradients, grid, output.particle_positions,
-                       output.particle_velocities, output.affine_velocities, output.deformation_gradients,
-                       sim.grid_origin, sim.grid_spacing, R, sim.time_step, self.error_flags)
-        self.material.AdvanceState(state, output, sim.time_step)
-        if isinstance(self.material, DingMaterial) and check:
+            self._engine.run(original, output, was_settling, PHASE_TRANSPORT | PHASE_MECHANICS, full)
+        if check and isinstance(self.material, DingMaterial):
             self.material.CheckState()
         if self.transport is not None:
-            self.transport.FinishStep(state, output)
+            self._engine.accumulate_surface(output.transport_state)
         if self.retain_history:
             self.state_history.append(output)
-        self.current_state = output
+        self._current = output
         self.next_state = original
+        self._stale = True
+        if full:
+            self._engine.materialize(output, plastic=False)
+            self._stale = False
         self.step_count += 1
         if was_settling:
             self.UpdateSettling(original)
         if getattr(self, "result_recorder", None) is not None:
             self.result_recorder.Record()
+
+    def MaxReturnResiduals(self):
+        """(max return residual, max porosity residual) of the last substep, on the host."""
+        return tuple(self._engine.max_residuals.tolist())
 
     def Step(self):
         self._substep(check=True)
@@ -273,6 +304,22 @@ class MpmSimulator:
         if messages:
             raise RuntimeError(messages[0] + f" (flag raised within substeps {start + 1}..{self.step_count})")
         return self.CheckState()
+
+    def AdvanceUnchecked(self, step_count):
+        """Run substeps with no host synchronisation; flags stay on the device until CheckState/Advance."""
+        for _ in range(step_count):
+            self._substep(check=False)
+
+    def StepSummary(self):
+        """Device tensor (grid mass, particle kinetic energy) of the current state, float64."""
+        masses = self.Masses().double()
+        v = self.current_state.particle_velocities.double()
+        return torch.stack([self.grid_state.node_masses.double().sum(), 0.5 * (masses * (v * v).sum(1)).sum()])
+
+    def AlgorithmicBytes(self, kernel, active_nodes):
+        """Bytes one launch of ``kernel`` must move (each input and output array once), or None."""
+        from ..roofline import algorithmic_bytes
+        return algorithmic_bytes(kernel, self, active_nodes)
 
     def UpdateMesh(self, force_update=False):
         if force_update or self.mesh_step_count != self.step_count:
@@ -316,7 +363,9 @@ class MpmSimulator:
             ms = st.material_state
             if not bool(torch.isfinite(ms.elastic_gradients).all()) or not bool(torch.isfinite(ms.plastic_gradients).all()):
                 raise RuntimeError("nonfinite Ding internal state")
-            if float(ms.return_residuals.max()) > 1e-4:
+            worst = (float(ms.return_residuals.max()) if self.diagnostics == "full"
+                     else self.MaxReturnResiduals()[0])
+            if worst > 1e-4:
                 raise RuntimeError("Ding local return mapping did not converge")
         self.UpdateMesh()
         vertices = arrays.to_numpy(self.vertex_positions)

@@ -1,0 +1,281 @@
+"""Host side of the fused substep (``bk_substep``/``bk_materialize`` in the C ABI).
+
+Builds the pointer structs of ``include/baking_b200.h`` from a simulator's
+tensors and launches one substep, or the two halves of one (transport, then
+mechanics) when the caller checks the device flags in between.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from .. import _lib, arrays
+from .materials.ding import DingMaterial, ding_params
+from .thermal_water import scalar_params
+
+P = C.c_void_p
+
+
+class BkState(C.Structure):
+    _fields_ = [("x", P), ("v", P), ("C", P), ("F", P), ("Fe", P), ("tau", P), ("porosity", P), ("gelled", P),
+                ("material_temperature", P), ("temperature", P), ("water", P), ("gas_moles", P)]
+
+
+class BkConstants(C.Structure):
+    _fields_ = [("volume", P), ("mass", P), ("capacity", P), ("dry_mass", P), ("gas_rate", P),
+                ("gas_rate_per_particle", C.c_int32), ("viscosity_parameter", P), ("heat_parameter", P)]
+
+
+class BkGrid(C.Structure):
+    _fields_ = [("node_pm", P), ("node_v", P), ("fields", P * 7), ("node_dT_ratio", P), ("bounds", P)]
+
+
+class BkSurface(C.Structure):
+    _fields_ = [("vertex_count", C.c_int64), ("vertex_ids", P), ("binding_offsets", P), ("binding_particles", P),
+                ("binding_weights", P), ("binding_pitch", C.c_int64), ("reference_offsets", P),
+                ("vertex_pitch", C.c_int64), ("vertices", P), ("reference_vertices", P), ("owner_count", C.c_int64),
+                ("owners", P), ("owner_face_offsets", P), ("faces", P), ("owner_heat", P), ("owner_loss", P),
+                ("floor_height", C.c_float), ("contact_distance", C.c_float)]
+
+
+class BkDiagnostics(C.Structure):
+    _fields_ = [("plastic_gradients", P), ("return_residuals", P), ("porosity_residuals", P), ("max_residuals", P)]
+
+
+class BkFlags(C.Structure):
+    _fields_ = [("simulation", P), ("ding", P), ("transport", P)]
+
+
+class BkSubstepParams(C.Structure):
+    _fields_ = [("n", C.c_int64), ("pitch", C.c_int64), ("resolution", C.c_int32), ("boundary_cells", C.c_int32),
+                ("origin", C.c_float * 3), ("spacing", C.c_float), ("time_step", C.c_float),
+                ("gravity", C.c_float * 3), ("material", C.c_int32), ("ding", _lib.BkDingParams),
+                ("transport", C.c_int32), ("gas", C.c_int32), ("settling", C.c_int32), ("scalar", _lib.BkScalarParams),
+                ("conductivity", C.c_float), ("diffusivity", C.c_float), ("initial_saturation", C.c_float),
+                ("water_stress", C.c_float), ("gas_ambient_pressure", C.c_float), ("density", C.c_float),
+                ("elastic_modulus", C.c_float), ("cfl_limit", C.c_float), ("gas_peak", C.c_float),
+                ("gas_width", C.c_float)]
+
+
+PHASE_TRANSPORT = 1
+PHASE_MECHANICS = 2
+
+_SIGS = {
+    "bk_substep": [P] * 8 + [C.c_int32, P],
+    "bk_materialize": [P] * 11 + [P],
+    "bk_surface_accumulate": [P, C.c_float, P, P, P],
+}
+
+
+def _declare():
+    lib = _lib.load()
+    for name, argtypes in _SIGS.items():
+        fn = getattr(lib, name)
+        if fn.argtypes != argtypes:
+            fn.restype = C.c_int
+            fn.argtypes = argtypes
+    return lib
+
+
+def _p(t):
+    return None if t is None else t.data_ptr()
+
+
+def state_struct(state, material_is_ding, transport, gas):
+    s = BkState()
+    s.x, s.v = _p(state.particle_positions), _p(state.particle_velocities)
+    s.C, s.F = _p(state.affine_velocities), _p(state.deformation_gradients)
+    if material_is_ding:
+        m = state.material_state
+        s.Fe, s.tau = _p(m.elastic_gradients), _p(m.kirchhoff_stresses)
+        s.porosity, s.gelled, s.material_temperature = _p(m.porosities), _p(m.gelled), _p(m.temperatures)
+        if gas:
+            s.gas_moles = _p(m.gas_moles)
+    if transport:
+        t = state.transport_state
+        s.temperature, s.water = _p(t.temperatures), _p(t.water_masses)
+    return s
+
+
+class SubstepEngine:
+    """Launches the fused substep for one ``MpmSimulator``."""
+
+    def __init__(self, sim):
+        self.sim = sim
+        self.lib = _declare()
+        dev = sim.device
+        s = sim.simulation_config
+        R = s.grid_resolution
+        self.is_ding = isinstance(sim.material, DingMaterial)
+        self.transport = sim.transport is not None
+        self.gas = bool(self.is_ding and sim.material.ding_config.gas_enabled)
+        n = sim.particle_data.particle_count
+        self.n = n
+        self.pitch = arrays.layout_pitch(sim._current.deformation_gradients)
+        # The grid state's momentum/velocity nodes hold the last substep; the transport fields are
+        # zero between substeps. The kernels keep both invariants over the active node boxes.
+        sim.grid_state.Clear()
+        self.node_pm = sim.grid_state.node_pm
+        self.node_v = sim.grid_state.node_v
+        self.fields = [torch.zeros(R ** 3 if self.transport else 1, dtype=torch.float64, device=dev)
+                       for _ in range(7)]
+        self.node_dT_ratio = torch.zeros(R ** 3 if self.transport else 1, 2, dtype=torch.float64, device=dev)
+        empty = [2 ** 31 - 1] * 3 + [-2 ** 31] * 3
+        self.bounds = torch.tensor(empty + empty, dtype=torch.int32, device=dev)
+        self.grid = BkGrid()
+        self.grid.node_pm, self.grid.node_v = _p(self.node_pm), _p(self.node_v)
+        for k in range(7):
+            self.grid.fields[k] = _p(self.fields[k])
+        self.grid.node_dT_ratio, self.grid.bounds = _p(self.node_dT_ratio), _p(self.bounds)
+        self.max_residuals = torch.zeros(2, dtype=torch.float32, device=dev)
+        self.surface = BkSurface()
+        if self.transport:
+            self._build_surface()
+        self.flags = BkFlags()
+        self.flags.simulation = _p(sim.error_flags)
+        self.flags.ding = _p(sim.material.error_flags) if self.is_ding else _p(sim.error_flags_ding_unused)
+        self.flags.transport = _p(sim.transport.error_flags) if self.transport else _p(sim.error_flags_transport_unused)
+
+    # ------------------------------------------------------------------ setup
+    def _build_surface(self):
+        sim, dev = self.sim, self.sim.device
+        tr = sim.transport
+        faces = tr.faces.cpu().numpy()
+        owners = tr.owners.cpu().numpy()
+        order = np.argsort(owners, kind="stable")
+        owner_ids, starts = np.unique(owners[order], return_index=True)
+        offsets = np.concatenate([starts, [len(order)]]).astype(np.int32)
+        self._surface_tensors = dict(
+            vertex_ids=torch.as_tensor(np.unique(faces).astype(np.int32), device=dev),
+            owners=torch.as_tensor(owner_ids.astype(np.int32), device=dev),
+            owner_face_offsets=torch.as_tensor(offsets, device=dev),
+            faces=torch.as_tensor(np.ascontiguousarray(faces[order]).astype(np.int32), device=dev),
+            owner_heat=torch.zeros(len(owner_ids), dtype=torch.float64, device=dev),
+            owner_loss=torch.zeros(len(owner_ids), dtype=torch.float64, device=dev))
+        t = self._surface_tensors
+        mb = sim.mesh_binding
+        sf = self.surface
+        sf.vertex_count = int(t["vertex_ids"].shape[0])
+        sf.vertex_ids = _p(t["vertex_ids"])
+        sf.binding_offsets = _p(mb.binding_offsets)
+        sf.binding_particles = _p(mb.binding_particles)
+        sf.binding_weights = _p(mb.binding_weights)
+        sf.binding_pitch = arrays.layout_pitch(mb.reference_offsets)
+        sf.reference_offsets = _p(mb.reference_offsets)
+        verts = sim.surface_vertices_buffer()
+        sf.vertex_pitch = arrays.layout_pitch(verts)
+        if arrays.layout_pitch(mb.reference_vertices) != sf.vertex_pitch:
+            raise RuntimeError("vertex arrays must share a plane pitch")
+        sf.vertices = _p(verts)
+        sf.reference_vertices = _p(mb.reference_vertices)
+        sf.owner_count = int(t["owners"].shape[0])
+        sf.owners, sf.owner_face_offsets, sf.faces = _p(t["owners"]), _p(t["owner_face_offsets"]), _p(t["faces"])
+        sf.owner_heat, sf.owner_loss = _p(t["owner_heat"]), _p(t["owner_loss"])
+        ids = t["vertex_ids"].cpu().numpy()
+        offs = mb.tables.binding_offsets
+        self.surface_bindings = int((offs[ids + 1] - offs[ids]).sum())
+        self.owned_faces = int(len(faces))
+        s = sim.simulation_config
+        sf.floor_height = s.grid_origin[1] + (s.boundary_cells - 1) * s.grid_spacing
+        sf.contact_distance = tr.config.contact_distance
+
+    def params(self, settling):
+        sim = self.sim
+        s = sim.simulation_config
+        mc = sim.material.material_config
+        p = BkSubstepParams()
+        p.n, p.pitch = self.n, self.pitch
+        p.resolution, p.boundary_cells = s.grid_resolution, s.boundary_cells
+        p.origin[:] = list(s.grid_origin)
+        p.spacing, p.time_step = s.grid_spacing, s.time_step
+        p.gravity[:] = list(s.gravity)
+        p.material = 1 if self.is_ding else 0
+        if self.is_ding:
+            p.ding = ding_params(mc, sim.material.ding_config, s.time_step)
+        else:
+            p.ding.shear_modulus, p.ding.lame_lambda = mc.shear_modulus, mc.lame_lambda
+        p.transport, p.gas, p.settling = int(self.transport), int(self.gas), int(settling)
+        p.density = mc.density
+        p.elastic_modulus = mc.lame_lambda + 2 * mc.shear_modulus
+        p.cfl_limit = s.cfl_limit
+        if self.transport:
+            c = sim.transport.config
+            p.scalar = scalar_params(c, s, settling)
+            p.conductivity = 0.0 if settling else c.conductivity
+            p.diffusivity = 0.0 if settling else c.water_diffusivity
+            p.initial_saturation = c.initial_saturation
+            p.water_stress = c.water_stress if c.water_enabled else 0.0
+        if self.gas:
+            d = sim.material.ding_config
+            p.gas_ambient_pressure = d.gas_ambient_pressure_pa
+            p.gas_peak, p.gas_width = d.gas_reaction_temperature_k, d.gas_reaction_width_k
+        return p
+
+    def constants(self, settling):
+        sim = self.sim
+        c = BkConstants()
+        c.volume = _p(sim.particle_data.reference_volumes)
+        c.mass = _p(sim.particle_data.particle_masses)
+        if self.transport:
+            c.capacity, c.dry_mass = _p(sim.transport.capacities), _p(sim.transport.dry_masses)
+            c.heat_parameter = _p(sim.transport._zero_parameter if settling else sim.transport.heat_transfer_parameter)
+        if self.is_ding:
+            c.viscosity_parameter = _p(sim.material.viscosity_parameter)
+            rates = sim.material.production_parameter
+            c.gas_rate = _p(rates)
+            c.gas_rate_per_particle = int(rates.shape[0] == self.n and self.n > 1)
+        return c
+
+    # ---------------------------------------------------------------- launch
+    def run(self, state_in, state_out, settling, phases, full_diagnostics):
+        p = self.params(settling)
+        cst = self.constants(settling)
+        sin = state_struct(state_in, self.is_ding, self.transport, self.gas)
+        sout = state_struct(state_out, self.is_ding, self.transport, self.gas)
+        diag = BkDiagnostics()
+        diag.max_residuals = _p(self.max_residuals)
+        if full_diagnostics and self.is_ding:
+            m = state_out.material_state
+            diag.plastic_gradients = _p(m.plastic_gradients)
+            diag.return_residuals = _p(m.return_residuals)
+            diag.porosity_residuals = _p(m.porosity_residuals)
+        timer = _lib.KernelTimer.active
+        stream = _lib.stream_handle()
+        if timer is not None:
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+        rc = self.lib.bk_substep(C.byref(p), C.byref(sin), C.byref(sout), C.byref(cst), C.byref(self.grid),
+                                 C.byref(self.surface), C.byref(diag), C.byref(self.flags), int(phases), stream)
+        if timer is not None:
+            end.record()
+            timer.add(f"bk_substep[{phases}]", start, end)
+        if rc != 0:
+            raise RuntimeError(f"bk_substep failed ({rc}): {self.lib.bk_last_error().decode(errors='replace')}")
+
+    def accumulate_surface(self, transport_state):
+        if not self.transport or self.surface.owner_count == 0:
+            return
+        _lib.call_raw(self.lib.bk_surface_accumulate, "bk_surface_accumulate", C.byref(self.surface),
+                      self.sim.simulation_config.time_step, _p(transport_state.water_losses),
+                      _p(transport_state.heat_exchanges), _lib.stream_handle())
+
+    def materialize(self, state, plastic=True):
+        """Fill the derivable reference fields of ``state`` from its primary arrays."""
+        p = self.params(False)
+        cst = self.constants(False)
+        s = state_struct(state, self.is_ding, self.transport, self.gas)
+        m, t = state.material_state, state.transport_state
+        args = [None] * 8
+        if self.is_ding:
+            args[0] = _p(m.plastic_gradients) if plastic else None
+            args[1] = _p(m.temperatures) if self.transport else None
+            args[2] = _p(m.reference_densities)
+            args[3], args[4] = _p(m.yield_stresses), _p(m.viscosities)
+            args[5] = _p(m.gas_pressures) if self.gas else None
+        if self.transport:
+            args[6], args[7] = _p(t.saturations), _p(t.particle_masses)
+        _lib.call_raw(self.lib.bk_materialize, "bk_materialize", C.byref(p), C.byref(s), C.byref(cst), *args,
+                      _lib.stream_handle())

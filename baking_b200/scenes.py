@@ -1,0 +1,166 @@
+"""Seeded synthetic baking scenes (no dataset is involved; all inputs are generated).
+
+``box_loaf``: a box of dough resting 0.1 mm above the floor wall of a unit-cube
+grid, filled with jittered particles (equal reference volumes) emitted cell by
+cell in Morton order of their grid cell, and a voxel tet mesh (six tets per
+voxel) whose boundary faces carry the transport's surface terms. Particles are
+assigned to tets by point location, so every tet owns particles.
+
+``jittered_sphere``: a ball of dough sampled with k x k x k jittered points per
+grid cell inside the ball, meshed with the voxels that the ball covers.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, replace
+
+import numpy as np
+
+from .config import DingConfig, MaterialConfig, SimulationConfig, TransportConfig
+from .geometry import ParticleSamples, VoxelTetMesh
+
+
+@dataclass
+class Scene:
+    name: str
+    tet_mesh: object
+    samples: ParticleSamples
+    simulation: SimulationConfig
+    material: MaterialConfig
+    ding: DingConfig
+    transport: TransportConfig
+    gas_source_rates: np.ndarray | None = None
+    initial_velocity: tuple = (0.0, 0.0, 0.0)
+
+    @property
+    def particle_count(self):
+        return len(self.samples.particle_positions)
+
+
+def _morton3(ix, iy, iz):
+    def spread(v):
+        v = v.astype(np.uint64) & np.uint64(0x1FFFFF)
+        v = (v | (v << np.uint64(32))) & np.uint64(0x1F00000000FFFF)
+        v = (v | (v << np.uint64(16))) & np.uint64(0x1F0000FF0000FF)
+        v = (v | (v << np.uint64(8))) & np.uint64(0x100F00F00F00F00F)
+        v = (v | (v << np.uint64(4))) & np.uint64(0x10C30C30C30C30C3)
+        v = (v | (v << np.uint64(2))) & np.uint64(0x1249249249249249)
+        return v
+    return spread(ix) | (spread(iy) << np.uint64(1)) | (spread(iz) << np.uint64(2))
+
+
+def _kuhn_index(local):
+    """Index (in VoxelTetMesh's tet order) of the Kuhn tet containing unit-voxel coordinates ``local``."""
+    from itertools import permutations
+    order = np.argsort(-local, axis=1, kind="stable")          # axes by descending coordinate
+    table = {p: k for k, p in enumerate(permutations(range(3)))}
+    codes = order[:, 0] * 9 + order[:, 1] * 3 + order[:, 2]
+    lut = np.zeros(27, dtype=np.int64)
+    for p, k in table.items():
+        lut[p[0] * 9 + p[1] * 3 + p[2]] = k
+    return lut[codes]
+
+
+def _locate(points, origin, voxel, shape):
+    rel = (points - origin) / voxel
+    cell = np.clip(np.floor(rel).astype(np.int64), 0, np.asarray(shape) - 1)
+    voxel_id = np.ravel_multi_index(cell.T, shape)
+    return voxel_id * 6 + _kuhn_index(rel - cell)
+
+
+def box_loaf(resolution=128, particle_count=1_000_000, seed=0, size=(0.4, 0.15, 0.2), gas=True,
+             time_step=5e-5, gas_rate_max=1e-3):
+    """Box loaf (x length, y height, z width) on the floor, ``particle_count`` jittered particles."""
+    dx = 1.0 / resolution
+    voxel = 2 * dx
+    nvox = np.maximum(1, np.round(np.asarray(size) / voxel).astype(np.int64))
+    extent = nvox * voxel
+    boundary_cells = 3
+    floor = (boundary_cells - 1) * dx
+    origin = np.array([0.5 - extent[0] / 2, floor + 1e-4, 0.5 - extent[2] / 2])
+    origin[[0, 2]] = np.round(origin[[0, 2]] / dx) * dx
+    mesh = VoxelTetMesh(np.ones(tuple(nvox), dtype=bool), origin, voxel)
+    # Cells of size dx inside the box, visited in Morton order; counts as even as possible.
+    ncell = nvox * 2
+    cells = np.stack(np.meshgrid(*[np.arange(c) for c in ncell], indexing="ij"), -1).reshape(-1, 3)
+    cells = cells[np.argsort(_morton3(cells[:, 0], cells[:, 1], cells[:, 2]), kind="stable")]
+    per = np.full(len(cells), particle_count // len(cells), dtype=np.int64)
+    per[: particle_count - per.sum()] += 1
+    rng = np.random.default_rng(seed)
+    corner = np.repeat(cells, per, axis=0).astype(np.float64)
+    points = origin + (corner + rng.random((particle_count, 3))) * dx
+    source_tets = _locate(points, origin, voxel, tuple(nvox))
+    if np.any(np.bincount(source_tets, minlength=len(mesh.tet_indices)) == 0):
+        raise ValueError("a tet received no particle; use more particles")
+    density = 1000.0
+    volumes = np.full(particle_count, float(np.prod(extent)) / particle_count)
+    samples = ParticleSamples(points, volumes, density * volumes, source_tets)
+    sim = replace(SimulationConfig(), grid_resolution=resolution, grid_spacing=dx, time_step=time_step,
+                  gravity=(0.0, -9.8, 0.0), boundary_cells=boundary_cells, device_name="cuda:0")
+    material = MaterialConfig(density=density, model="ding2019")
+    ding = DingConfig(porosity=0.2 if gas else 0.0, temperature_enabled=True, gas_enabled=gas)
+    transport = TransportConfig(enabled=True)
+    rates = rng.uniform(0.0, gas_rate_max, particle_count).astype(np.float32) if gas else None
+    return Scene("box_loaf", mesh, samples, sim, material, ding, transport, rates)
+
+
+def jittered_sphere(resolution=64, per_axis=2, radius=0.1, center=(0.5, 0.5, 0.3), seed=0, time_step=1e-4):
+    """Sphere of dough, ``per_axis``^3 jittered particles per cell, Ding defaults, transport on, gas off."""
+    dx = 1.0 / resolution
+    sub = dx / per_axis
+    lo = np.floor((np.asarray(center) - radius) / dx).astype(int)
+    hi = np.ceil((np.asarray(center) + radius) / dx).astype(int)
+    axes = [np.arange(lo[a] * per_axis, hi[a] * per_axis) for a in range(3)]
+    grid = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, 3)
+    rng = np.random.default_rng(seed)
+    points = (grid + 0.5 + rng.uniform(-0.5, 0.5, grid.shape)) * sub
+    points = points[np.linalg.norm(points - np.asarray(center), axis=1) <= radius]
+    cell = np.floor(points / dx).astype(np.int64)
+    order = np.argsort(_morton3(cell[:, 0], cell[:, 1], cell[:, 2]), kind="stable")
+    points = points[order]
+    # Mesh: the voxels (size dx) that hold particles.
+    vox_lo = np.floor(points.min(axis=0) / dx).astype(int)
+    vcell = np.floor(points / dx).astype(np.int64) - vox_lo
+    shape = tuple(vcell.max(axis=0) + 1)
+    occupied = np.zeros(shape, dtype=bool)
+    occupied[tuple(vcell.T)] = True
+    mesh = VoxelTetMesh(occupied, vox_lo * dx, dx)
+    # Tet ids of VoxelTetMesh follow the occupied voxels in x-major order.
+    voxel_rank = np.cumsum(occupied.reshape(-1)) - 1
+    local = points / dx - np.floor(points / dx)
+    source_tets = voxel_rank[np.ravel_multi_index(vcell.T, shape)] * 6 + _kuhn_index(local)
+    counts = np.bincount(source_tets, minlength=len(mesh.tet_indices))
+    keep_tets = counts > 0
+    if not keep_tets.all():
+        # Drop tets without particles (reference binding needs every tet sampled).
+        remap = np.cumsum(keep_tets) - 1
+        from .geometry import ValidateTetMesh
+        mesh = ValidateTetMesh(mesh.vertex_positions, mesh.tet_indices[keep_tets])
+        source_tets = remap[source_tets]
+        used = np.unique(mesh.tet_indices)
+        vmap = np.full(len(mesh.vertex_positions), -1)
+        vmap[used] = np.arange(len(used))
+        mesh = ValidateTetMesh(mesh.vertex_positions[used], vmap[mesh.tet_indices])
+    density = 1000.0
+    volumes = np.full(len(points), sub ** 3)
+    samples = ParticleSamples(points, volumes, density * volumes, source_tets)
+    sim = replace(SimulationConfig(), grid_resolution=resolution, grid_spacing=dx, time_step=time_step,
+                  gravity=(0.0, -9.8, 0.0), device_name="cuda:0")
+    return Scene("jittered_sphere", mesh, samples, sim, MaterialConfig(model="ding2019"), DingConfig(),
+                 TransportConfig(enabled=True, initial_temperature_k=298.15, oven_temperature_k=453.15,
+                                 tray_temperature_k=453.15, initial_saturation=0.4))
+
+
+def make_simulator(scene, engine="cuda", **kwargs):
+    """Build the device ``MpmSimulator`` (or, for tests, another engine class) for a scene."""
+    if engine == "cuda":
+        from .physics.mpm import MpmSimulator
+        cls = MpmSimulator
+    else:
+        cls = engine
+    sim_cfg = scene.simulation if engine == "cuda" else replace(scene.simulation, device_name="cpu")
+    sim = cls(scene.tet_mesh, scene.samples, sim_cfg, scene.material, scene.initial_velocity,
+              ding_config=scene.ding, transport_config=scene.transport, **kwargs)
+    if scene.gas_source_rates is not None:
+        sim.SetGasSourceRates(scene.gas_source_rates)
+    return sim

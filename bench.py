@@ -1,0 +1,304 @@
+"""Throughput of the MLS-MPM baking substep (particle-substeps/s) on B200s.
+
+Workload: the 1,000,000-particle box loaf on a 128^3 grid (Ding viscoplastic dough
+with temperature dependence, coupled gas porosity, thermal-water transport, a
+per-particle gas source rate alpha_i ~ U[0, 1e-3], gravity, dt = 5e-5). One
+bench "step" is one substep of every particle. Inputs are seeded synthetic data
+larger than L2, generated on the host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs under torchrun: every rank simulates its own copy of the loaf (the
+substep has no exchange between independent bodies), ranks are timed on the
+device, and the slowest rank's time sets the whole-job throughput.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-substeps/s at 1M particles (plain vs surrogate vs fwd+bwd) on 1 B200"
+UNIT = "particle-substeps/s"
+
+# Algorithmic HBM bytes: every required per-particle state array read once and
+# written once per substep at its stored precision (gas mode), plus the grid
+# traffic of each active node. Derivation in DESIGN.md.
+BYTES_PER_PARTICLE = 404
+BYTES_PER_ACTIVE_NODE = 232
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--particles", type=int, default=1_000_000)
+    p.add_argument("--resolution", type=int, default=128)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = max(smax, float(parts[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[4:8]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    path = ROOT / "profiles" / "traffic.json"
+    if path.exists():
+        return json.loads(path.read_text())
+    return {}
+
+
+def active_node_count(sim):
+    import torch
+    return int((sim.grid_state.node_masses > 0).sum().item())
+
+
+def cpu_baseline_sample(scene, seconds=20.0, max_steps=50):
+    """The CPU oracle on the same scene, all host threads, for about ``seconds``."""
+    from oracle import ora
+    from oracle.sim import OracleSimulator
+    from baking_b200.scenes import make_simulator
+    threads = os.cpu_count() or 1
+    ora.set_threads(threads)
+    sim = make_simulator(scene, engine=OracleSimulator)
+    sim.Step()  # warm-up (allocations, page faults)
+    steps, start = 0, time.perf_counter()
+    while steps < max_steps:
+        sim.Step()
+        steps += 1
+        if time.perf_counter() - start > seconds:
+            break
+    elapsed = time.perf_counter() - start
+    n = scene.particle_count
+    return {"value": n * steps / elapsed, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} substeps of the {n}-particle loaf after 1 warm-up substep ({elapsed:.1f} s)"}
+
+
+def run_reference(args):
+    """Reference arm: the CPU oracle of the reference substep, all host threads."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from baking_b200.scenes import box_loaf
+    scene = box_loaf(args.resolution, args.particles)
+    from oracle import ora
+    from oracle.sim import OracleSimulator
+    from baking_b200.scenes import make_simulator
+    threads = os.cpu_count() or 1
+    ora.set_threads(threads)
+    sim = make_simulator(scene, engine=OracleSimulator)
+    for _ in range(min(args.warmup, 1)):
+        sim.Step()
+    budget = 90.0
+    steps, start = 0, time.perf_counter()
+    while steps < args.steps:
+        sim.Step()
+        steps += 1
+        if time.perf_counter() - start > budget:
+            break
+    elapsed = time.perf_counter() - start
+    value = scene.particle_count * steps / elapsed
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * elapsed / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"box loaf, {scene.particle_count} particles, {args.resolution}^3 grid, "
+                                   "Ding+gas+thermal-water, dt=5e-5", "inputs": "larger than L2"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{steps} substeps of the full loaf (bounded to ~{budget:.0f} s)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    from baking_b200 import _lib
+    from baking_b200.scenes import box_loaf, make_simulator
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    scene = box_loaf(args.resolution, args.particles, seed=rank)
+    sim = make_simulator(scene, diagnostics="lean")
+    n = scene.particle_count
+    for _ in range(args.warmup):
+        sim.AdvanceUnchecked(1)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    stream = torch.cuda.current_stream()
+    kernel_events = _lib.KernelTimer()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        with kernel_events:
+            start.record(stream)
+            sim.AdvanceUnchecked(args.steps)
+            end.record(stream)
+        torch.cuda.synchronize()
+    elapsed = start.elapsed_time(end) / 1e3
+    if dist:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    sim.CheckState()
+    per_kernel = kernel_events.summary()
+    active = active_node_count(sim)
+
+    # End to end through the public API: pinned host inputs (the per-particle gas source rates) uploaded
+    # every substep, the substep, and the step's result (grid mass, kinetic energy) read back to the host.
+    host_rates = torch.from_numpy(scene.gas_source_rates).pin_memory()
+    device_rates = sim.material.production_parameter
+    e2e_steps = max(1, min(args.steps, 100))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    wall0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        device_rates.copy_(host_rates, non_blocking=True)
+        sim.AdvanceUnchecked(1)
+        result = sim.StepSummary().cpu()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_elapsed = max(e0.elapsed_time(e1) / 1e3, time.perf_counter() - wall0)
+    if dist:
+        t = torch.tensor([e2e_elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_elapsed = float(t.item())
+    del result
+
+    peak, peak_kind = load_peaks()
+    traffic = load_traffic()
+    dominant = max(per_kernel.items(), key=lambda kv: kv[1]["total_s"]) if per_kernel else None
+    roofline = None
+    if dominant:
+        name, info = dominant
+        algo = sim.AlgorithmicBytes(name, active)
+        achieved = algo / info["mean_s"] / 1e9 if algo else None
+        roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
+                    "traffic": traffic.get(name), "launches": info["count"], "mean_us": info["mean_s"] * 1e6,
+                    "share": info["total_s"] / sum(v["total_s"] for v in per_kernel.values())}
+    step_bytes = n * BYTES_PER_PARTICLE + active * BYTES_PER_ACTIVE_NODE
+    value = world * n * args.steps / elapsed
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"box loaf, {n} particles per GPU, {args.resolution}^3 grid, Ding+gas+"
+                                   "thermal-water, per-particle gas source, dt=5e-5",
+                       "particles": n, "resolution": args.resolution, "active_nodes": active,
+                       "inputs": "larger than L2 (about 0.6 GB of particle state per GPU)",
+                       "parallelism": f"replicas{world}"},
+            "roofline": roofline,
+            "step_roofline": {"bytes_per_step": step_bytes, "achieved_gbs": step_bytes * args.steps / elapsed / 1e9,
+                              "peak": peak, "frac": step_bytes * args.steps / elapsed / 1e9 / peak},
+            "kernels": {k: {"launches": v["count"], "mean_us": v["mean_s"] * 1e6} for k, v in per_kernel.items()},
+            "gpu_launches": int(sum(v["count"] for v in per_kernel.values())),
+            "e2e": {"value": world * n * e2e_steps / e2e_elapsed, "unit": UNIT,
+                    "h2d_bytes_per_step": int(host_rates.numel() * 4), "d2h_bytes_per_step": int(result_bytes()),
+                    "steps": e2e_steps},
+            "clocks": clocks.summary()}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(scene)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def result_bytes():
+    return 2 * 8
+
+
+if __name__ == "__main__":
+    main()

@@ -178,6 +178,117 @@ BK_API int bk_solve_porosity(int64_t n, const float *q, const float *p, const fl
 /* Device evaluation of porosity_coefficient (physics/materials/ding.py:68-74) per entry. */
 BK_API int bk_porosity_coefficient(int64_t n, const float *porosity, float *coefficient, void *stream);
 
+/* ---- fused substep (the simulator's hot path) ----------------------------- */
+
+/* One particle state (ping-pong buffer). Planes share BkSubstepParams.pitch. */
+typedef struct BkState {
+    float *x, *v, *C, *F;          /* 3, 3, 9, 9 planes */
+    float *Fe, *tau;               /* Ding elastic gradient and Kirchhoff stress (9 planes); NULL if neo-Hookean */
+    float *porosity;               /* Ding */
+    int32_t *gelled;               /* Ding */
+    float *material_temperature;   /* Ding temperature when transport is off (read) */
+    double *temperature, *water;   /* transport; NULL when off */
+    double *gas_moles;             /* gas mode; NULL when off */
+} BkState;
+
+/* Per-particle constants and device-resident scalar parameters. */
+typedef struct BkConstants {
+    const float *volume;           /* reference volume V0 */
+    const float *mass;             /* particle mass (used when transport is off) */
+    const double *capacity;        /* rho c V0 (transport) */
+    const double *dry_mass;        /* (rho - rho_w s0) V0 (transport) */
+    const float *gas_rate;         /* alpha: 1 value, or one per particle */
+    int32_t gas_rate_per_particle;
+    const float *viscosity_parameter;  /* 1 value */
+    const float *heat_parameter;       /* 1 value (zero while settling) */
+} BkConstants;
+
+/* Dense R^3 grid; only the active box of the current particles is touched per substep. */
+typedef struct BkGrid {
+    float *node_pm;                /* R^3 float4 (px, py, pz, m); the last substep's values, zero elsewhere */
+    float *node_v;                 /* R^3 float4 (vx, vy, vz, 0); the last substep's values, zero elsewhere */
+    double *fields[7];             /* volumes, capacities, energy, water, heat, loss, exchange -- zero between substeps */
+    double *node_dT_ratio;         /* R^3 x 2 doubles: temperature change, water change / node water */
+    int32_t *bounds;               /* 12 ints (device): lo[3], hi[3] of the active node box being built,
+                                      then lo[3], hi[3] of the last substep's box. Start as
+                                      {INT_MAX x3, INT_MIN x3, INT_MAX x3, INT_MIN x3} on a zero grid. */
+} BkGrid;
+
+/* Surface terms: the boundary-face vertices and the particles that own boundary faces. */
+typedef struct BkSurface {
+    int64_t vertex_count;          /* surface vertices to rebuild */
+    const int32_t *vertex_ids;     /* mesh vertex index of each */
+    const int32_t *binding_offsets;/* mesh vertex -> binding range (CSR over all mesh vertices) */
+    const int32_t *binding_particles;
+    const float *binding_weights;
+    int64_t binding_pitch;
+    const float *reference_offsets;/* 3 planes of binding_pitch */
+    int64_t vertex_pitch;
+    float *vertices;               /* 3 planes of vertex_pitch (surface entries rebuilt) */
+    const float *reference_vertices;   /* 3 planes of vertex_pitch (used for unbound vertices) */
+    int64_t owner_count;           /* particles that own boundary faces */
+    const int32_t *owners;
+    const int32_t *owner_face_offsets; /* owner -> face range */
+    const int32_t *faces;          /* 3 vertex ids per face, grouped by owner */
+    double *owner_heat, *owner_loss;   /* per owner, this substep */
+    float floor_height, contact_distance;
+} BkSurface;
+
+/* Optional full per-particle outputs of the reference kernels (NULL pointers are skipped). */
+typedef struct BkDiagnostics {
+    float *plastic_gradients;      /* Fp, 9 planes */
+    float *return_residuals, *porosity_residuals;
+    float *max_residuals;          /* device [2]: max return residual, max porosity residual (always) */
+} BkDiagnostics;
+
+typedef struct BkFlags {
+    int32_t *simulation;           /* [2]: J, stencil (physics/mpm.py:145) */
+    int32_t *ding;                 /* [3]: porosity domain, porosity solve, gas CFL (ding.py:232) */
+    int32_t *transport;            /* [2]: heat bound, water bound (thermal_water.py:279) */
+} BkFlags;
+
+typedef struct BkSubstepParams {
+    int64_t n, pitch;
+    int32_t resolution, boundary_cells;
+    float origin[3], spacing, time_step, gravity[3];
+    int32_t material;              /* 0 neo-Hookean, 1 Ding */
+    BkDingParams ding;
+    int32_t transport, gas, settling;
+    BkScalarParams scalar;
+    float conductivity, diffusivity, initial_saturation, water_stress;
+    float gas_ambient_pressure, density, elastic_modulus, cfl_limit, gas_peak, gas_width;
+} BkSubstepParams;
+
+#define BK_PHASE_TRANSPORT 1       /* surface terms, scalar P2G, diffusion */
+#define BK_PHASE_MECHANICS 2       /* scalar G2P + gas/water stress + P2G, grid update, G2P + return map */
+
+/* The fused substep of physics/mpm.py:163-225: reads `in`, writes `out`, uses `grid` as scratch. */
+BK_API int bk_substep(const BkSubstepParams *params, const BkState *in, BkState *out, const BkConstants *constants,
+                      BkGrid *grid, BkSurface *surface, BkDiagnostics *diagnostics, BkFlags *flags,
+                      int32_t phases, void *stream);
+
+/* Per-kernel timing of the fused entry points with CUDA events on the launching stream.
+   bk_profile_start clears old records and starts recording; bk_profile_stop stops;
+   bk_profile_report waits for the events and writes, per kernel name (name_capacity bytes each),
+   the total milliseconds and launch count. */
+BK_API int bk_profile_start(void);
+BK_API int bk_profile_stop(void);
+BK_API int bk_profile_report(int32_t max_kernels, char *names, int32_t name_capacity, double *total_ms,
+                             int32_t *counts, int32_t *kernel_count);
+
+/* Water-loss and heat-exchange accumulators of the face-owning particles after an accepted substep
+   (physics/thermal_water.py:225-226): += time_step * the owner rates bk_substep stored in `surface`. */
+BK_API int bk_surface_accumulate(const BkSurface *surface, float time_step, double *water_losses,
+                                 double *heat_exchanges, void *stream);
+
+/* Recompute the derivable reference outputs of a state from its primary arrays: plastic gradients
+   Fp = Fe^-1 F, material temperature, reference density, yield stress, viscosity, gas pressure,
+   saturation and particle mass (any output pointer may be NULL). */
+BK_API int bk_materialize(const BkSubstepParams *params, const BkState *state, const BkConstants *constants,
+                          float *plastic_gradients, float *material_temperature, float *reference_density,
+                          float *yield_stress, float *viscosity, double *gas_pressure, double *saturation,
+                          float *particle_mass, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

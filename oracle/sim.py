@@ -336,6 +336,9 @@ class OracleSimulator:
         self.Reset()
 
     # ------------------------------------------------------------ helpers
+    def SetGasSourceRates(self, rates):
+        self.material.production_parameter = np.ascontiguousarray(np.asarray(rates, np.float32).reshape(-1))
+
     def mesh_binding_reconstruct(self, state, out):
         ref, offsets, particles, weights, offs = self._binding_arrays
         ora.reconstruct_mesh_vertices(state.particle_positions, state.deformation_gradients, ref, offsets,

@@ -64,3 +64,33 @@ def test_transport_scene_matches_oracle():
     ref.Advance(10)
     dev.Advance(10)
     _compare_state(ref, dev, ref.simulation_config.grid_spacing, 10)
+
+
+@pytest.mark.parametrize("diagnostics", ["lean", "full"])
+def test_box_loaf_matches_oracle(diagnostics):
+    """The benchmark workload at reduced size (48^3 grid, 20k particles), both diagnostics modes."""
+    from baking_b200.scenes import box_loaf, make_simulator
+    from oracle.sim import OracleSimulator
+    scene = box_loaf(resolution=48, particle_count=20000, seed=3, time_step=1e-4)
+    ref = make_simulator(scene, engine=OracleSimulator)
+    dev = make_simulator(scene, diagnostics=diagnostics)
+    for _ in range(15):
+        ref.Step()
+    dev.Advance(15)
+    dx = scene.simulation.grid_spacing
+    _compare_state(ref, dev, dx, 15)
+    a, b = ref.current_state, dev.current_state
+    for name in ("temperatures", "yield_stresses", "viscosities", "reference_densities"):
+        np.testing.assert_allclose(to_np(getattr(b.material_state, name)), getattr(a.material_state, name), rtol=1e-4,
+                                   err_msg=name)
+    np.testing.assert_allclose(to_np(b.material_state.plastic_gradients), a.material_state.plastic_gradients,
+                               rtol=1e-4, atol=1e-4)
+    np.testing.assert_allclose(to_np(b.material_state.gas_pressures), a.material_state.gas_pressures, rtol=1e-4)
+    np.testing.assert_allclose(to_np(b.transport_state.saturations), a.transport_state.saturations, rtol=1e-4)
+    np.testing.assert_allclose(to_np(b.transport_state.particle_masses), a.transport_state.particle_masses, rtol=1e-6)
+    np.testing.assert_allclose(to_np(b.transport_state.water_losses), a.transport_state.water_losses, rtol=1e-4,
+                               atol=1e-15)
+    np.testing.assert_allclose(to_np(b.transport_state.heat_exchanges), a.transport_state.heat_exchanges, rtol=1e-4,
+                               atol=1e-12)
+    np.testing.assert_allclose(to_np(dev.grid_state.node_masses), ref.grid_masses, rtol=1e-5,
+                               atol=1e-5 * ref.grid_masses.max())
