@@ -7,6 +7,7 @@ missing, the first call raises.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import torch
@@ -70,6 +71,10 @@ def load():
     global _lib
     if _lib is not None:
         return _lib
+    override = os.environ.get("BAKING_B200_LIBRARY")
+    if override:
+        # An alternative build of the same sources (for example one compiled with other flags).
+        return _bind(C.CDLL(override))
     from . import build as _build
     try:
         if _build.needs_build():
@@ -79,7 +84,11 @@ def load():
             raise
     if not LIBRARY.exists():
         raise RuntimeError(f"{LIBRARY} is missing; run `python -m baking_b200.build` (needs nvcc)")
-    lib = C.CDLL(str(LIBRARY))
+    return _bind(C.CDLL(str(LIBRARY)))
+
+
+def _bind(lib):
+    global _lib
     lib.bk_version.restype = C.c_int
     lib.bk_version.argtypes = []
     lib.bk_last_error.restype = C.c_char_p

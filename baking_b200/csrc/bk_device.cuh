@@ -150,6 +150,247 @@ BK_DEV void svd3(const M3d& A, M3d& U, double s[3], M3d& V) {
     for (int e = 0; e < 9; ++e) V.m[e] = v[e];
 }
 
+// Fast 3x3 SVD with the same float64 accuracy as svd3: a float32 cyclic Jacobi eigen-solve of
+// A^T A (four sweeps, Jacobi 1846 / Golub-Van Loan 8.4) gives approximate right singular vectors;
+// after re-orthonormalising them in float64, the one-sided float64 Jacobi iteration of svd3
+// continues from B = A V, whose columns are already nearly orthogonal, so it usually converges in
+// one sweep instead of four to six.
+BK_DEV void svd3_fast(const M3d& A, M3d& U, double s[3], M3d& V) {
+    // float32 warm start on S = A^T A.
+    float S[3][3], a32[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) a32[e] = (float)A.m[e];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) S[i][j] = a32[i] * a32[j] + a32[3 + i] * a32[3 + j] + a32[6 + i] * a32[6 + j];
+    float v[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
+#pragma unroll
+    for (int sweep = 0; sweep < 4; ++sweep) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int p = k == 2 ? 1 : 0;
+            const int q = k == 0 ? 1 : 2;
+            const int r = 3 - p - q;
+            float apq = S[p][q];
+            if (fabsf(apq) <= 1e-30f) continue;
+            float theta = (S[q][q] - S[p][p]) / (2.0f * apq);
+            float t = copysignf(1.0f, theta) / (fabsf(theta) + sqrtf(theta * theta + 1.0f));
+            float c = rsqrtf(t * t + 1.0f);
+            float sn = t * c;
+            S[p][p] -= t * apq;
+            S[q][q] += t * apq;
+            S[p][q] = S[q][p] = 0.0f;
+            float arp = S[r][p], arq = S[r][q];
+            S[r][p] = S[p][r] = c * arp - sn * arq;
+            S[r][q] = S[q][r] = sn * arp + c * arq;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                float vp = v[i][p], vq = v[i][q];
+                v[i][p] = c * vp - sn * vq;
+                v[i][q] = sn * vp + c * vq;
+            }
+        }
+    }
+    // Re-orthonormalise in float64 (Gram-Schmidt on columns 0, 1; column 2 = c0 x c1).
+    double c0[3] = {v[0][0], v[1][0], v[2][0]}, c1[3] = {v[0][1], v[1][1], v[2][1]};
+    double n0 = rsqrt(c0[0] * c0[0] + c0[1] * c0[1] + c0[2] * c0[2]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) c0[i] *= n0;
+    double d01 = c0[0] * c1[0] + c0[1] * c1[1] + c0[2] * c1[2];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) c1[i] -= d01 * c0[i];
+    double n1 = rsqrt(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) c1[i] *= n1;
+    double c2[3] = {c0[1] * c1[2] - c0[2] * c1[1], c0[2] * c1[0] - c0[0] * c1[2], c0[0] * c1[1] - c0[1] * c1[0]};
+    double vv[9] = {c0[0], c1[0], c2[0], c0[1], c1[1], c2[1], c0[2], c1[2], c2[2]};
+    // B = A V; one-sided float64 Jacobi on B's columns, V accumulating the rotations.
+    double b[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            b[3 * i + j] = A.m[3 * i] * vv[j] + A.m[3 * i + 1] * vv[3 + j] + A.m[3 * i + 2] * vv[6 + j];
+    for (int sweep = 0; sweep < 12; ++sweep) {
+        bool rotated = false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int p = k == 2 ? 1 : 0;
+            const int q = k == 0 ? 1 : 2;
+            double alpha = 0, beta = 0, gamma = 0;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                alpha += b[3 * r + p] * b[3 * r + p];
+                beta += b[3 * r + q] * b[3 * r + q];
+                gamma += b[3 * r + p] * b[3 * r + q];
+            }
+            if (gamma * gamma <= 1e-30 * alpha * beta) continue;
+            rotated = true;
+            double zeta = (beta - alpha) / (2.0 * gamma);
+            double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+            double c = rsqrt(1.0 + t * t);
+            double sn = c * t;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                double bp = b[3 * r + p], bq = b[3 * r + q];
+                b[3 * r + p] = c * bp - sn * bq;
+                b[3 * r + q] = sn * bp + c * bq;
+                double vp = vv[3 * r + p], vq = vv[3 * r + q];
+                vv[3 * r + p] = c * vp - sn * vq;
+                vv[3 * r + q] = sn * vp + c * vq;
+            }
+        }
+        if (!rotated) break;
+    }
+    bool zero[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double n = sqrt(b[c] * b[c] + b[3 + c] * b[3 + c] + b[6 + c] * b[6 + c]);
+        s[c] = n;
+        zero[c] = !(n > 1e-300);
+        double inv = zero[c] ? 0.0 : 1.0 / n;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) U.m[3 * r + c] = b[3 * r + c] * inv;
+    }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) V.m[e] = vv[e];
+    if (zero[0] || zero[1] || zero[2]) {
+        // Rank-deficient input: fall back to the reference-path solver, which completes U.
+        svd3(A, U, s, V);
+    }
+}
+
+// 3x3 SVD A = U diag(s) V^T in float32 by one-sided Jacobi (Hestenes 1958), iterated to float32
+// convergence. The reference computes its SVD in float64 and rounds U, s and V to float32 before
+// using them (physics/materials/ding.py:106-109); a converged float32 Jacobi SVD carries errors of
+// the same few-ulp size, with a third of the registers and latency of the float64 solve.
+// Rank-deficient input (a zero singular value) falls back to the float64 solver.
+BK_DEV void svd3f(const M3& A, M3& U, float s[3], M3& V) {
+    float b[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) b[e] = A.m[e];
+    float v[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
+    for (int sweep = 0; sweep < 6; ++sweep) {
+        bool rotated = false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int p = k == 2 ? 1 : 0;
+            const int q = k == 0 ? 1 : 2;
+            float alpha = 0.f, beta = 0.f, gamma = 0.f;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                alpha = fmaf(b[3 * r + p], b[3 * r + p], alpha);
+                beta = fmaf(b[3 * r + q], b[3 * r + q], beta);
+                gamma = fmaf(b[3 * r + p], b[3 * r + q], gamma);
+            }
+            // Columns orthogonal to 1e-6 (|gamma| <= 1e-6 sqrt(alpha beta)) are enough: the float64
+            // sweep below takes the off-diagonal terms from there to ~1e-12 / gap.
+            if (gamma * gamma <= 1e-12f * alpha * beta) continue;
+            rotated = true;
+            float zeta = (beta - alpha) / (2.0f * gamma);
+            float t = fabsf(zeta) > 1e18f ? 0.5f / zeta
+                                           : copysignf(1.0f, zeta) / (fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.0f)));
+            float c = rsqrtf(fmaf(t, t, 1.0f));
+            float sn = c * t;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                float bp = b[3 * r + p], bq = b[3 * r + q];
+                b[3 * r + p] = c * bp - sn * bq;
+                b[3 * r + q] = sn * bp + c * bq;
+                float vp = v[3 * r + p], vq = v[3 * r + q];
+                v[3 * r + p] = c * vp - sn * vq;
+                v[3 * r + q] = sn * vp + c * vq;
+            }
+        }
+        if (!rotated) break;
+    }
+    // Finish in float64. The float32 rotations leave the columns of B = A V orthogonal to ~2^-24,
+    // but nearly equal singular values (small elastic strains) make float32 mix their singular
+    // vectors by ~2^-24 / gap. One float64 Jacobi sweep from this start reduces the off-diagonal
+    // terms to ~2^-48 / gap (Jacobi's quadratic convergence), after which s = |B_i| and U = B / s
+    // agree with the float64 SVD to float32 rounding.
+    // The accumulated float32 rotations are orthonormal only to ~1e-7, which would scale s by as
+    // much; re-orthonormalise them in float64 first (Gram-Schmidt, third column = cross product).
+    double vv[9], bb[9];
+    {
+        double c0[3] = {v[0], v[3], v[6]}, c1[3] = {v[1], v[4], v[7]};
+        double n0 = rsqrt(c0[0] * c0[0] + c0[1] * c0[1] + c0[2] * c0[2]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) c0[i] *= n0;
+        double d01 = c0[0] * c1[0] + c0[1] * c1[1] + c0[2] * c1[2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) c1[i] -= d01 * c0[i];
+        double n1 = rsqrt(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) c1[i] *= n1;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            vv[3 * i] = c0[i];
+            vv[3 * i + 1] = c1[i];
+        }
+        vv[2] = c0[1] * c1[2] - c0[2] * c1[1];
+        vv[5] = c0[2] * c1[0] - c0[0] * c1[2];
+        vv[8] = c0[0] * c1[1] - c0[1] * c1[0];
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            bb[3 * r + c] = (double)A.m[3 * r] * vv[c] + (double)A.m[3 * r + 1] * vv[3 + c] +
+                            (double)A.m[3 * r + 2] * vv[6 + c];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int p = k == 2 ? 1 : 0;
+        const int q = k == 0 ? 1 : 2;
+        double alpha = 0, beta = 0, gamma = 0;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            alpha += bb[3 * r + p] * bb[3 * r + p];
+            beta += bb[3 * r + q] * bb[3 * r + q];
+            gamma += bb[3 * r + p] * bb[3 * r + q];
+        }
+        if (gamma * gamma <= 1e-30 * alpha * beta) continue;
+        // tan of the rotation angle, t = 2 gamma sign(d) / (|d| + sqrt(d^2 + 4 gamma^2)), d = beta - alpha.
+        double d = beta - alpha;
+        double t = 2.0 * gamma / (d >= 0.0 ? d + sqrt(d * d + 4.0 * gamma * gamma) : d - sqrt(d * d + 4.0 * gamma * gamma));
+        double c = rsqrt(1.0 + t * t);
+        double sn = c * t;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            double bp = bb[3 * r + p], bq = bb[3 * r + q];
+            bb[3 * r + p] = c * bp - sn * bq;
+            bb[3 * r + q] = sn * bp + c * bq;
+            double vp = vv[3 * r + p], vq = vv[3 * r + q];
+            vv[3 * r + p] = c * vp - sn * vq;
+            vv[3 * r + q] = sn * vp + c * vq;
+        }
+    }
+    bool degenerate = false;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double n2 = bb[c] * bb[c] + bb[3 + c] * bb[3 + c] + bb[6 + c] * bb[6 + c];
+        degenerate |= !(n2 > 1e-30);
+        double inv = rsqrt(n2);
+        s[c] = (float)(n2 * inv);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) U.m[3 * r + c] = (float)(bb[3 * r + c] * inv);
+    }
+#pragma unroll
+    for (int e = 0; e < 9; ++e) V.m[e] = (float)vv[e];
+    if (degenerate) {
+        M3d Ad, Ud, Vd;
+        double sd[3];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) Ad.m[e] = (double)A.m[e];
+        svd3(Ad, Ud, sd, Vd);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) { U.m[e] = (float)Ud.m[e]; V.m[e] = (float)Vd.m[e]; }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s[k] = (float)sd[k];
+    }
+}
+
 // ------------------------------------------------- physics/transfer.py:4-28
 BK_DEV float qweight(float l, int i) {
     if (i == 0) return 0.5f * (1.5f - l) * (1.5f - l);
@@ -208,9 +449,10 @@ BK_DEV float porosity_coefficient(float n) {
     return c;
 }
 
-// Scalar overstress Newton solve (ding.py:77-87): 32 steps from r = 0 in float32.
-// Iterates of this concave increasing residual approach the root monotonically from
-// below, so once a step no longer changes r the remaining steps are no-ops.
+// Scalar overstress Newton solve (ding.py:77-87): up to 32 steps from r = 0 in float32.
+// Iterates of this concave increasing residual approach the root monotonically from below;
+// once a step moves r by no more than a few float32 ulps the iteration has converged and the
+// reference's remaining steps only toggle the last bit, so it stops there.
 BK_DEV float solve_overstress(float q2, float p2, float d, float h) {
     float r = 0.0f;
     if (q2 + p2 > 1.0f) {
@@ -220,8 +462,9 @@ BK_DEV float solve_overstress(float q2, float p2, float d, float h) {
             float res = r + 1.0f - q2 / dd2 - p2 / md2;
             float der = 1.0f + 2.0f * d * q2 / (dd2 * dd) + 2.0f * h * p2 / (md2 * md);
             float rn = r - res / der;
-            if (rn == r) break;
+            bool done = fabsf(rn - r) <= 2.4e-7f * fabsf(rn);
             r = rn;
+            if (done) break;
         }
     }
     return r;
@@ -259,14 +502,34 @@ BK_DEV double porosity_prediction(double n, float q, float p, float d, float h, 
     return Vp * exp((double)e * (1.0 - 1.0 / den)) - 1.0 + (double)n0;
 }
 
-// End-state porosity (porous_return.py:43-61): elastic early exit, else 64 bisection
-// steps of n -> prediction(n) on [0, 1 - 1e-9].
-BK_DEV float solve_porosity(float q, float p, float d, float h, float e, double Vp, float n0) {
-    double trial = Vp - 1.0 + (double)n0;
-    if (trial > 0.0 && trial < 1.0) {
-        double a = pressure_coefficient64(trial);
-        if ((double)q + a * (double)p <= 1.0) return (float)trial;
+// prediction(n) and its derivative in n. The overstress root r(n) is the reference's 48-step Newton
+// solve; dr/dn follows from the implicit function theorem on its residual
+// R = r + 1 - q/(1+dr)^2 - a p/(1+h a r)^2 with a = a(n) (the derivatives the reference's
+// SolvePorosityGradient uses, porous_return.py:68-92).
+BK_DEV double porosity_prediction_slope(double n, float qf, float pf, float df, float hf, float ef, double Vp,
+                                        float n0, double& slope) {
+    const double q = qf, p = pf, d = df, h = hf, e = ef;
+    double a = pressure_coefficient64(n);
+    double r = overstress64(q, a * p, d, h * a);
+    double v = 1.0 + h * a * r;
+    double core = Vp * exp(e * (1.0 - 1.0 / v));
+    double da = 0.0;
+    if (n > 0.0) {
+        double lg = log(1.0 / n);
+        da = a * (2.0 / (n * lg) - 3.5 / (3.5 * n + 1.0));
     }
+    double dr = 0.0;
+    if (q + a * p > 1.0) {
+        double u = 1.0 + d * r;
+        double Rr = 1.0 + 2.0 * d * q / (u * u * u) + 2.0 * h * a * a * p / (v * v * v);
+        dr = p * (1.0 - h * a * r) / (Rr * v * v * v) * da;
+    }
+    slope = core * e * h * (da * r + a * dr) / (v * v);
+    return core - 1.0 + (double)n0;
+}
+
+// The reference's 64-step bisection of n -> prediction(n) on [0, 1 - 1e-9] (porous_return.py:51-61).
+BK_DEV float solve_porosity_bisection(float q, float p, float d, float h, float e, double Vp, float n0) {
     double lo = 0.0, hi = 1.0 - 1.0e-9;
     for (int it = 0; it < 64; ++it) {
         double mid = (lo + hi) * 0.5;
@@ -276,19 +539,48 @@ BK_DEV float solve_porosity(float q, float p, float d, float h, float e, double 
     return (float)((lo + hi) * 0.5);
 }
 
+// End-state porosity (porous_return.py:43-61): the elastic early exit, then the root of
+// g(n) = n - prediction(n) on the reference's bracket [0, 1 - 1e-9] with the reference's test
+// (n lies below the root when n < prediction(n)). Safeguarded Newton steps replace the 64
+// bisection steps: a step that leaves the current bracket becomes a bisection step, so the
+// iteration cannot escape the bracket and converges in a few evaluations. When the bracket's
+// lower end is not below the root (g(0+) >= 0) the reference's bisection runs unchanged. The root
+// is resolved to ~1e-14 relative, far below the float32 rounding of the returned porosity.
+BK_DEV float solve_porosity(float q, float p, float d, float h, float e, double Vp, float n0) {
+    double trial = Vp - 1.0 + (double)n0;
+    if (trial > 0.0 && trial < 1.0) {
+        double a = pressure_coefficient64(trial);
+        if ((double)q + a * (double)p <= 1.0) return (float)trial;
+    }
+    double lo = 0.0, hi = 1.0 - 1.0e-9;
+    // g(0+) = -trial: the root lies above zero only when the elastic prediction is positive.
+    if (!(trial > 0.0)) return solve_porosity_bisection(q, p, d, h, e, Vp, n0);
+    double n = trial < hi ? trial : 0.5 * (lo + hi);
+    for (int it = 0; it < 100; ++it) {
+        double slope;
+        double pred = porosity_prediction_slope(n, q, p, d, h, e, Vp, n0, slope);
+        double g = n - pred;
+        if (n < pred) lo = n; else hi = n;
+        double dg = 1.0 - slope;
+        double next = n - g / dg;
+        if (!(next > lo && next < hi)) next = 0.5 * (lo + hi);
+        double step = fabs(next - n);
+        n = next;
+        if (step <= 1e-14 * n || hi - lo <= 1e-15 * hi) break;
+    }
+    return (float)n;
+}
+
 struct DingOut {
     M3 Fe, tau;
     float residual;
 };
 
-// Ding return map (ding.py:103-137) given the float64 SVD of the trial gradient.
-BK_DEV DingOut ding_return(const M3& trial, const M3d& Ud, const double* sd, const M3d& Vd, float mu, float lam,
+// Ding return map (ding.py:103-137) given the SVD of the trial gradient (float32 factors).
+BK_DEV DingOut ding_return(const M3& trial, const M3& Um, const float* s, const M3& Vm, float mu, float lam,
                            float ty, float eta, float a, float dt) {
-    float U[9], V[9], s[3];
-#pragma unroll
-    for (int e = 0; e < 9; ++e) { U[e] = (float)Ud.m[e]; V[e] = (float)Vd.m[e]; }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) s[k] = (float)sd[k];
+    const float* U = Um.m;
+    const float* V = Vm.m;
     float eps[3] = {logf(s[0]), logf(s[1]), logf(s[2])};
     float tr = eps[0] + eps[1] + eps[2];
     float ts[3];
@@ -320,7 +612,8 @@ BK_DEV DingOut ding_return(const M3& trial, const M3d& Ud, const double* sd, con
                                + (U[3 * i + 2] * cs[2]) * U[3 * k + 2];
         }
     if (a == 0.0f) {
-        float scale = powf(det3(trial) / det3(o.Fe), 1.0f / 3.0f);
+        // pow(x, 1/3) of the reference; cube root of the same argument.
+        float scale = cbrtf(det3(trial) / det3(o.Fe));
 #pragma unroll
         for (int e = 0; e < 9; ++e) o.Fe.m[e] *= scale;
     }
@@ -345,9 +638,11 @@ struct DingParticleOut {
 };
 
 // UpdateDing for one particle (ding.py:154-221). Returns false when the old porosity is
-// outside [0, 1) (flag 0 set, nothing written, as in the reference).
+// outside [0, 1) (flag 0 set, nothing written, as in the reference). Fp = Fe^-1 F is formed
+// only when `need_fp` or when the porosity update needs it (uncoupled mode).
 BK_DEV bool update_ding_particle(const DingParamsDev& P, const M3& Fe_old, float por, int gel, const M3& F_tot,
-                                 const M3& C_new, float T, float eta_base, int32_t* flags, DingParticleOut& out) {
+                                 const M3& C_new, float T, float eta_base, int32_t* flags, DingParticleOut& out,
+                                 bool need_fp = true) {
     if (!isfinite(por) || por < 0.0f || por >= 1.0f) { set_flag(flags, 0); return false; }
     int reached = T >= P.knots[3];
     float Teff = T;
@@ -364,14 +659,12 @@ BK_DEV bool update_ding_particle(const DingParamsDev& P, const M3& Fe_old, float
 #pragma unroll
     for (int e = 0; e < 9; ++e) G.m[e] = dt * C_new.m[e] + ((e % 4) == 0 ? 1.0f : 0.0f);
     M3 trial = matmul(G, Fe_old);
-    M3d Ad, Ud, Vd;
-    double sd[3];
-#pragma unroll
-    for (int e = 0; e < 9; ++e) Ad.m[e] = (double)trial.m[e];
-    svd3(Ad, Ud, sd, Vd);
+    M3 Ud, Vd;
+    float sd[3];
+    svd3f(trial, Ud, sd, Vd);
     float ret_por = por, consistency = 0.0f;
     if (P.coupled_porosity) {
-        float st[3] = {logf((float)sd[0]), logf((float)sd[1]), logf((float)sd[2])};
+        float st[3] = {logf(sd[0]), logf(sd[1]), logf(sd[2])};
         float tr = st[0] + st[1] + st[2];
         float ts[3];
 #pragma unroll
@@ -398,13 +691,19 @@ BK_DEV bool update_ding_particle(const DingParamsDev& P, const M3& Fe_old, float
 #pragma unroll
         for (int e = 0; e < 9; ++e) { Fd.m[e] = (double)F_tot.m[e]; Fed.m[e] = (double)Fe.m[e]; }
         double vs = det3(Fd) / (target * det3(Fed));
-        float scale = (float)pow(vs, 1.0 / 3.0);
+        float scale = (float)cbrt(vs);  // pow(vs, 1/3) in the reference
 #pragma unroll
         for (int e = 0; e < 9; ++e) Fe.m[e] *= scale;
     }
-    M3 Fp = matmul(inverse3(Fe), F_tot);
-    float npor = det3(Fp) - 1.0f + n0;
-    if (P.coupled_porosity) npor = ret_por;
+    M3 Fp;
+    float npor;
+    if (P.coupled_porosity) {
+        npor = ret_por;
+        if (need_fp) Fp = matmul(inverse3(Fe), F_tot);
+    } else {
+        Fp = matmul(inverse3(Fe), F_tot);
+        npor = det3(Fp) - 1.0f + n0;
+    }
     if (n0 == 0.0f && por == 0.0f) npor = 0.0f;
     if (!isfinite(npor) || npor < 0.0f || npor >= 1.0f) set_flag(flags, 0);
     out.Fe = Fe;

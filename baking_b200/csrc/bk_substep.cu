@@ -110,9 +110,18 @@ __device__ __forceinline__ long long pack_base(const int* b) {
     return ((long long)b[0] << 42) | ((long long)b[1] << 21) | (long long)b[2];
 }
 
-// Block-level min/max of valid stencil nodes into the active node box (bounds[0..2] lo, [3..5] hi).
-// Every thread of the block must call this (it synchronises the block).
-__device__ void update_bounds(int* bounds, bool valid, const int* b) {
+// Nodes a block may stage in shared memory before flushing them to the grid.
+constexpr int kTileNodes = 512;
+
+// Node box touched by one block's particles.
+struct BlockBox {
+    int lo[3], ext[3], count;  // count = 0: no valid particle in the block
+    bool tiled;                // the box fits a shared-memory tile of kTileNodes
+};
+
+// Block-level min/max of valid stencil nodes; also widens the active node box of the substep
+// (bounds[0..2] lo, [3..5] hi). Every thread of the block must call this (it synchronises the block).
+__device__ BlockBox block_box(int* bounds, bool valid, const int* b) {
     __shared__ int s_box[6];
     if (threadIdx.x < 6) s_box[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
     __syncthreads();
@@ -126,10 +135,36 @@ __device__ void update_bounds(int* bounds, bool valid, const int* b) {
         }
     }
     __syncthreads();
-    if (threadIdx.x < 3 && s_box[threadIdx.x] != INT_MAX) {
-        atomicMin(bounds + threadIdx.x, s_box[threadIdx.x]);
-        atomicMax(bounds + 3 + threadIdx.x, s_box[3 + threadIdx.x]);
+    BlockBox bb;
+    bb.count = 0;
+    bb.tiled = true;
+    if (s_box[0] != INT_MAX) {
+        long long count = 1;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            bb.lo[a] = s_box[a];
+            bb.ext[a] = s_box[3 + a] - s_box[a] + 1;
+            count *= bb.ext[a];
+        }
+        bb.tiled = count <= kTileNodes;
+        bb.count = bb.tiled ? (int)count : 0;
+        if (threadIdx.x < 3) {
+            atomicMin(bounds + threadIdx.x, s_box[threadIdx.x]);
+            atomicMax(bounds + 3 + threadIdx.x, s_box[3 + threadIdx.x]);
+        }
     }
+    return bb;
+}
+
+__device__ __forceinline__ int tile_index(const BlockBox& bb, int x, int y, int z) {
+    return ((x - bb.lo[0]) * bb.ext[1] + (y - bb.lo[1])) * bb.ext[2] + (z - bb.lo[2]);
+}
+
+__device__ __forceinline__ int64_t tile_node(const BlockBox& bb, int t, int R) {
+    int z = t % bb.ext[2];
+    int y = (t / bb.ext[2]) % bb.ext[1];
+    int x = t / (bb.ext[2] * bb.ext[1]);
+    return node_index(bb.lo[0] + x, bb.lo[1] + y, bb.lo[2] + z, R);
 }
 
 // ------------------------------------------------------------------ surface
@@ -227,6 +262,7 @@ __global__ void k_surface_owners(Params P, BkState in, BkConstants cst, BkSurfac
 struct TransportSmem {
     float w[kThreads][9];
     double val[kThreads][4];
+    double tile[4][kTileNodes];
 };
 
 __global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkState in, BkConstants cst, GridPtrs g,
@@ -260,7 +296,11 @@ __global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkStat
 #pragma unroll
         for (int k = 0; k < 9; ++k) sm.w[tid][k] = 0.f;
     }
-    update_bounds(g.bounds, valid, st.b);  // contains __syncthreads
+    const BlockBox bb = block_box(g.bounds, valid, st.b);  // synchronises the block
+    for (int t = tid; t < bb.count; t += kThreads)
+#pragma unroll
+        for (int f = 0; f < 4; ++f) sm.tile[f][t] = 0.0;
+    __syncthreads();
     long long key = valid ? pack_base(st.b) : -1;
     long long prev = __shfl_up_sync(kFull, key, 1);
     unsigned starts = __ballot_sync(kFull, valid && (lane == 0 || prev != key));
@@ -279,10 +319,23 @@ __global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkStat
 #pragma unroll
                 for (int f = 0; f < 4; ++f) acc[f] += w * sm.val[k][f];
             }
-            int64_t node = node_index(b0 + ox, b1 + oy, b2 + oz, P.R);
+            if (bb.tiled) {
+                int t = tile_index(bb, b0 + ox, b1 + oy, b2 + oz);
 #pragma unroll
-            for (int f = 0; f < 4; ++f) atomicAdd(g.f[f] + node, acc[f]);
+                for (int f = 0; f < 4; ++f) atomicAdd(&sm.tile[f][t], acc[f]);
+            } else {
+                int64_t node = node_index(b0 + ox, b1 + oy, b2 + oz, P.R);
+#pragma unroll
+                for (int f = 0; f < 4; ++f) atomicAdd(g.f[f] + node, acc[f]);
+            }
         }
+    }
+    __syncthreads();
+    for (int t = tid; t < bb.count; t += kThreads) {
+        if (sm.tile[1][t] == 0.0 && sm.tile[0][t] == 0.0 && sm.tile[3][t] == 0.0) continue;
+        int64_t node = tile_node(bb, t, P.R);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) atomicAdd(g.f[f] + node, sm.tile[f][t]);
     }
 }
 
@@ -419,6 +472,7 @@ struct P2GSmem {
     float m[kThreads];
     float q[kThreads][3];
     float A[kThreads][9];
+    float4 tile[kTileNodes];
 };
 
 __global__ void __launch_bounds__(kThreads) k_p2g(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
@@ -542,7 +596,9 @@ __global__ void __launch_bounds__(kThreads) k_p2g(Params P, BkState in, BkState 
     for (int r = 0; r < 3; ++r) sm.q[tid][r] = q[r];
 #pragma unroll
     for (int e = 0; e < 9; ++e) sm.A[tid][e] = A[e];
-    update_bounds(g.bounds, valid, st.b);  // contains __syncthreads
+    const BlockBox bb = block_box(g.bounds, valid, st.b);  // synchronises the block
+    for (int t = tid; t < bb.count; t += kThreads) sm.tile[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
     long long key = valid ? pack_base(st.b) : -1;
     long long prev = __shfl_up_sync(kFull, key, 1);
     unsigned starts = __ballot_sync(kFull, valid && (lane == 0 || prev != key));
@@ -564,8 +620,22 @@ __global__ void __launch_bounds__(kThreads) k_p2g(Params P, BkState in, BkState 
                 for (int r = 0; r < 3; ++r)
                     ap[r] += w * (sm.q[k][r] + (sm.A[k][3 * r] * fo[0] + sm.A[k][3 * r + 1] * fo[1] + sm.A[k][3 * r + 2] * fo[2]));
             }
-            atomicAdd(g.pm + node_index(b0 + ox, b1 + oy, b2 + oz, P.R), make_float4(ap[0], ap[1], ap[2], am));
+            if (bb.tiled) {
+                float* cell = reinterpret_cast<float*>(&sm.tile[tile_index(bb, b0 + ox, b1 + oy, b2 + oz)]);
+                atomicAdd(cell + 0, ap[0]);
+                atomicAdd(cell + 1, ap[1]);
+                atomicAdd(cell + 2, ap[2]);
+                atomicAdd(cell + 3, am);
+            } else {
+                atomicAdd(g.pm + node_index(b0 + ox, b1 + oy, b2 + oz, P.R), make_float4(ap[0], ap[1], ap[2], am));
+            }
         }
+    }
+    __syncthreads();
+    for (int t = tid; t < bb.count; t += kThreads) {
+        float4 v = sm.tile[t];
+        if (v.w == 0.0f && v.x == 0.0f && v.y == 0.0f && v.z == 0.0f) continue;
+        atomicAdd(g.pm + tile_node(bb, t, P.R), v);
     }
 }
 
@@ -574,7 +644,9 @@ __device__ __forceinline__ void atomic_max_nonneg(float* addr, float value) {
     if (value > 0.0f) atomicMax(reinterpret_cast<int*>(addr), __float_as_int(value));
 }
 
-__global__ void __launch_bounds__(128) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
+// 6 blocks of 128 threads per SM (80 registers): the float64 steps of the return map are latency
+// bound, so the extra resident warps outweigh a few spilled registers.
+__global__ void __launch_bounds__(128, 6) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
                                                    BkDiagnostics diag, BkFlags flags) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (blockIdx.x == 0 && threadIdx.x < 6) {
@@ -624,7 +696,7 @@ __global__ void __launch_bounds__(128) k_g2p_return(Params P, BkState in, BkStat
     float T = P.transport ? (float)out.temperature[i] : in.material_temperature[i];
     DingParticleOut o;
     if (!update_ding_particle(P.ding, load_m3(in.Fe, i, pitch), in.porosity[i], in.gelled[i], Fn, Cn, T,
-                              __ldg(cst.viscosity_parameter), flags.ding, o))
+                              __ldg(cst.viscosity_parameter), flags.ding, o, diag.plastic_gradients != nullptr))
         return;
     store_m3(out.Fe, i, pitch, o.Fe);
     store_m3(out.tau, i, pitch, o.tau);

@@ -49,6 +49,17 @@ def _morton3(ix, iy, iz):
     return spread(ix) | (spread(iy) << np.uint64(1)) | (spread(iz) << np.uint64(2))
 
 
+def stencil_order(points, spacing, origin=(0.0, 0.0, 0.0)):
+    """Permutation that groups particles by quadratic stencil base floor(x/dx - 0.5), Morton order.
+
+    Particles sharing a base scatter to the same 27 nodes, so the device scatter sums them in
+    registers and shared memory before touching the grid.
+    """
+    base = np.floor((np.asarray(points) - np.asarray(origin)) / spacing - 0.5).astype(np.int64)
+    base -= base.min(axis=0)
+    return np.argsort(_morton3(base[:, 0], base[:, 1], base[:, 2]), kind="stable")
+
+
 def _kuhn_index(local):
     """Index (in VoxelTetMesh's tet order) of the Kuhn tet containing unit-voxel coordinates ``local``."""
     from itertools import permutations
@@ -89,6 +100,7 @@ def box_loaf(resolution=128, particle_count=1_000_000, seed=0, size=(0.4, 0.15, 
     rng = np.random.default_rng(seed)
     corner = np.repeat(cells, per, axis=0).astype(np.float64)
     points = origin + (corner + rng.random((particle_count, 3))) * dx
+    points = points[stencil_order(points, dx)]
     source_tets = _locate(points, origin, voxel, tuple(nvox))
     if np.any(np.bincount(source_tets, minlength=len(mesh.tet_indices)) == 0):
         raise ValueError("a tet received no particle; use more particles")
@@ -115,9 +127,7 @@ def jittered_sphere(resolution=64, per_axis=2, radius=0.1, center=(0.5, 0.5, 0.3
     rng = np.random.default_rng(seed)
     points = (grid + 0.5 + rng.uniform(-0.5, 0.5, grid.shape)) * sub
     points = points[np.linalg.norm(points - np.asarray(center), axis=1) <= radius]
-    cell = np.floor(points / dx).astype(np.int64)
-    order = np.argsort(_morton3(cell[:, 0], cell[:, 1], cell[:, 2]), kind="stable")
-    points = points[order]
+    points = points[stencil_order(points, dx)]
     # Mesh: the voxels (size dx) that hold particles.
     vox_lo = np.floor(points.min(axis=0) / dx).astype(int)
     vcell = np.floor(points / dx).astype(np.int64) - vox_lo
