@@ -267,6 +267,19 @@ BK_API int bk_substep(const BkSubstepParams *params, const BkState *in, BkState 
                       BkGrid *grid, BkSurface *surface, BkDiagnostics *diagnostics, BkFlags *flags,
                       int32_t phases, void *stream);
 
+/* bk_substep's mechanics phase with the grid held in a fixed array inside this library, for
+   callers that must not allocate device memory (code inside an allocator hook, a real-time or
+   signal-safe path, or a process that forbids device allocation after start-up): the call
+   allocates and frees nothing. It has no counterpart in the reference. Limits: neo-Hookean or
+   Ding without transport or gas, grid resolution 4..48 (48^3 nodes, about 3.4 MB held on every
+   GPU that loads the library until exit); larger grids return BK_ERR_ARGUMENT with a message.
+   The first call on each device looks up the array's device address (make it before any stream
+   capture). All calls on a device share the array and each call clears it first, so calls that
+   overlap on the GPU race and must be serialised by the caller. */
+BK_API int bk_substep_static_grid(const BkSubstepParams *params, const BkState *in, BkState *out,
+                                  const BkConstants *constants, BkDiagnostics *diagnostics, BkFlags *flags,
+                                  void *stream);
+
 /* Per-kernel timing of the fused entry points with CUDA events on the launching stream.
    bk_profile_start clears old records and starts recording; bk_profile_stop stops;
    bk_profile_report waits for the events and writes, per kernel name (name_capacity bytes each),
