@@ -498,6 +498,7 @@ BK_DEV double overstress64(double q, double p, double d, double h) {
 BK_DEV double porosity_prediction(double n, float q, float p, float d, float h, float e, double Vp, float n0) {
     double a = pressure_coefficient64(n);
     double r = overstress64((double)q, a * (double)p, (double)d, (double)h * a);
+    if (r == 0.0) return Vp - 1.0 + (double)n0;  // no overstress: exp(e (1 - 1/1)) = exp(0) = 1 exactly
     double den = 1.0 + (double)h * a * r;
     return Vp * exp((double)e * (1.0 - 1.0 / den)) - 1.0 + (double)n0;
 }
