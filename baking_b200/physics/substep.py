@@ -229,8 +229,24 @@ class SubstepEngine:
             c.gas_rate_per_particle = int(rates.shape[0] == self.n and self.n > 1)
         return c
 
+    def mechanics_grid(self):
+        """A second grid for mechanics-only substeps (its own node arrays and active boxes), so that
+        recomputed substeps leave the simulator's grid holding its last substep."""
+        R = self.sim.simulation_config.grid_resolution
+        dev = self.sim.device
+        empty = [2 ** 31 - 1] * 3 + [-2 ** 31] * 3
+        tensors = dict(node_pm=torch.zeros(R ** 3, 4, dtype=torch.float32, device=dev),
+                       node_v=torch.zeros(R ** 3, 4, dtype=torch.float32, device=dev),
+                       bounds=torch.tensor(empty + empty, dtype=torch.int32, device=dev))
+        grid = BkGrid()
+        grid.node_pm, grid.node_v, grid.bounds = (_p(tensors[k]) for k in ("node_pm", "node_v", "bounds"))
+        grid.node_dT_ratio = _p(self.node_dT_ratio)
+        for k in range(7):
+            grid.fields[k] = _p(self.fields[k])
+        return grid, tensors
+
     # ---------------------------------------------------------------- launch
-    def run(self, state_in, state_out, settling, phases, full_diagnostics):
+    def run(self, state_in, state_out, settling, phases, full_diagnostics, grid=None):
         p = self.params(settling)
         cst = self.constants(settling)
         sin = state_struct(state_in, self.is_ding, self.transport, self.gas)
@@ -247,7 +263,8 @@ class SubstepEngine:
         if timer is not None:
             start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             start.record()
-        rc = self.lib.bk_substep(C.byref(p), C.byref(sin), C.byref(sout), C.byref(cst), C.byref(self.grid),
+        rc = self.lib.bk_substep(C.byref(p), C.byref(sin), C.byref(sout), C.byref(cst),
+                                 C.byref(self.grid if grid is None else grid),
                                  C.byref(self.surface), C.byref(diag), C.byref(self.flags), int(phases), stream)
         if timer is not None:
             end.record()

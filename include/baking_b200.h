@@ -302,6 +302,33 @@ BK_API int bk_materialize(const BkSubstepParams *params, const BkState *state, c
                           float *yield_stress, float *viscosity, double *gas_pressure, double *saturation,
                           float *particle_mass, void *stream);
 
+/* Adjoint (reverse-mode derivative) of one state of the mechanics substep, in the plane layout of
+   BkState. Ding fields may be NULL for the neo-Hookean model. `temperature` is the adjoint of the
+   per-particle material temperature, which is constant without transport: the call adds this
+   substep's contribution to the incoming value. */
+typedef struct BkAdjointState {
+    float *x, *v, *C, *F;          /* 3, 3, 9, 9 planes */
+    float *Fe, *tau;               /* Ding, 9 planes */
+    float *porosity;               /* Ding */
+    float *temperature;            /* Ding, accumulated over substeps */
+} BkAdjointState;
+
+/* Reverse sweep of one mechanics substep (P2G, grid update, G2P, neo-Hookean stress or the
+   uncoupled Ding return map; physics/mpm.py:163-205 with transfer.py:37-105, grid.py:20-38,
+   elastic.py:4-26, ding.py:103-221). The reference gets these derivatives from Warp's tape replaying
+   its kernels' generated adjoints; this entry point replaces that replay for one substep.
+   Inputs: the substep's input state `in`, the grid that bk_substep left after running from `in`
+   (node_pm, node_v: R^3 float4), and `out_adjoint` = dL/d(output state). Writes
+   `in_adjoint` = dL/d(input state); `in_adjoint` may be the same arrays as `out_adjoint`.
+   `node_v_adjoint` and `node_pm_adjoint` are R^3 float4 scratch arrays. `parameter_adjoint`
+   (device, float64, may be NULL) accumulates dL/d(shear modulus), dL/d(Lame lambda) and
+   dL/d(viscosity parameter). Transport, gas and the coupled porosity solve are not covered
+   (BK_ERR_UNSUPPORTED). */
+BK_API int bk_substep_adjoint(const BkSubstepParams *params, const BkState *in, const BkConstants *constants,
+                              const float *node_pm, const float *node_v, const BkAdjointState *out_adjoint,
+                              BkAdjointState *in_adjoint, float *node_v_adjoint, float *node_pm_adjoint,
+                              double *parameter_adjoint, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
