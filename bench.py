@@ -114,11 +114,14 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def load_traffic():
+def load_traffic(n):
+    """Per-launch DRAM bytes (read + write) of each kernel from the committed ncu capture, scaled to
+    ``n`` particles (the kernels' traffic is per particle up to the small grid part)."""
     path = ROOT / "profiles" / "traffic.json"
-    if path.exists():
-        return json.loads(path.read_text())
-    return {}
+    if not path.exists():
+        return {}
+    data = json.loads(path.read_text())
+    return {k: v["bytes_per_launch"] * n / v["particles"] for k, v in data.items() if isinstance(v, dict)}
 
 
 def active_node_count(sim):
@@ -257,7 +260,7 @@ def main():
     del result
 
     peak, peak_kind = load_peaks()
-    traffic = load_traffic()
+    traffic = load_traffic(n)
     dominant = max(per_kernel.items(), key=lambda kv: kv[1]["total_s"]) if per_kernel else None
     roofline = None
     if dominant:
