@@ -1,0 +1,193 @@
+"""Learned surrogate of the Ding return map: MLP 7 -> 64 -> 64 -> 3 (SiLU), BF16 weights, FP32 accumulation.
+
+Inputs per yielding particle: the three log singular values of the trial elastic gradient (sorted
+descending), the effective temperature after the gelation latch, the water saturation, the gas
+content and the plastic volume strain log(1 - n0 + n). Outputs: the return's change of the three
+log principal strains (before the coupled-porosity volume correction), from which the returned
+elastic gradient, the Kirchhoff stress and the end-state porosity follow exactly. The reference
+has no learned component; its exact return map (physics/materials/ding.py:103-137,
+porous_return.py:43-61) produces the training pairs, runs for particles outside the training
+range, and judges the surrogate's error.
+
+Training runs on the device through the library's own kernels: ``bk_mlp_gradient`` (forward +
+backward, rounded like inference), ``bk_mlp_adam`` and ``bk_mlp_pack``; inference uses the tensor
+cores (``bk_mlp_infer`` stand-alone, or fused into the substep's G2P kernel).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+
+P = C.c_void_p
+FEATURES, OUTPUTS, PARAMS, PACKED_BYTES = 7, 3, 4867, 12864
+FEATURE_NAMES = ("log_s1", "log_s2", "log_s3", "temperature", "saturation", "gas", "plastic_volume_strain")
+
+
+class BkMlpNorm(C.Structure):
+    _fields_ = [("in_mean", C.c_float * 8), ("in_scale", C.c_float * 8), ("out_scale", C.c_float * 4)]
+
+
+SIGNATURES = {
+    "bk_mlp_infer": [C.c_int64, P, P, P, P, P, P],
+    "bk_mlp_gradient": [C.c_int64, P, P, P, P, P, P, P],
+    "bk_mlp_adam": [P, P, P, P, C.c_int32, C.c_float, C.c_float, C.c_float, C.c_float, P],
+    "bk_mlp_pack": [P, P, P],
+}
+
+
+def _lib_handle():
+    lib = _lib.load()
+    for name, argtypes in SIGNATURES.items():
+        fn = getattr(lib, name)
+        if fn.argtypes != argtypes:
+            fn.restype = C.c_int
+            fn.argtypes = argtypes
+    return lib
+
+
+def _call(lib, name, *args):
+    rc = getattr(lib, name)(*args)
+    if rc != 0:
+        raise RuntimeError(f"{name} failed ({rc}): {lib.bk_last_error().decode(errors='replace')}")
+
+
+def initial_parameters(seed=0):
+    """He-style initial weights for SiLU layers, zero biases (FP32 vector of PARAMS values)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(PARAMS, np.float32)
+    p[0:448] = rng.standard_normal(448) * np.sqrt(2.0 / FEATURES)
+    p[512:4608] = rng.standard_normal(4096) * np.sqrt(2.0 / 64)
+    p[4672:4864] = rng.standard_normal(192) * np.sqrt(1.0 / 64)
+    return p
+
+
+@dataclass
+class Normalisation:
+    in_mean: np.ndarray      # (7,)
+    in_scale: np.ndarray     # (7,)
+    out_scale: np.ndarray    # (3,)
+    in_low: np.ndarray       # (7,) training range (raw units) for the out-of-distribution test
+    in_high: np.ndarray
+
+    @classmethod
+    def fit(cls, features, targets, margin=0.0):
+        f = np.asarray(features, np.float64)[:, :FEATURES]
+        t = np.asarray(targets, np.float64)[:, :OUTPUTS]
+        mean = f.mean(0)
+        scale = f.std(0)
+        scale[scale < 1e-12] = 1.0
+        out = np.sqrt((t * t).mean(0))
+        out[out < 1e-12] = 1.0
+        lo, hi = f.min(0), f.max(0)
+        pad = margin * (hi - lo)
+        return cls(mean.astype(np.float32), scale.astype(np.float32), out.astype(np.float32),
+                   (lo - pad).astype(np.float32), (hi + pad).astype(np.float32))
+
+    def struct(self):
+        s = BkMlpNorm()
+        s.in_mean[:FEATURES] = [float(v) for v in self.in_mean]
+        s.in_scale[:] = [float(v) for v in self.in_scale] + [1.0]
+        s.out_scale[:OUTPUTS] = [float(v) for v in self.out_scale]
+        s.out_scale[3] = 1.0
+        return s
+
+
+class ReturnMapMlp:
+    """Device-resident parameters, Adam state and packed operands of the surrogate network."""
+
+    def __init__(self, normalisation, params=None, device="cuda", seed=0):
+        self.device = torch.device(device)
+        self.lib = _lib_handle()
+        self.norm = normalisation
+        self._norm_struct = normalisation.struct()
+        p = initial_parameters(seed) if params is None else np.asarray(params, np.float32)
+        self.params = torch.as_tensor(p, device=self.device).clone()
+        self.grads = torch.zeros(PARAMS, dtype=torch.float32, device=self.device)
+        self.m = torch.zeros_like(self.grads)
+        self.v = torch.zeros_like(self.grads)
+        self.step = 0
+        self.packed = torch.zeros(PACKED_BYTES, dtype=torch.uint8, device=self.device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.loss_sum = torch.zeros(1, dtype=torch.float64, device=self.device)
+        self.pack()
+
+    def pack(self):
+        _call(self.lib, "bk_mlp_pack", self.params.data_ptr(), self.packed.data_ptr(), _lib.stream_handle())
+
+    @staticmethod
+    def _rows8(x):
+        x = torch.as_tensor(x, dtype=torch.float32)
+        out = torch.zeros(x.shape[0], 8 if x.shape[1] <= 8 else x.shape[1], dtype=torch.float32, device=x.device)
+        out[:, :x.shape[1]] = x
+        return out.contiguous()
+
+    def infer(self, features):
+        """Predicted return (n, 3) for raw features (n, 7) on the device, via the tensor cores."""
+        f = self._rows8(features.to(self.device))
+        n = f.shape[0]
+        out = torch.empty(n, 4, dtype=torch.float32, device=self.device)
+        self.status.zero_()
+        _call(self.lib, "bk_mlp_infer", n, f.data_ptr(), C.byref(self._norm_struct), self.packed.data_ptr(),
+              out.data_ptr(), self.status.data_ptr(), _lib.stream_handle())
+        if int(self.status.item()) != 0:
+            raise RuntimeError("bk_mlp_infer: a tensor-core completion wait gave up")
+        return out[:, :OUTPUTS]
+
+    def gradient(self, features, targets, accumulate=False):
+        """Loss gradient of one batch into self.grads; returns the batch's mean squared error (device)."""
+        f = self._rows8(features.to(self.device))
+        t = torch.zeros(f.shape[0], 4, dtype=torch.float32, device=self.device)
+        t[:, :OUTPUTS] = torch.as_tensor(targets, dtype=torch.float32, device=self.device)[:, :OUTPUTS]
+        if not accumulate:
+            self.grads.zero_()
+        self.loss_sum.zero_()
+        _call(self.lib, "bk_mlp_gradient", f.shape[0], f.data_ptr(), t.data_ptr(), C.byref(self._norm_struct),
+              self.params.data_ptr(), self.grads.data_ptr(), self.loss_sum.data_ptr(), _lib.stream_handle())
+        return self.loss_sum / (f.shape[0] * OUTPUTS)
+
+    def adam(self, lr, beta1=0.9, beta2=0.999, eps=1e-8):
+        self.step += 1
+        _call(self.lib, "bk_mlp_adam", self.grads.data_ptr(), self.params.data_ptr(), self.m.data_ptr(),
+              self.v.data_ptr(), self.step, lr, beta1, beta2, eps, _lib.stream_handle())
+
+    def train(self, features, targets, epochs=10, batch=8192, lr=2e-3, lr_final=1e-4, seed=0, log=None):
+        """Adam on the mean squared error (units of out_scale) with a cosine learning-rate decay.
+        ``features``/``targets`` are device tensors (n, 7) / (n, 3). Returns the per-epoch mean losses."""
+        f = self._rows8(features.to(self.device))
+        t = torch.as_tensor(targets, dtype=torch.float32, device=self.device)
+        n = f.shape[0]
+        g = torch.Generator(device=self.device).manual_seed(seed)
+        steps_per_epoch = max(1, n // batch)
+        total = epochs * steps_per_epoch
+        history = []
+        k = 0
+        for epoch in range(epochs):
+            order = torch.randperm(n, device=self.device, generator=g)
+            acc = torch.zeros((), dtype=torch.float64, device=self.device)
+            for s in range(steps_per_epoch):
+                idx = order[s * batch:(s + 1) * batch]
+                acc += self.gradient(f[idx], t[idx])[0]
+                rate = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / max(1, total - 1)))
+                self.adam(float(rate))
+                k += 1
+            history.append(float(acc) / steps_per_epoch)
+            if log:
+                log(epoch, history[-1])
+        self.pack()
+        return history
+
+    def state_dict(self):
+        n = self.norm
+        return dict(params=self.params.cpu().numpy(), in_mean=n.in_mean, in_scale=n.in_scale, out_scale=n.out_scale,
+                    in_low=n.in_low, in_high=n.in_high)
+
+    @classmethod
+    def from_state_dict(cls, d, device="cuda"):
+        norm = Normalisation(*(np.asarray(d[k], np.float32) for k in ("in_mean", "in_scale", "out_scale",
+                                                                        "in_low", "in_high")))
+        return cls(norm, params=d["params"], device=device)

@@ -329,6 +329,35 @@ BK_API int bk_substep_adjoint(const BkSubstepParams *params, const BkState *in, 
                               BkAdjointState *in_adjoint, float *node_v_adjoint, float *node_pm_adjoint,
                               double *parameter_adjoint, void *stream);
 
+/* ---- Return-map surrogate MLP (7 -> 64 -> 64 -> 3, SiLU; BF16 weights, FP32 accumulation) ----
+   The reference has no learned component; these entry points serve the surrogate that may replace
+   the Ding return map (ding.py:103-137 with porous_return.py:43-61) for in-distribution particles.
+   Parameters are an FP32 vector of BK_MLP_PARAMS values: W1[7][64], b1[64], W2[64][64], b2[64],
+   W3[64][3], b3[3] (input x output, row-major). Inference reads them packed by bk_mlp_pack into
+   BK_MLP_PACKED_BYTES bytes (16-byte aligned): BF16 tensor-core operands plus FP32 biases. */
+#define BK_MLP_PARAMS 4867
+#define BK_MLP_PACKED_BYTES 12864
+
+typedef struct BkMlpNorm {
+    float in_mean[8], in_scale[8];  /* network input k = (feature k - in_mean[k]) / in_scale[k], k < 7 */
+    float out_scale[4];             /* prediction k = network output k * out_scale[k], k < 3 */
+} BkMlpNorm;
+
+/* outputs[i*4 + k] (k < 3) for the raw features[i*8 + k] (k < 7), on the tensor cores. *status
+   (device) is set to 1 if a tensor-core completion wait gave up. */
+BK_API int bk_mlp_infer(int64_t n, const float *features, const BkMlpNorm *norm, const void *packed,
+                        float *outputs, int32_t *status, void *stream);
+/* grads += dL/dparams of L = mean over the batch and the 3 outputs of (prediction/out_scale -
+   target/out_scale)^2, with the forward rounded like inference (BF16 inputs, weights and hidden
+   activations; FP32 accumulation); *loss_sum (device, may be NULL) += sum of squared errors. */
+BK_API int bk_mlp_gradient(int64_t batch, const float *features, const float *targets, const BkMlpNorm *norm,
+                           const float *params, float *grads, double *loss_sum, void *stream);
+/* One Adam step (bias-corrected, `step` >= 1) on the parameter vector. */
+BK_API int bk_mlp_adam(const float *grads, float *params, float *first_moment, float *second_moment, int32_t step,
+                       float learning_rate, float beta1, float beta2, float epsilon, void *stream);
+/* FP32 parameters -> packed BF16 operands + FP32 biases for bk_mlp_infer and the fused substep. */
+BK_API int bk_mlp_pack(const float *params, void *packed, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

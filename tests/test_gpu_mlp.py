@@ -1,0 +1,83 @@
+"""Surrogate MLP kernels on the device against the CPU oracle (oracle/mlp.py): packed operands
+byte for byte, tensor-core inference, the fused training gradient, and one Adam step."""
+import numpy as np
+import pytest
+
+from oracle import mlp as omlp
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(n=1000, seed=0):
+    import torch
+    from baking_b200.surrogate import Normalisation, ReturnMapMlp
+    rng = np.random.default_rng(seed)
+    feats = rng.standard_normal((n, 7)).astype(np.float32) * np.array([0.02, 0.01, 0.03, 30, 0.2, 5, 0.1],
+                                                                      np.float32) \
+        + np.array([0.01, 0.0, -0.01, 320, 0.4, 10, 0.05], np.float32)
+    targets = rng.standard_normal((n, 3)).astype(np.float32) * 0.01
+    norm = Normalisation.fit(feats, targets)
+    params = omlp.init_params(seed + 1)
+    params[omlp.P_B1:omlp.P_W2] = 0.1 * rng.standard_normal(64)
+    params[omlp.P_B2:omlp.P_W3] = 0.1 * rng.standard_normal(64)
+    params[omlp.P_B3:] = 0.1 * rng.standard_normal(3)
+    net = ReturnMapMlp(norm, params=params)
+    return torch, net, norm, params, feats, targets
+
+
+def test_pack_matches_oracle_bytes():
+    torch, net, norm, params, _, _ = _setup()
+    np.testing.assert_array_equal(net.packed.cpu().numpy(), omlp.pack(params))
+
+
+@pytest.mark.parametrize("n", [1, 127, 128, 1000, 300_000])
+def test_tensor_core_inference_matches_oracle(n):
+    torch, net, norm, params, feats, _ = _setup(n=max(n, 1))
+    out = net.infer(torch.as_tensor(feats[:n], device="cuda")).cpu().numpy()
+    x = omlp.normalise(feats[:n], norm.in_mean, norm.in_scale)
+    ref = omlp.forward(params, x) * norm.out_scale
+    scale = np.abs(ref).max()
+    # BF16 hidden activations may round differently where FP32 sums differ in their last bits.
+    np.testing.assert_allclose(out, ref, rtol=0, atol=2e-3 * scale)
+    assert np.abs(out - ref).mean() < 2e-4 * scale
+
+
+def test_training_gradient_matches_oracle():
+    torch, net, norm, params, feats, targets = _setup(n=1000)
+    loss = float(net.gradient(torch.as_tensor(feats, device="cuda"), torch.as_tensor(targets, device="cuda"))[0])
+    g = net.grads.cpu().numpy().astype(np.float64)
+    x = omlp.normalise(feats, norm.in_mean, norm.in_scale)
+    ref_loss, ref_g = omlp.loss_and_gradient(params, x, targets / norm.out_scale)
+    np.testing.assert_allclose(loss, ref_loss, rtol=1e-4)
+    err = np.linalg.norm(g - ref_g) / np.linalg.norm(ref_g)
+    assert err < 1e-3, err
+    for name, a, b in (("W1", omlp.P_W1, omlp.P_B1), ("W2", omlp.P_W2, omlp.P_B2), ("W3", omlp.P_W3, omlp.P_B3)):
+        e = np.linalg.norm(g[a:b] - ref_g[a:b]) / np.linalg.norm(ref_g[a:b])
+        assert e < 2e-3, (name, e)
+
+
+def test_adam_step_matches_oracle():
+    torch, net, norm, params, feats, targets = _setup(n=512)
+    net.gradient(torch.as_tensor(feats, device="cuda"), torch.as_tensor(targets, device="cuda"))
+    g = net.grads.cpu().numpy()
+    net.adam(1e-3)
+    ref, m, v = omlp.adam(params.astype(np.float64), g.astype(np.float64), np.zeros(omlp.PARAMS), np.zeros(omlp.PARAMS),
+                          1, 1e-3)
+    np.testing.assert_allclose(net.params.cpu().numpy(), ref, rtol=1e-5, atol=1e-7)
+    np.testing.assert_allclose(net.m.cpu().numpy(), m, rtol=1e-5, atol=1e-12)
+
+
+def test_training_reduces_the_loss_on_a_smooth_function():
+    """A few epochs of the device training fit a smooth map far better than the initial network."""
+    import torch
+    from baking_b200.surrogate import Normalisation, ReturnMapMlp
+    rng = np.random.default_rng(3)
+    f = rng.uniform(-1, 1, (65536, 7)).astype(np.float32)
+    t = np.stack([np.tanh(f[:, 0] + 0.5 * f[:, 1]), f[:, 2] * f[:, 3], np.sin(f[:, 4]) * f[:, 6]], 1).astype(np.float32)
+    net = ReturnMapMlp(Normalisation.fit(f, t))
+    ft, tt = torch.as_tensor(f, device="cuda"), torch.as_tensor(t, device="cuda")
+    history = net.train(ft, tt, epochs=20, batch=1024, lr=3e-3)
+    assert history[-1] < 0.02 * history[0], history
+    pred = net.infer(ft).cpu().numpy()
+    rel = np.sqrt(((pred - t) ** 2).mean(0)) / np.sqrt((t ** 2).mean(0))
+    assert rel.max() < 0.08, rel  # BF16 hidden activations bound the attainable accuracy
