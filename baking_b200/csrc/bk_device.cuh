@@ -575,6 +575,8 @@ BK_DEV float solve_porosity(float q, float p, float d, float h, float e, double 
 struct DingOut {
     M3 Fe, tau;
     float residual;
+    float e[3];     // returned log principal strains before the isochoric correction (exponents of Fe)
+    bool yielded;   // q^2 + p^2 > 1: the overstress solve ran
 };
 
 // Ding return map (ding.py:103-137) given the SVD of the trial gradient (float32 factors).
@@ -600,9 +602,12 @@ BK_DEV DingOut ding_return(const M3& trial, const M3& Um, const float* s, const 
     for (int k = 0; k < 3; ++k) cs[k] = dev[k] / (1.0f + df * r) + mean / (1.0f + mf * r);
     float cm = (cs[0] + cs[1] + cs[2]) / 3.0f;
     float ex[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) ex[k] = expf((cs[k] - cm) / (2.0f * mu) + cm / (2.0f * mu + 3.0f * lam));
     DingOut o;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        o.e[k] = (cs[k] - cm) / (2.0f * mu) + cm / (2.0f * mu + 3.0f * lam);
+        ex[k] = expf(o.e[k]);
+    }
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -619,7 +624,8 @@ BK_DEV DingOut ding_return(const M3& trial, const M3& Um, const float* s, const 
         for (int e = 0; e < 9; ++e) o.Fe.m[e] *= scale;
     }
     o.residual = 0.0f;
-    if (q2 + p2 > 1.0f) {
+    o.yielded = q2 + p2 > 1.0f;
+    if (o.yielded) {
         float u = 1.0f + df * r, w = 1.0f + mf * r;
         o.residual = fabsf(r + 1.0f - q2 / (u * u) - p2 / (w * w));
     }
@@ -636,14 +642,21 @@ struct DingParticleOut {
     M3 Fe, Fp, tau;
     float residual, porosity, porosity_residual, yield_stress, viscosity;
     int gelled;
+    float e[3];     // returned log principal strains, before volume corrections (SVD order)
+    bool yielded;
 };
 
-// UpdateDing for one particle (ding.py:154-221). Returns false when the old porosity is
-// outside [0, 1) (flag 0 set, nothing written, as in the reference). Fp = Fe^-1 F is formed
-// only when `need_fp` or when the porosity update needs it (uncoupled mode).
-BK_DEV bool update_ding_particle(const DingParamsDev& P, const M3& Fe_old, float por, int gel, const M3& F_tot,
-                                 const M3& C_new, float T, float eta_base, int32_t* flags, DingParticleOut& out,
-                                 bool need_fp = true) {
+// The part of UpdateDing (ding.py:154-180) before the return: gelation latch, temperature tables,
+// trial gradient and its SVD.
+struct DingPrelude {
+    M3 trial, U, V;
+    float s[3];
+    float ty, eta, T_eff;
+    int gel;
+};
+
+BK_DEV bool ding_prelude(const DingParamsDev& P, const M3& Fe_old, float por, int gel, const M3& C_new, float T,
+                         float eta_base, int32_t* flags, DingPrelude& d) {
     if (!isfinite(por) || por < 0.0f || por >= 1.0f) { set_flag(flags, 0); return false; }
     int reached = T >= P.knots[3];
     float Teff = T;
@@ -655,37 +668,23 @@ BK_DEV bool update_ding_particle(const DingParamsDev& P, const M3& Fe_old, float
         ty = P.yield_stress * temperature_factor(Teff, P.knots, P.yield_factors);
         eta = eta_base * temperature_factor(Teff, P.knots, P.viscosity_factors);
     }
-    const float dt = P.dt, mu = P.mu, lam = P.lam, n0 = P.initial_porosity;
-    M3 G = C_new;
+    M3 G;
 #pragma unroll
-    for (int e = 0; e < 9; ++e) G.m[e] = dt * C_new.m[e] + ((e % 4) == 0 ? 1.0f : 0.0f);
-    M3 trial = matmul(G, Fe_old);
-    M3 Ud, Vd;
-    float sd[3];
-    svd3f(trial, Ud, sd, Vd);
-    float ret_por = por, consistency = 0.0f;
-    if (P.coupled_porosity) {
-        float st[3] = {logf(sd[0]), logf(sd[1]), logf(sd[2])};
-        float tr = st[0] + st[1] + st[2];
-        float ts[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) ts[k] = 2.0f * mu * st[k] + lam * tr;
-        float mean = (ts[0] + ts[1] + ts[2]) / 3.0f;
-        float dev[3] = {ts[0] - mean, ts[1] - mean, ts[2] - mean};
-        float ty2 = ty * ty;
-        float qv = 1.5f * (dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]) / ty2;
-        float pv = mean * mean / ty2;
-        float df = 6.0f * mu * dt * ty * ty / eta;
-        float ms = 2.0f / 3.0f * (2.0f * mu + 3.0f * lam) * dt * ty * ty / eta;
-        float ex = 3.0f * mean / (2.0f * mu + 3.0f * lam);
-        double Vp = 1.0 - (double)n0 + (double)por;
-        ret_por = solve_porosity(qv, pv, df, ms, ex, Vp, n0);
-        double pred = porosity_prediction((double)ret_por, qv, pv, df, ms, ex, Vp, n0);
-        consistency = (float)fabs((double)ret_por - pred);
-        if (consistency > 1.0e-6f || ret_por <= 0.0f || ret_por >= 1.0f) set_flag(flags, 1);
-    }
-    DingOut d = ding_return(trial, Ud, sd, Vd, mu, lam, ty, eta, porosity_coefficient(ret_por), dt);
-    M3 Fe = d.Fe;
+    for (int e = 0; e < 9; ++e) G.m[e] = P.dt * C_new.m[e] + ((e % 4) == 0 ? 1.0f : 0.0f);
+    d.trial = matmul(G, Fe_old);
+    svd3f(d.trial, d.U, d.s, d.V);
+    d.ty = ty;
+    d.eta = eta;
+    d.T_eff = Teff;
+    d.gel = gel;
+    return true;
+}
+
+// Volume correction (gas mode), plastic gradient and porosity update shared by the exact and the
+// surrogate returns (ding.py:200-221).
+BK_DEV void ding_close(const DingParamsDev& P, float por, const M3& F_tot, float ret_por, M3 Fe, int32_t* flags,
+                       DingParticleOut& out, bool need_fp) {
+    const float n0 = P.initial_porosity;
     if (P.coupled_porosity) {
         double target = 1.0 - (double)n0 + (double)ret_por;
         M3d Fd, Fed;
@@ -709,13 +708,57 @@ BK_DEV bool update_ding_particle(const DingParamsDev& P, const M3& Fe_old, float
     if (!isfinite(npor) || npor < 0.0f || npor >= 1.0f) set_flag(flags, 0);
     out.Fe = Fe;
     out.Fp = Fp;
-    out.tau = d.tau;
-    out.residual = d.residual;
     out.porosity = npor;
+}
+
+// The exact return of UpdateDing after the prelude (ding.py:181-221).
+BK_DEV void ding_exact(const DingParamsDev& P, const DingPrelude& d, float por, const M3& F_tot, int32_t* flags,
+                       DingParticleOut& out, bool need_fp) {
+    const float dt = P.dt, mu = P.mu, lam = P.lam, n0 = P.initial_porosity;
+    const float ty = d.ty, eta = d.eta;
+    float ret_por = por, consistency = 0.0f;
+    if (P.coupled_porosity) {
+        float st[3] = {logf(d.s[0]), logf(d.s[1]), logf(d.s[2])};
+        float tr = st[0] + st[1] + st[2];
+        float ts[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) ts[k] = 2.0f * mu * st[k] + lam * tr;
+        float mean = (ts[0] + ts[1] + ts[2]) / 3.0f;
+        float dev[3] = {ts[0] - mean, ts[1] - mean, ts[2] - mean};
+        float ty2 = ty * ty;
+        float qv = 1.5f * (dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]) / ty2;
+        float pv = mean * mean / ty2;
+        float df = 6.0f * mu * dt * ty * ty / eta;
+        float ms = 2.0f / 3.0f * (2.0f * mu + 3.0f * lam) * dt * ty * ty / eta;
+        float ex = 3.0f * mean / (2.0f * mu + 3.0f * lam);
+        double Vp = 1.0 - (double)n0 + (double)por;
+        ret_por = solve_porosity(qv, pv, df, ms, ex, Vp, n0);
+        double pred = porosity_prediction((double)ret_por, qv, pv, df, ms, ex, Vp, n0);
+        consistency = (float)fabs((double)ret_por - pred);
+        if (consistency > 1.0e-6f || ret_por <= 0.0f || ret_por >= 1.0f) set_flag(flags, 1);
+    }
+    DingOut r = ding_return(d.trial, d.U, d.s, d.V, mu, lam, ty, eta, porosity_coefficient(ret_por), dt);
+    ding_close(P, por, F_tot, ret_por, r.Fe, flags, out, need_fp);
+    out.tau = r.tau;
+    out.residual = r.residual;
     out.porosity_residual = consistency;
     out.yield_stress = ty;
     out.viscosity = eta;
-    out.gelled = gel;
+    out.gelled = d.gel;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out.e[k] = r.e[k];
+    out.yielded = r.yielded;
+}
+
+// UpdateDing for one particle (ding.py:154-221). Returns false when the old porosity is
+// outside [0, 1) (flag 0 set, nothing written, as in the reference). Fp = Fe^-1 F is formed
+// only when `need_fp` or when the porosity update needs it (uncoupled mode).
+BK_DEV bool update_ding_particle(const DingParamsDev& P, const M3& Fe_old, float por, int gel, const M3& F_tot,
+                                 const M3& C_new, float T, float eta_base, int32_t* flags, DingParticleOut& out,
+                                 bool need_fp = true) {
+    DingPrelude d;
+    if (!ding_prelude(P, Fe_old, por, gel, C_new, T, eta_base, flags, d)) return false;
+    ding_exact(P, d, por, F_tot, flags, out, need_fp);
     return true;
 }
 

@@ -205,7 +205,7 @@ __device__ __forceinline__ bool tile_layer(TileSmem& s, int w_off, int K, int N,
 // `active` is false, which writes a zero row). On return `y` holds the kOutputs outputs. `phase`
 // counts the mbarrier completions of this CTA (3 per call). Returns false if a tensor-core wait
 // gave up (outputs then undefined; the caller falls back).
-__device__ bool tile_eval(TileSmem& s, const float* x, bool active, float* y, uint32_t& phase) {
+__device__ inline bool tile_eval(TileSmem& s, const float* x, bool active, float* y, uint32_t& phase) {
     const int row = threadIdx.x;
     const uint32_t lane_base = s.tmem_base + ((uint32_t)(row & ~31) << 16);
     {

@@ -29,6 +29,7 @@
 #include "baking_b200.h"
 #include "bk_common.h"
 #include "bk_device.cuh"
+#include "bk_mlp.cuh"
 #include "bk_profile.h"
 
 using namespace bk;
@@ -663,24 +664,17 @@ __device__ __forceinline__ void atomic_max_nonneg(float* addr, float value) {
     if (value > 0.0f) atomicMax(reinterpret_cast<int*>(addr), __float_as_int(value));
 }
 
-// 6 blocks of 128 threads per SM (80 registers): the float64 steps of the return map are latency
-// bound, so the extra resident warps outweigh a few spilled registers.
-__global__ void __launch_bounds__(128, 6) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
-                                                   BkDiagnostics diag, BkFlags flags) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (blockIdx.x == 0 && threadIdx.x < 6) {
-        // This substep's box becomes the box the next substep clears; the active box restarts empty.
-        g.bounds[6 + threadIdx.x] = g.bounds[threadIdx.x];
-        g.bounds[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
-    }
-    if (i >= P.n) return;
+// G2P of one particle (transfer.py:73-109): writes x', v', C', F' and returns F', C'. False (and the
+// stencil flag) when the stencil leaves the grid.
+// v = sum w v_i and C = 4/dx^2 sum w v_i (o_i - l) dx, accumulated as the moments
+// S = sum w v_i and M_c = sum w v_i o_ic with the stencil offsets o_i in {0, 1, 2} known at compile
+// time; C_rc = 4/dx (M_rc - l_c S_r).
+__device__ __forceinline__ bool g2p_gather(const Params& P, const BkState& in, const BkState& out, const GridPtrs& g,
+                                           const BkFlags& flags, int64_t i, M3& Fn, M3& Cn) {
     const int64_t pitch = P.pitch;
     V3 xi = load_v3(in.x, i, pitch);
     Stencil st = make_stencil(xi, P.origin, P.dx, P.R);
-    if (!st.valid) { set_flag(flags.simulation, 1); return; }
-    // v = sum w v_i and C = 4/dx^2 sum w v_i (o_i - l) dx, accumulated as the moments
-    // S = sum w v_i and M_c = sum w v_i o_ic with the stencil offsets o_i in {0, 1, 2} known at compile
-    // time; C_rc = 4/dx (M_rc - l_c S_r).
+    if (!st.valid) { set_flag(flags.simulation, 1); return false; }
     float nv[3] = {0.f, 0.f, 0.f}, mo[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     const float4* vbase = g.v + node_index(st.b[0], st.b[1], st.b[2], P.R);
     const int64_t R = P.R;
@@ -710,24 +704,24 @@ __global__ void __launch_bounds__(128, 6) k_g2p_return(Params P, BkState in, BkS
 #pragma unroll
         for (int c = 0; c < 3; ++c) nc[3 * r + c] = kdx * (mo[3 * r + c] - st.l[c] * nv[r]);
     M3 F = load_m3(in.F, i, pitch);
-    M3 G, Cn;
+    M3 G;
 #pragma unroll
     for (int e = 0; e < 9; ++e) {
         Cn.m[e] = nc[e];
         G.m[e] = P.dt * nc[e] + ((e % 4) == 0 ? 1.0f : 0.0f);
     }
-    M3 Fn = matmul(G, F);
+    Fn = matmul(G, F);
     V3 vo{{nv[0], nv[1], nv[2]}}, xo{{xi.v[0] + P.dt * nv[0], xi.v[1] + P.dt * nv[1], xi.v[2] + P.dt * nv[2]}};
     store_v3(out.v, i, pitch, vo);
     store_m3(out.C, i, pitch, Cn);
     store_v3(out.x, i, pitch, xo);
     store_m3(out.F, i, pitch, Fn);
-    if (P.material != 1) return;
-    float T = P.transport ? (float)out.temperature[i] : in.material_temperature[i];
-    DingParticleOut o;
-    if (!update_ding_particle(P.ding, load_m3(in.Fe, i, pitch), in.porosity[i], in.gelled[i], Fn, Cn, T,
-                              __ldg(cst.viscosity_parameter), flags.ding, o, diag.plastic_gradients != nullptr))
-        return;
+    return true;
+}
+
+__device__ __forceinline__ void ding_store(const Params& P, const BkState& out, const BkDiagnostics& diag, int64_t i,
+                                           float T, const DingParticleOut& o) {
+    const int64_t pitch = P.pitch;
     store_m3(out.Fe, i, pitch, o.Fe);
     store_m3(out.tau, i, pitch, o.tau);
     out.porosity[i] = o.porosity;
@@ -738,6 +732,256 @@ __global__ void __launch_bounds__(128, 6) k_g2p_return(Params P, BkState in, BkS
     if (diag.porosity_residuals) diag.porosity_residuals[i] = o.porosity_residual;
     atomic_max_nonneg(diag.max_residuals, o.residual);
     atomic_max_nonneg(diag.max_residuals + 1, o.porosity_residual);
+}
+
+// ------------------------------------------------------ return-map surrogate
+struct SurrogateDev {
+    const unsigned char* blob;
+    float in_mean[8], in_scale[8], in_low[8], in_high[8], out_scale[4];
+    float* samples;
+    int32_t* sample_count;
+    int sample_capacity, sample_stride, sample_offset;
+    float* judge_error;
+    int judge_stride;
+    int32_t* path_counts;
+};
+
+SurrogateDev surrogate_dev(const BkReturnSurrogate* r) {
+    SurrogateDev d{};
+    if (!r) return d;
+    d.blob = static_cast<const unsigned char*>(r->packed);
+    for (int k = 0; k < 8; ++k) {
+        d.in_mean[k] = r->norm.in_mean[k];
+        d.in_scale[k] = r->norm.in_scale[k] != 0.0f ? r->norm.in_scale[k] : 1.0f;
+        d.in_low[k] = r->in_low[k];
+        d.in_high[k] = r->in_high[k];
+    }
+    for (int k = 0; k < 4; ++k) d.out_scale[k] = r->norm.out_scale[k];
+    d.samples = r->samples;
+    d.sample_count = r->sample_count;
+    d.sample_capacity = r->sample_capacity;
+    d.sample_stride = r->sample_stride > 0 ? r->sample_stride : 1;
+    d.sample_offset = r->sample_offset;
+    d.judge_error = r->judge_error;
+    d.judge_stride = r->judge_stride;
+    d.path_counts = r->path_counts;
+    return d;
+}
+
+// a[k] for a runtime k in {0, 1, 2} without dynamic register indexing (which would move `a` to
+// local memory).
+__device__ __forceinline__ float sel3(const float* a, int k) { return k == 0 ? a[0] : (k == 1 ? a[1] : a[2]); }
+
+// Singular-value order (descending) the network sees.
+__device__ __forceinline__ void order3(const float* s, int* perm) {
+    int a = 0, b = 1, c = 2, t;
+    if (s[a] < s[b]) { t = a; a = b; b = t; }
+    if (s[b] < s[c]) { t = b; b = c; c = t; }
+    if (s[a] < s[b]) { t = a; a = b; b = t; }
+    perm[0] = a; perm[1] = b; perm[2] = c;
+}
+
+// The 7 raw network inputs of a particle: sorted log singular values of the trial elastic
+// gradient, effective temperature, water saturation, gas content, plastic volume strain.
+__device__ __forceinline__ void surrogate_features(const Params& P, const BkState& out, const BkConstants& cst,
+                                                   int64_t i, const DingPrelude& d, float por, float J,
+                                                   const int* perm, float* f) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) f[k] = logf(sel3(d.s, perm[k]));
+    f[3] = d.T_eff;
+    f[4] = P.transport ? (float)(out.water[i] / ((double)P.water_density * (double)cst.volume[i] * (double)J)) : 0.0f;
+    f[5] = P.gas ? (float)out.gas_moles[i] : 0.0f;
+    f[6] = logf(1.0f - P.ding.initial_porosity + por);
+}
+
+// True when the exact return map leaves the particle elastic (no overstress solve): the cheap
+// path for which the exact map runs unchanged.
+__device__ __forceinline__ bool ding_elastic(const DingParamsDev& D, const DingPrelude& d, float por) {
+    float st[3] = {logf(d.s[0]), logf(d.s[1]), logf(d.s[2])};
+    float tr = st[0] + st[1] + st[2];
+    float ts[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ts[k] = 2.0f * D.mu * st[k] + D.lam * tr;
+    float mean = (ts[0] + ts[1] + ts[2]) / 3.0f;
+    float dev[3] = {ts[0] - mean, ts[1] - mean, ts[2] - mean};
+    float ty2 = d.ty * d.ty;
+    float q = 1.5f * (dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]) / ty2;
+    float p = mean * mean / ty2;
+    if (D.coupled_porosity) {
+        // elastic trial porosity Vp - 1 + n0 with Vp = 1 - n0 + n, as in solve_porosity's early exit
+        double trial = 1.0 - (double)D.initial_porosity + (double)por - 1.0 + (double)D.initial_porosity;
+        if (trial > 0.0 && trial < 1.0) return (double)q + pressure_coefficient64(trial) * (double)p <= 1.0;
+        return false;
+    }
+    return q + porosity_coefficient(por) * p <= 1.0f;
+}
+
+// Close the return from predicted log principal strains e (SVD order, before volume corrections):
+// tau = U diag(2 mu dev(e) + K mean(e)) U^T, Fe = U exp(e) V^T; in gas mode the end-state porosity
+// is the plastic volume change Vp exp(tr eps_trial - tr e) - 1 + n0. False when that porosity
+// leaves (0, 1), in which case the caller runs the exact map.
+__device__ bool ding_surrogate(const DingParamsDev& D, const DingPrelude& d, float por, const M3& F_tot,
+                               const float* e, int32_t* flags, DingParticleOut& out, bool need_fp) {
+    const float mu = D.mu, bulk = 2.0f * D.mu + 3.0f * D.lam;
+    float ret_por = por;
+    if (D.coupled_porosity) {
+        double dv = (double)logf(d.s[0]) + (double)logf(d.s[1]) + (double)logf(d.s[2]) - ((double)e[0] + e[1] + e[2]);
+        double rp = (1.0 - (double)D.initial_porosity + (double)por) * exp(dv) - 1.0 + (double)D.initial_porosity;
+        if (!(rp > 0.0 && rp < 1.0)) return false;
+        ret_por = (float)rp;
+    }
+    const float eb = (e[0] + e[1] + e[2]) / 3.0f;
+    float cs[3], ex[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        cs[k] = 2.0f * mu * (e[k] - eb) + bulk * eb;
+        ex[k] = expf(e[k]);
+    }
+    const float* U = d.U.m;
+    const float* V = d.V.m;
+    M3 Fe, tau;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            Fe.m[3 * r + c] = (U[3 * r] * ex[0]) * V[3 * c] + (U[3 * r + 1] * ex[1]) * V[3 * c + 1] +
+                              (U[3 * r + 2] * ex[2]) * V[3 * c + 2];
+            tau.m[3 * r + c] = (U[3 * r] * cs[0]) * U[3 * c] + (U[3 * r + 1] * cs[1]) * U[3 * c + 1] +
+                               (U[3 * r + 2] * cs[2]) * U[3 * c + 2];
+        }
+    if (!D.coupled_porosity && porosity_coefficient(por) == 0.0f) {
+        float scale = cbrtf(det3(d.trial) / det3(Fe));
+#pragma unroll
+        for (int k = 0; k < 9; ++k) Fe.m[k] *= scale;
+    }
+    ding_close(D, por, F_tot, ret_por, Fe, flags, out, need_fp);
+    out.tau = tau;
+    out.residual = 0.0f;
+    out.porosity_residual = 0.0f;
+    out.yield_stress = d.ty;
+    out.viscosity = d.eta;
+    out.gelled = d.gel;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out.e[k] = e[k];
+    out.yielded = true;
+    return true;
+}
+
+// 6 blocks of 128 threads per SM (80 registers): the float64 steps of the return map are latency
+// bound, so the extra resident warps outweigh a few spilled registers. With `sg.samples` set
+// (harvest), yielding particles on the sampling stride append (features, return) rows.
+__global__ void __launch_bounds__(128, 6) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
+                                                   BkDiagnostics diag, BkFlags flags, SurrogateDev sg) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (blockIdx.x == 0 && threadIdx.x < 6) {
+        // This substep's box becomes the box the next substep clears; the active box restarts empty.
+        g.bounds[6 + threadIdx.x] = g.bounds[threadIdx.x];
+        g.bounds[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
+    }
+    if (i >= P.n) return;
+    M3 Fn, Cn;
+    if (!g2p_gather(P, in, out, g, flags, i, Fn, Cn)) return;
+    if (P.material != 1) return;
+    const int64_t pitch = P.pitch;
+    float T = P.transport ? (float)out.temperature[i] : in.material_temperature[i];
+    const float por = in.porosity[i];
+    DingPrelude d;
+    if (!ding_prelude(P.ding, load_m3(in.Fe, i, pitch), por, in.gelled[i], Cn, T, __ldg(cst.viscosity_parameter),
+                      flags.ding, d))
+        return;
+    DingParticleOut o;
+    ding_exact(P.ding, d, por, Fn, flags.ding, o, diag.plastic_gradients != nullptr);
+    ding_store(P, out, diag, i, T, o);
+    if (sg.samples && o.yielded && i % sg.sample_stride == sg.sample_offset) {
+        int slot = atomicAdd(sg.sample_count, 1);
+        if (slot < sg.sample_capacity) {
+            int perm[3];
+            order3(d.s, perm);
+            float f[7];
+            surrogate_features(P, out, cst, i, d, por, det3(Fn), perm, f);
+            float* row = sg.samples + (int64_t)slot * 12;
+#pragma unroll
+            for (int k = 0; k < 7; ++k) row[k] = f[k];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) row[7 + k] = sel3(o.e, perm[k]) - f[k];
+            row[10] = 0.0f;
+            row[11] = 0.0f;
+        }
+    }
+}
+
+// G2P + return map with the learned surrogate: each CTA evaluates the network for its 128
+// particles on the tensor cores (bk_mlp.cuh); yielding particles inside the training range take
+// the surrogate's return, all others (elastic, out of range, invalid porosity) the exact map.
+__global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkState in, BkState out, BkConstants cst,
+                                                             GridPtrs g, BkDiagnostics diag, BkFlags flags,
+                                                             SurrogateDev sg) {
+    __shared__ mlp::TileSmem ts;
+    __shared__ int s_counts[3];
+    mlp::tile_setup(ts, sg.blob);
+    if (threadIdx.x < 3) s_counts[threadIdx.x] = 0;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (blockIdx.x == 0 && threadIdx.x < 6) {
+        g.bounds[6 + threadIdx.x] = g.bounds[threadIdx.x];
+        g.bounds[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
+    }
+    const int64_t pitch = P.pitch;
+    M3 Fn, Cn;
+    bool ding = false, use_mlp = false;
+    DingPrelude d;
+    float T = 0.f, por = 0.f, x[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int perm[3] = {0, 1, 2};
+    if (i < P.n && g2p_gather(P, in, out, g, flags, i, Fn, Cn) && P.material == 1) {
+        T = P.transport ? (float)out.temperature[i] : in.material_temperature[i];
+        por = in.porosity[i];
+        ding = ding_prelude(P.ding, load_m3(in.Fe, i, pitch), por, in.gelled[i], Cn, T, __ldg(cst.viscosity_parameter),
+                            flags.ding, d);
+        if (ding && !ding_elastic(P.ding, d, por)) {
+            order3(d.s, perm);
+            float f[7];
+            surrogate_features(P, out, cst, i, d, por, det3(Fn), perm, f);
+            use_mlp = true;
+#pragma unroll
+            for (int k = 0; k < 7; ++k) {
+                use_mlp = use_mlp && f[k] >= sg.in_low[k] && f[k] <= sg.in_high[k];
+                x[k] = (f[k] - sg.in_mean[k]) / sg.in_scale[k];
+            }
+        }
+    }
+    __syncthreads();  // s_counts initialised before any thread adds to it
+    float y[3];
+    uint32_t phase = 0;
+    const bool tile_ok = mlp::tile_eval(ts, x, use_mlp, y, phase);
+    int path = -1;
+    if (ding) {
+        DingParticleOut o;
+        bool done = false;
+        if (use_mlp && tile_ok) {
+            // y is in the sorted order: singular value j has rank r_j with perm[r_j] = j.
+            float e[3];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const int r = perm[0] == j ? 0 : (perm[1] == j ? 1 : 2);
+                e[j] = logf(d.s[j]) + sel3(y, r) * sel3(sg.out_scale, r);
+            }
+            done = ding_surrogate(P.ding, d, por, Fn, e, flags.ding, o, diag.plastic_gradients != nullptr);
+            if (done && sg.judge_error && sg.judge_stride > 0 && i % sg.judge_stride == 0) {
+                DingParticleOut ex;
+                int32_t scratch[3] = {0, 0, 0};
+                ding_exact(P.ding, d, por, Fn, scratch, ex, false);
+                float err = 0.f;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) err = fmaxf(err, fabsf(ex.e[k] - e[k]));
+                atomic_max_nonneg(sg.judge_error, err);
+            }
+        }
+        if (!done) ding_exact(P.ding, d, por, Fn, flags.ding, o, diag.plastic_gradients != nullptr);
+        path = done ? 1 : (o.yielded ? 2 : 0);
+        ding_store(P, out, diag, i, T, o);
+    }
+    if (sg.path_counts && path >= 0) atomicAdd(&s_counts[path], 1);
+    mlp::tile_teardown(ts);
+    if (sg.path_counts && threadIdx.x < 3 && s_counts[threadIdx.x]) atomicAdd(sg.path_counts + threadIdx.x, s_counts[threadIdx.x]);
 }
 
 // ------------------------------------------------------------ materialize
@@ -888,9 +1132,15 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
             profile_end(rec, s);
         }
         if (int rc = check_launch("bk_substep/grid_update")) return rc;
-        {
+        const SurrogateDev sg = surrogate_dev(p.surrogate);
+        if (sg.blob && p.material == 1) {
+            int rec = profile_begin("g2p_return_surrogate", s);
+            k_g2p_return_surrogate<<<blocks_for(p.n, 128), 128, 0, s>>>(P, *in, *out, *constants, g, *diagnostics,
+                                                                     *flags, sg);
+            profile_end(rec, s);
+        } else {
             int rec = profile_begin("g2p_return", s);
-            k_g2p_return<<<blocks_for(p.n, 128), 128, 0, s>>>(P, *in, *out, *constants, g, *diagnostics, *flags);
+            k_g2p_return<<<blocks_for(p.n, 128), 128, 0, s>>>(P, *in, *out, *constants, g, *diagnostics, *flags, sg);
             profile_end(rec, s);
         }
         if (int rc = check_launch("bk_substep/g2p_return")) return rc;

@@ -13,6 +13,7 @@ import numpy as np
 import torch
 
 from .. import _lib, arrays
+from ..surrogate import BkMlpNorm
 from .materials.ding import DingMaterial, ding_params
 from .thermal_water import scalar_params
 
@@ -49,6 +50,12 @@ class BkFlags(C.Structure):
     _fields_ = [("simulation", P), ("ding", P), ("transport", P)]
 
 
+class BkReturnSurrogate(C.Structure):
+    _fields_ = [("packed", P), ("norm", BkMlpNorm), ("in_low", C.c_float * 8), ("in_high", C.c_float * 8),
+                ("samples", P), ("sample_count", P), ("sample_capacity", C.c_int32), ("sample_stride", C.c_int32),
+                ("sample_offset", C.c_int32), ("judge_error", P), ("judge_stride", C.c_int32), ("path_counts", P)]
+
+
 class BkSubstepParams(C.Structure):
     _fields_ = [("n", C.c_int64), ("pitch", C.c_int64), ("resolution", C.c_int32), ("boundary_cells", C.c_int32),
                 ("origin", C.c_float * 3), ("spacing", C.c_float), ("time_step", C.c_float),
@@ -57,7 +64,7 @@ class BkSubstepParams(C.Structure):
                 ("conductivity", C.c_float), ("diffusivity", C.c_float), ("initial_saturation", C.c_float),
                 ("water_stress", C.c_float), ("gas_ambient_pressure", C.c_float), ("density", C.c_float),
                 ("elastic_modulus", C.c_float), ("cfl_limit", C.c_float), ("gas_peak", C.c_float),
-                ("gas_width", C.c_float)]
+                ("gas_width", C.c_float), ("surrogate", C.POINTER(BkReturnSurrogate))]
 
 
 PHASE_TRANSPORT = 1
@@ -134,6 +141,8 @@ class SubstepEngine:
         self.surface = BkSurface()
         if self.transport:
             self._build_surface()
+        # Return-map surrogate or sample harvest (BkReturnSurrogate), None for the exact map.
+        self.surrogate = None
         self.flags = BkFlags()
         self.flags.simulation = _p(sim.error_flags)
         self.flags.ding = _p(sim.material.error_flags) if self.is_ding else _p(sim.error_flags_ding_unused)
@@ -212,6 +221,8 @@ class SubstepEngine:
             d = sim.material.ding_config
             p.gas_ambient_pressure = d.gas_ambient_pressure_pa
             p.gas_peak, p.gas_width = d.gas_reaction_temperature_k, d.gas_reaction_width_k
+        if self.surrogate is not None:
+            p.surrogate = C.pointer(self.surrogate)
         return p
 
     def constants(self, settling):

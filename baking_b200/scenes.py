@@ -31,6 +31,9 @@ class Scene:
     transport: TransportConfig
     gas_source_rates: np.ndarray | None = None
     initial_velocity: tuple = (0.0, 0.0, 0.0)
+    # Initial elastic stretch (principal log strains along x, y, z) applied to F and Fe of every
+    # particle: a shaped, pre-stressed crumb. Zero for a stress-free start.
+    initial_log_strain: tuple = (0.0, 0.0, 0.0)
 
     @property
     def particle_count(self):
@@ -80,8 +83,12 @@ def _locate(points, origin, voxel, shape):
 
 
 def box_loaf(resolution=128, particle_count=1_000_000, seed=0, size=(0.4, 0.15, 0.2), gas=True,
-             time_step=5e-5, gas_rate_max=1e-3):
-    """Box loaf (x length, y height, z width) on the floor, ``particle_count`` jittered particles."""
+             time_step=5e-5, gas_rate_max=1e-3, initial_temperature=None, prestrain=0.0):
+    """Box loaf (x length, y height, z width) on the floor, ``particle_count`` jittered particles.
+    ``initial_temperature`` (K) starts the crumb part-baked (default: the transport default, 293.15 K;
+    at 318 K the temperature tables lower the yield stress to 0.425 of its base value).
+    ``prestrain`` a > 0 starts every particle with the isochoric elastic stretch
+    diag(exp(a/2), exp(-a), exp(a/2)) (compressed in y), which yields from the first substep."""
     dx = 1.0 / resolution
     voxel = 2 * dx
     nvox = np.maximum(1, np.round(np.asarray(size) / voxel).astype(np.int64))
@@ -111,9 +118,11 @@ def box_loaf(resolution=128, particle_count=1_000_000, seed=0, size=(0.4, 0.15, 
                   gravity=(0.0, -9.8, 0.0), boundary_cells=boundary_cells, device_name="cuda:0")
     material = MaterialConfig(density=density, model="ding2019")
     ding = DingConfig(porosity=0.2 if gas else 0.0, temperature_enabled=True, gas_enabled=gas)
-    transport = TransportConfig(enabled=True)
+    transport = TransportConfig(enabled=True) if initial_temperature is None else \
+        TransportConfig(enabled=True, initial_temperature_k=float(initial_temperature))
     rates = rng.uniform(0.0, gas_rate_max, particle_count).astype(np.float32) if gas else None
-    return Scene("box_loaf", mesh, samples, sim, material, ding, transport, rates)
+    strain = (0.5 * prestrain, -prestrain, 0.5 * prestrain)
+    return Scene("box_loaf", mesh, samples, sim, material, ding, transport, rates, initial_log_strain=strain)
 
 
 def jittered_sphere(resolution=64, per_axis=2, radius=0.1, center=(0.5, 0.5, 0.3), seed=0, time_step=1e-4):
@@ -173,4 +182,11 @@ def make_simulator(scene, engine="cuda", **kwargs):
               ding_config=scene.ding, transport_config=scene.transport, **kwargs)
     if scene.gas_source_rates is not None:
         sim.SetGasSourceRates(scene.gas_source_rates)
+    if any(scene.initial_log_strain):
+        import torch
+        stretch = np.diag(np.exp(np.asarray(scene.initial_log_strain, np.float64))).astype(np.float32)
+        st = sim.current_state
+        for target in (st.deformation_gradients, getattr(st.material_state, "elastic_gradients", None)):
+            if target is not None:
+                target.copy_(torch.as_tensor(stretch, device=target.device).expand(target.shape))
     return sim

@@ -191,3 +191,114 @@ class ReturnMapMlp:
         norm = Normalisation(*(np.asarray(d[k], np.float32) for k in ("in_mean", "in_scale", "out_scale",
                                                                         "in_low", "in_high")))
         return cls(norm, params=d["params"], device=device)
+
+
+def _surrogate_struct(net=None, samples=None, sample_count=None, stride=1, offset=0, judge_error=None,
+                      judge_stride=0, path_counts=None):
+    from .physics.substep import BkReturnSurrogate
+    s = BkReturnSurrogate()
+    if net is not None:
+        s.packed = net.packed.data_ptr()
+        s.norm = net.norm.struct()
+        s.in_low[:FEATURES] = [float(v) for v in net.norm.in_low]
+        s.in_high[:FEATURES] = [float(v) for v in net.norm.in_high]
+    if samples is not None:
+        s.samples = samples.data_ptr()
+        s.sample_count = sample_count.data_ptr()
+        s.sample_capacity = samples.shape[0]
+        s.sample_stride, s.sample_offset = int(stride), int(offset)
+    if judge_error is not None:
+        s.judge_error, s.judge_stride = judge_error.data_ptr(), int(judge_stride)
+    if path_counts is not None:
+        s.path_counts = path_counts.data_ptr()
+    return s
+
+
+def _engine(sim):
+    from .physics.materials.ding import DingMaterial
+    if not isinstance(sim.material, DingMaterial):
+        raise ValueError("the return-map surrogate needs the ding2019 material")
+    return sim._engine
+
+
+def RandomizeReturnInputs(sim, seed=0, strain=0.12, volume=0.03, temperature=(295.0, 345.0),
+                          porosity=(0.05, 0.45), water_scale=(0.25, 1.75), gas_scale=(0.2, 3.0)):
+    """Give every particle of ``sim``'s current state an independent random material state for
+    harvesting training pairs: elastic gradient Fe = R diag(exp(e)) R^T (random rotation, deviatoric
+    log strains of scale ``strain``, volumetric within +-``volume``), deformation gradient
+    F = Fe (1 - n0 + n)^(1/3), porosity n, temperature, water and gas content drawn from the given
+    ranges. The exact return map is then evaluated on a broad cover of its inputs."""
+    eng = _engine(sim)
+    st = sim.current_state
+    dev = sim.device
+    n = sim.particle_data.particle_count
+    g = torch.Generator(device=dev).manual_seed(int(seed))
+    q, _ = torch.linalg.qr(torch.randn(n, 3, 3, device=dev, generator=g, dtype=torch.float64))
+    q = q * torch.sign(torch.linalg.det(q))[:, None, None]
+    e = torch.randn(n, 3, device=dev, generator=g, dtype=torch.float64) * (strain / 2)
+    e = e - e.mean(1, keepdim=True) + (torch.rand(n, 1, device=dev, generator=g, dtype=torch.float64) * 2 - 1) * volume
+    Fe = q @ torch.diag_embed(torch.exp(e)) @ q.transpose(1, 2)
+    n0 = sim.material.ding_config.porosity
+    por = porosity[0] + (porosity[1] - porosity[0]) * torch.rand(n, device=dev, generator=g, dtype=torch.float64)
+    m = st.material_state
+    m.elastic_gradients.copy_(Fe)
+    st.deformation_gradients.copy_(Fe * torch.pow(1.0 - n0 + por, 1.0 / 3.0)[:, None, None])
+    m.porosities.copy_(por)
+    u = lambda lo, hi: lo + (hi - lo) * torch.rand(n, device=dev, generator=g, dtype=torch.float64)  # noqa: E731
+    T = u(*temperature)
+    m.temperatures.copy_(T)
+    if st.transport_state is not None:
+        st.transport_state.temperatures.copy_(T)
+        st.transport_state.water_masses.mul_(u(*water_scale))
+    if eng.gas:
+        m.gas_moles.mul_(u(*gas_scale))
+
+
+def HarvestReturnSamples(sim, steps, capacity, stride=1):
+    """Run ``steps`` substeps of ``sim`` on the exact return map, keeping up to ``capacity``
+    (features, return) pairs of yielding particles, every ``stride``-th particle (the sampled offset
+    rotates per substep). Returns device tensors (n, 7) and (n, 3) and the number of yielding
+    particle-substeps seen on the stride."""
+    eng = _engine(sim)
+    rows = torch.zeros(capacity, 12, dtype=torch.float32, device=sim.device)
+    count = torch.zeros(1, dtype=torch.int32, device=sim.device)
+    try:
+        for k in range(steps):
+            eng.surrogate = _surrogate_struct(samples=rows, sample_count=count, stride=stride, offset=k % stride)
+            sim.AdvanceUnchecked(1)
+    finally:
+        eng.surrogate = None
+    seen = int(count.item())
+    n = min(seen, capacity)
+    return rows[:n, :FEATURES].clone(), rows[:n, FEATURES:FEATURES + OUTPUTS].clone(), seen
+
+
+class ReturnMapSurrogate:
+    """A trained ``ReturnMapMlp`` attached to simulators: the fused G2P kernel then evaluates the
+    network on the tensor cores and returns yielding in-range particles with it."""
+
+    def __init__(self, net, judge_stride=0):
+        self.net = net
+        self.judge_stride = int(judge_stride)
+        self.path_counts = torch.zeros(3, dtype=torch.int32, device=net.device)
+        self.judge_error = torch.zeros(1, dtype=torch.float32, device=net.device)
+
+    def attach(self, sim):
+        eng = _engine(sim)
+        self.net.pack()
+        eng.surrogate = _surrogate_struct(net=self.net, judge_error=self.judge_error if self.judge_stride else None,
+                                          judge_stride=self.judge_stride, path_counts=self.path_counts)
+        return self
+
+    @staticmethod
+    def detach(sim):
+        _engine(sim).surrogate = None
+
+    def reset_statistics(self):
+        self.path_counts.zero_()
+        self.judge_error.zero_()
+
+    def statistics(self):
+        c = self.path_counts.tolist()
+        return dict(elastic=c[0], surrogate=c[1], exact_yielding=c[2],
+                    judge_max_log_strain_error=float(self.judge_error.item()) if self.judge_stride else None)

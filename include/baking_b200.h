@@ -247,6 +247,35 @@ typedef struct BkFlags {
     int32_t *transport;            /* [2]: heat bound, water bound (thermal_water.py:279) */
 } BkFlags;
 
+typedef struct BkMlpNorm {
+    float in_mean[8], in_scale[8];  /* network input k = (feature k - in_mean[k]) / in_scale[k], k < 7 */
+    float out_scale[4];             /* prediction k = network output k * out_scale[k], k < 3 */
+} BkMlpNorm;
+
+/* Learned return-map surrogate for the Ding model (no counterpart in the reference). Features of a
+   particle: the trial elastic gradient's log singular values (descending), the temperature after
+   the gelation latch, water saturation, gas content and log(1 - n0 + n); targets: the change of the
+   three log principal strains made by the return (before volume corrections), same order.
+   - packed != NULL: the surrogate replaces the return for yielding particles whose features lie in
+     [in_low, in_high]; elastic and out-of-range particles keep the exact map.
+   - packed == NULL, samples != NULL: exact map; yielding particles with index % sample_stride ==
+     sample_offset append rows of 12 floats (7 features, 3 targets, 2 zero) while
+     *sample_count < sample_capacity (*sample_count keeps counting past it).
+   judge_error (device, may be NULL): max |surrogate - exact| of the log strains over the particles
+   with index % judge_stride == 0. path_counts (device [3], may be NULL): += particles that took the
+   elastic, surrogate and exact-yielding paths. */
+typedef struct BkReturnSurrogate {
+    const void *packed;            /* bk_mlp_pack output (16-byte aligned) */
+    BkMlpNorm norm;
+    float in_low[8], in_high[8];
+    float *samples;
+    int32_t *sample_count;
+    int32_t sample_capacity, sample_stride, sample_offset;
+    float *judge_error;
+    int32_t judge_stride;
+    int32_t *path_counts;
+} BkReturnSurrogate;
+
 typedef struct BkSubstepParams {
     int64_t n, pitch;
     int32_t resolution, boundary_cells;
@@ -257,6 +286,7 @@ typedef struct BkSubstepParams {
     BkScalarParams scalar;
     float conductivity, diffusivity, initial_saturation, water_stress;
     float gas_ambient_pressure, density, elastic_modulus, cfl_limit, gas_peak, gas_width;
+    const BkReturnSurrogate *surrogate;  /* NULL: exact return map */
 } BkSubstepParams;
 
 #define BK_PHASE_TRANSPORT 1       /* surface terms, scalar P2G, diffusion */
@@ -338,10 +368,7 @@ BK_API int bk_substep_adjoint(const BkSubstepParams *params, const BkState *in, 
 #define BK_MLP_PARAMS 4867
 #define BK_MLP_PACKED_BYTES 12864
 
-typedef struct BkMlpNorm {
-    float in_mean[8], in_scale[8];  /* network input k = (feature k - in_mean[k]) / in_scale[k], k < 7 */
-    float out_scale[4];             /* prediction k = network output k * out_scale[k], k < 3 */
-} BkMlpNorm;
+/* BkMlpNorm is declared with BkReturnSurrogate above. */
 
 /* outputs[i*4 + k] (k < 3) for the raw features[i*8 + k] (k < 7), on the tensor cores. *status
    (device) is set to 1 if a tensor-core completion wait gave up. */

@@ -35,10 +35,12 @@ def test_library_exports_every_declared_symbol():
 
 def test_bindings_match_declared_arity():
     from baking_b200 import _lib
+    from baking_b200 import surrogate
     from baking_b200.physics import adjoint, substep
     funcs = declared_functions()
     bindings = dict(_lib.SIGNATURES)
     bindings.update(substep._SIGS)
+    bindings.update(surrogate.SIGNATURES)
     bindings["bk_substep_adjoint"] = adjoint._SIGNATURE
     for name, argtypes in bindings.items():
         assert name in funcs, f"{name} bound but not declared"
