@@ -965,7 +965,8 @@ __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkSta
                 e[j] = logf(d.s[j]) + sel3(y, r) * sel3(sg.out_scale, r);
             }
             done = ding_surrogate(P.ding, d, por, Fn, e, flags.ding, o, diag.plastic_gradients != nullptr);
-            if (done && sg.judge_error && sg.judge_stride > 0 && i % sg.judge_stride == 0) {
+            // Judged in whole warps, so that the exact map's cost falls on 1 warp in judge_stride.
+            if (done && sg.judge_error && sg.judge_stride > 0 && (i >> 5) % sg.judge_stride == 0) {
                 DingParticleOut ex;
                 int32_t scratch[3] = {0, 0, 0};
                 ding_exact(P.ding, d, por, Fn, scratch, ex, false);

@@ -221,37 +221,55 @@ def _engine(sim):
     return sim._engine
 
 
+def _random_rotations(n, generator, device):
+    """Uniform random rotations from unit quaternions (closed form, float64)."""
+    q = torch.randn(n, 4, device=device, generator=generator, dtype=torch.float64)
+    q = q / q.norm(dim=1, keepdim=True)
+    w, x, y, z = q.unbind(1)
+    return torch.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y),
+                        2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                        2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], 1).view(n, 3, 3)
+
+
 def RandomizeReturnInputs(sim, seed=0, strain=0.12, volume=0.03, temperature=(295.0, 345.0),
                           porosity=(0.05, 0.45), water_scale=(0.25, 1.75), gas_scale=(0.2, 3.0)):
     """Give every particle of ``sim``'s current state an independent random material state for
     harvesting training pairs: elastic gradient Fe = R diag(exp(e)) R^T (random rotation, deviatoric
     log strains of scale ``strain``, volumetric within +-``volume``), deformation gradient
-    F = Fe (1 - n0 + n)^(1/3), porosity n, temperature, water and gas content drawn from the given
-    ranges. The exact return map is then evaluated on a broad cover of its inputs."""
+    F = Fe (1 - n0 + n)^(1/3), porosity n, temperature, and water and gas content scaled from the
+    values the simulator held at its first randomisation. The exact return map is then evaluated on
+    a broad cover of its inputs."""
     eng = _engine(sim)
     st = sim.current_state
     dev = sim.device
     n = sim.particle_data.particle_count
+    m = st.material_state
+    base = sim._buffers.get("randomize_base")
+    if base is None:
+        base = dict(water=st.transport_state.water_masses.clone() if st.transport_state is not None else None,
+                    gas=m.gas_moles.clone() if eng.gas else None)
+        sim._buffers["randomize_base"] = base
     g = torch.Generator(device=dev).manual_seed(int(seed))
-    q, _ = torch.linalg.qr(torch.randn(n, 3, 3, device=dev, generator=g, dtype=torch.float64))
-    q = q * torch.sign(torch.linalg.det(q))[:, None, None]
+    q = _random_rotations(n, g, dev)
     e = torch.randn(n, 3, device=dev, generator=g, dtype=torch.float64) * (strain / 2)
     e = e - e.mean(1, keepdim=True) + (torch.rand(n, 1, device=dev, generator=g, dtype=torch.float64) * 2 - 1) * volume
     Fe = q @ torch.diag_embed(torch.exp(e)) @ q.transpose(1, 2)
     n0 = sim.material.ding_config.porosity
-    por = porosity[0] + (porosity[1] - porosity[0]) * torch.rand(n, device=dev, generator=g, dtype=torch.float64)
-    m = st.material_state
+    u = lambda lo, hi: lo + (hi - lo) * torch.rand(n, device=dev, generator=g, dtype=torch.float64)  # noqa: E731
+    por = u(*porosity)
     m.elastic_gradients.copy_(Fe)
     st.deformation_gradients.copy_(Fe * torch.pow(1.0 - n0 + por, 1.0 / 3.0)[:, None, None])
+    st.affine_velocities.zero_()
+    st.particle_velocities.zero_()
     m.porosities.copy_(por)
-    u = lambda lo, hi: lo + (hi - lo) * torch.rand(n, device=dev, generator=g, dtype=torch.float64)  # noqa: E731
+    m.gelled.zero_()
     T = u(*temperature)
     m.temperatures.copy_(T)
     if st.transport_state is not None:
         st.transport_state.temperatures.copy_(T)
-        st.transport_state.water_masses.mul_(u(*water_scale))
+        st.transport_state.water_masses.copy_(base["water"] * u(*water_scale))
     if eng.gas:
-        m.gas_moles.mul_(u(*gas_scale))
+        m.gas_moles.copy_(base["gas"] * u(*gas_scale))
 
 
 def HarvestReturnSamples(sim, steps, capacity, stride=1):
@@ -302,3 +320,69 @@ class ReturnMapSurrogate:
         c = self.path_counts.tolist()
         return dict(elastic=c[0], surrogate=c[1], exact_yielding=c[2],
                     judge_max_log_strain_error=float(self.judge_error.item()) if self.judge_stride else None)
+
+
+def BuildTrainingSet(sim, rounds=6, steps=3, capacity_per_round=3_000_000, seed=0):
+    """Harvest (features, return) pairs from ``rounds`` randomised material states of ``sim``
+    (RandomizeReturnInputs), ``steps`` exact substeps each; non-finite rows are dropped."""
+    feats, targs = [], []
+    for r in range(rounds):
+        RandomizeReturnInputs(sim, seed=seed + r)
+        f, t, _ = HarvestReturnSamples(sim, steps, capacity_per_round)
+        ok = torch.isfinite(f).all(1) & torch.isfinite(t).all(1)
+        feats.append(f[ok])
+        targs.append(t[ok])
+    return torch.cat(feats), torch.cat(targs)
+
+
+def TrainReturnSurrogate(features, targets, epochs=30, batch=8192, lr=3e-3, lr_final=3e-5, validation=0.05, seed=0):
+    """Fit a ReturnMapMlp on device tensors; returns (net, history, validation RMS error per output,
+    validation RMS of the targets)."""
+    g = torch.Generator(device=features.device).manual_seed(seed)
+    perm = torch.randperm(features.shape[0], device=features.device, generator=g)
+    nv = max(1, int(features.shape[0] * validation))
+    fv, tv = features[perm[:nv]], targets[perm[:nv]]
+    ft, tt = features[perm[nv:]], targets[perm[nv:]]
+    net = ReturnMapMlp(Normalisation.fit(ft.cpu().numpy(), tt.cpu().numpy()), device=features.device, seed=seed)
+    history = net.train(ft, tt, epochs=epochs, batch=batch, lr=lr, lr_final=lr_final, seed=seed)
+    err = (net.infer(fv) - tv).pow(2).mean(0).sqrt()
+    return net, history, err.tolist(), tv.pow(2).mean(0).sqrt().tolist()
+
+
+def SaveReturnSurrogate(net, path, **metadata):
+    np.savez(path, **net.state_dict(), **{k: np.asarray(v) for k, v in metadata.items()})
+
+
+def LoadReturnSurrogate(path, device="cuda"):
+    with np.load(path) as d:
+        return ReturnMapMlp.from_state_dict({k: d[k] for k in d.files}, device=device)
+
+
+def main(argv=None):
+    """Harvest from the randomised box loaf (1M particles, 128^3, Ding + gas + thermal-water) and
+    train the surrogate; writes the weights, normalisation and training range to ``--out``."""
+    import argparse
+    import time
+    from . import scenes
+    p = argparse.ArgumentParser(description=main.__doc__)
+    p.add_argument("--out", required=True)
+    p.add_argument("--particles", type=int, default=1_000_000)
+    p.add_argument("--rounds", type=int, default=6)
+    p.add_argument("--epochs", type=int, default=30)
+    p.add_argument("--seed", type=int, default=0)
+    a = p.parse_args(argv)
+    t0 = time.time()
+    scene = scenes.box_loaf(resolution=128, particle_count=a.particles, seed=a.seed, initial_temperature=318.15)
+    sim = scenes.make_simulator(scene, diagnostics="lean")
+    f, t = BuildTrainingSet(sim, rounds=a.rounds, seed=a.seed)
+    t1 = time.time()
+    net, history, err, rms = TrainReturnSurrogate(f, t, epochs=a.epochs, seed=a.seed)
+    t2 = time.time()
+    SaveReturnSurrogate(net, a.out, samples=f.shape[0], history=np.asarray(history), validation_rms_error=err,
+                        target_rms=rms)
+    print(f"samples {f.shape[0]} (harvest {t1 - t0:.1f} s), training {t2 - t1:.1f} s, validation RMS error {err} "
+          f"of target RMS {rms}", flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -262,7 +262,7 @@ typedef struct BkMlpNorm {
      sample_offset append rows of 12 floats (7 features, 3 targets, 2 zero) while
      *sample_count < sample_capacity (*sample_count keeps counting past it).
    judge_error (device, may be NULL): max |surrogate - exact| of the log strains over the particles
-   with index % judge_stride == 0. path_counts (device [3], may be NULL): += particles that took the
+   with (index / 32) % judge_stride == 0 (whole warps, so the exact map's cost stays on those). path_counts (device [3], may be NULL): += particles that took the
    elastic, surrogate and exact-yielding paths. */
 typedef struct BkReturnSurrogate {
     const void *packed;            /* bk_mlp_pack output (16-byte aligned) */
