@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--particles", type=int, default=1_000_000)
     p.add_argument("--resolution", type=int, default=128)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-variants", action="store_true", help="skip the surrogate and fwd+bwd forms")
     return p.parse_args()
 
 
@@ -290,6 +291,9 @@ def main():
                     "h2d_bytes_per_step": int(host_rates.numel() * 4), "d2h_bytes_per_step": int(result_bytes()),
                     "steps": e2e_steps},
             "clocks": clocks.summary()}
+    if not args.no_variants:
+        del sim
+        line["variants"] = variants(args, rank, dist)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(scene)
     if rank == 0:
@@ -301,6 +305,99 @@ def main():
 
 def result_bytes():
     return 2 * 8
+
+
+def _timed(fn, dist, stream):
+    """Device time of fn() between CUDA events on the launching stream, max over ranks."""
+    import torch
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    out = fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    t = a.elapsed_time(b) / 1e3
+    if dist:
+        tt = torch.tensor([t], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    return t, out
+
+
+def variants(args, rank, dist):
+    """The metric's other two forms at the same particle count and grid.
+
+    surrogate: the learned return map (committed weights) against the exact map on a loaf that yields
+    from its first substep (part-baked at 318 K, isochoric elastic prestrain 0.08), both timed over
+    the same substeps from the same state; the plain loaf of the headline never yields in the timed
+    window, so the surrogate has nothing to replace there.
+    fwd_bwd: forward + hand-written adjoint of 64 substeps with a checkpoint every 8 (Rollout) on the
+    loaf without transport or gas (the adjoint's scope), loss = mean squared distance of the final
+    positions to the initial cloud scaled by 1.2 about its centre, gradients with respect to the
+    per-particle velocities and temperatures and Young's modulus."""
+    import torch
+    from dataclasses import replace
+    from baking_b200.config import TransportConfig
+    from baking_b200.physics.adjoint import Rollout
+    from baking_b200.scenes import box_loaf, make_simulator
+    from baking_b200.surrogate import LoadReturnSurrogate, ReturnMapSurrogate
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    stream = torch.cuda.current_stream()
+    out = {}
+    steps = max(1, min(args.steps, 100))
+    loaf = box_loaf(args.resolution, args.particles, seed=rank, initial_temperature=318.15, prestrain=0.08)
+    n = loaf.particle_count
+    net = LoadReturnSurrogate(ROOT / "baking_b200" / "data" / "return_surrogate_box_loaf.npz")
+    results = {}
+    for mode in ("exact", "surrogate"):
+        sim = make_simulator(loaf, diagnostics="lean")
+        sur = ReturnMapSurrogate(net).attach(sim) if mode == "surrogate" else None
+        sim.AdvanceUnchecked(max(3, min(args.warmup, 10)))
+        if sur:
+            sur.reset_statistics()
+        t, _ = _timed(lambda: sim.AdvanceUnchecked(steps), dist, stream)
+        sim.CheckState()
+        results[mode] = (t, sim.current_state.particle_positions.double().clone(), sur.statistics() if sur else None)
+        del sim
+    (te, xe, _), (ts, xs, stats) = results["exact"], results["surrogate"]
+    x0 = torch.as_tensor(loaf.samples.particle_positions, device=xe.device)
+    moved = float((xe - x0).norm(dim=1).max())
+    dev = float((xs - xe).norm(dim=1).max())
+    out["surrogate"] = {"value": world * n * steps / ts, "unit": UNIT, "exact_same_scene": world * n * steps / te,
+                        "speedup": te / ts, "steps": steps, "paths": stats,
+                        "max_position_deviation_m": dev, "deviation_over_max_displacement": dev / moved,
+                        "scene": f"box loaf {n} particles, {args.resolution}^3, 318 K, prestrain 0.08, gas + transport"}
+    del results, xe, xs
+    # forward + backward
+    fb_steps, every = 64, 8
+    mech = replace(loaf, transport=TransportConfig(enabled=False), gas_source_rates=None,
+                   ding=replace(loaf.ding, gas_enabled=False), initial_log_strain=(0.0, 0.0, 0.0))
+    sim = make_simulator(mech, diagnostics="lean")
+    sim.AdvanceUnchecked(2)
+    st = sim.current_state
+    x0 = st.particle_positions.clone()
+    center = x0.mean(0)
+    target = 1.2 * (x0 - center) + center
+    v0 = st.particle_velocities.clone().requires_grad_(True)
+    T0 = st.material_state.temperatures.clone().requires_grad_(True)
+    E0 = torch.tensor([sim.material.material_config.young_modulus], device="cuda", requires_grad=True)
+
+    def fwd_bwd():
+        res = Rollout(sim, fb_steps, checkpoint_every=every, velocities=v0, temperatures=T0, young_modulus=E0)
+        loss = ((res["positions"] - target) ** 2).sum(1).mean()
+        loss.backward()
+        return loss
+
+    t_fb, _ = _timed(fwd_bwd, dist, stream)
+    t_f, _ = _timed(lambda: sim.AdvanceUnchecked(fb_steps), dist, stream)
+    out["fwd_bwd"] = {"value": world * n * fb_steps / t_fb, "unit": UNIT, "forward_only": world * n * fb_steps / t_f,
+                      "steps": fb_steps, "checkpoint_every": every,
+                      "finite_gradients": bool(torch.isfinite(v0.grad).all() and torch.isfinite(T0.grad).all()
+                                               and torch.isfinite(E0.grad).all()),
+                      "scene": f"box loaf {n} particles, {args.resolution}^3, Ding without transport/gas"}
+    return out
 
 
 if __name__ == "__main__":
