@@ -190,3 +190,42 @@ def make_simulator(scene, engine="cuda", **kwargs):
             if target is not None:
                 target.copy_(torch.as_tensor(stretch, device=target.device).expand(target.shape))
     return sim
+
+
+def dough_ball(resolution, particle_count, seed=0, oven_temperature=453.15, initial_temperature=318.15,
+               prestrain=0.0, time_step=5e-5, gas_rate_max=1e-3):
+    """A sphere of the box loaf's dough (Ding with temperature tables, porosity 0.2, gas, thermal-water
+    transport) centred in the unit cube with about ``particle_count`` jittered particles: the radius
+    and the particles per cell axis (2..8) are chosen so that the sphere fits within 0.3 of the centre."""
+    from dataclasses import replace as _replace
+    dx = 1.0 / resolution
+    per_axis, radius = 2, None
+    for per_axis in range(2, 9):
+        radius = (3.0 * particle_count / (4.0 * np.pi)) ** (1.0 / 3.0) / (resolution * per_axis)
+        if radius <= 0.3:
+            break
+    radius = min(radius, 0.3)
+    base = jittered_sphere(resolution, per_axis, radius, (0.5, 0.5, 0.5), seed, time_step)
+    rng = np.random.default_rng(seed + 7919)
+    n = len(base.samples.particle_positions)
+    transport = _replace(base.transport, oven_temperature_k=float(oven_temperature),
+                         tray_temperature_k=float(oven_temperature), initial_temperature_k=float(initial_temperature))
+    ding = DingConfig(porosity=0.2, temperature_enabled=True, gas_enabled=True)
+    rates = rng.uniform(0.0, gas_rate_max, n).astype(np.float32)
+    del dx
+    return _replace(base, name="dough_ball", ding=ding, transport=transport, gas_source_rates=rates,
+                    initial_log_strain=(0.5 * prestrain, -prestrain, 0.5 * prestrain))
+
+
+def dough_batch(count=64, seed=0, particles=(5_000, 200_000), resolutions=(32, 48, 64, 96),
+                oven_celsius=(150.0, 220.0), prestrain=(0.0, 0.0)):
+    """``count`` independent dough balls drawn from ``seed``: particle count uniform in ``particles``,
+    grid resolution from ``resolutions``, oven temperature uniform in ``oven_celsius``, isochoric
+    prestrain uniform in ``prestrain``."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        out.append(dough_ball(int(rng.choice(resolutions)), int(rng.integers(particles[0], particles[1] + 1)),
+                              seed=seed * 1000 + k, oven_temperature=273.15 + rng.uniform(*oven_celsius),
+                              prestrain=float(rng.uniform(*prestrain))))
+    return out
