@@ -453,8 +453,9 @@ BK_DEV float porosity_coefficient(float n) {
 // Iterates of this concave increasing residual approach the root monotonically from below;
 // once a step moves r by no more than a few float32 ulps the iteration has converged and the
 // reference's remaining steps only toggle the last bit, so it stops there.
-BK_DEV float solve_overstress(float q2, float p2, float d, float h) {
-    float r = 0.0f;
+BK_DEV float solve_overstress(float q2, float p2, float d, float h, float r0 = 0.0f) {
+    // r0 > 0 warm-starts the iteration (a root of a nearby problem); the same stopping test applies.
+    float r = r0 > 0.0f ? r0 : 0.0f;
     if (q2 + p2 > 1.0f) {
         for (int it = 0; it < 32; ++it) {
             float dd = 1.0f + d * r, md = 1.0f + h * r;
@@ -462,6 +463,7 @@ BK_DEV float solve_overstress(float q2, float p2, float d, float h) {
             float res = r + 1.0f - q2 / dd2 - p2 / md2;
             float der = 1.0f + 2.0f * d * q2 / (dd2 * dd) + 2.0f * h * p2 / (md2 * md);
             float rn = r - res / der;
+            if (rn < 0.0f) { r = 0.0f; continue; }  // see overstress64
             bool done = fabsf(rn - r) <= 2.4e-7f * fabsf(rn);
             r = rn;
             if (done) break;
@@ -480,8 +482,12 @@ BK_DEV double pressure_coefficient64(double n) {
     return c;
 }
 
-BK_DEV double overstress64(double q, double p, double d, double h) {
-    double r = 0.0;
+// `warm` (may be NULL): in, a root of a nearby problem to start from (0 starts at r = 0 like the
+// reference); out, this problem's root. Newton on this concave increasing residual converges to the
+// same root from either side, to the same |residual| < 1e-12 test.
+BK_DEV double overstress64(double q, double p, double d, double h, double* warm = nullptr) {
+    double r = (warm && *warm > 0.0) ? *warm : 0.0;
+    if (!(q + p > 1.0)) r = 0.0;
     if (q + p > 1.0) {
         for (int it = 0; it < 48; ++it) {
             double u = 1.0 + d * r, v = 1.0 + h * r;
@@ -489,15 +495,20 @@ BK_DEV double overstress64(double q, double p, double d, double h) {
             double res = r + 1.0 - q / u2 - p / v2;
             double der = 1.0 + 2.0 * d * q / (u2 * u) + 2.0 * h * p / (v2 * v);
             r -= res / der;
+            // From a warm start above the root a step can pass zero; restart from r = 0 (the
+            // iterates from 0 increase monotonically and never get here).
+            if (r < 0.0) { r = 0.0; continue; }
             if (fabs(res) < 1.0e-12) break;
         }
     }
+    if (warm) *warm = r;
     return r;
 }
 
-BK_DEV double porosity_prediction(double n, float q, float p, float d, float h, float e, double Vp, float n0) {
+BK_DEV double porosity_prediction(double n, float q, float p, float d, float h, float e, double Vp, float n0,
+                                  double* warm = nullptr) {
     double a = pressure_coefficient64(n);
-    double r = overstress64((double)q, a * (double)p, (double)d, (double)h * a);
+    double r = overstress64((double)q, a * (double)p, (double)d, (double)h * a, warm);
     if (r == 0.0) return Vp - 1.0 + (double)n0;  // no overstress: exp(e (1 - 1/1)) = exp(0) = 1 exactly
     double den = 1.0 + (double)h * a * r;
     return Vp * exp((double)e * (1.0 - 1.0 / den)) - 1.0 + (double)n0;
@@ -508,10 +519,10 @@ BK_DEV double porosity_prediction(double n, float q, float p, float d, float h, 
 // R = r + 1 - q/(1+dr)^2 - a p/(1+h a r)^2 with a = a(n) (the derivatives the reference's
 // SolvePorosityGradient uses, porous_return.py:68-92).
 BK_DEV double porosity_prediction_slope(double n, float qf, float pf, float df, float hf, float ef, double Vp,
-                                        float n0, double& slope) {
+                                        float n0, double& slope, double* warm = nullptr) {
     const double q = qf, p = pf, d = df, h = hf, e = ef;
     double a = pressure_coefficient64(n);
-    double r = overstress64(q, a * p, d, h * a);
+    double r = overstress64(q, a * p, d, h * a, warm);
     double v = 1.0 + h * a * r;
     double core = Vp * exp(e * (1.0 - 1.0 / v));
     double da = 0.0;
@@ -530,11 +541,12 @@ BK_DEV double porosity_prediction_slope(double n, float qf, float pf, float df, 
 }
 
 // The reference's 64-step bisection of n -> prediction(n) on [0, 1 - 1e-9] (porous_return.py:51-61).
-BK_DEV float solve_porosity_bisection(float q, float p, float d, float h, float e, double Vp, float n0) {
+BK_DEV float solve_porosity_bisection(float q, float p, float d, float h, float e, double Vp, float n0,
+                                      double* warm = nullptr) {
     double lo = 0.0, hi = 1.0 - 1.0e-9;
     for (int it = 0; it < 64; ++it) {
         double mid = (lo + hi) * 0.5;
-        double pred = porosity_prediction(mid, q, p, d, h, e, Vp, n0);
+        double pred = porosity_prediction(mid, q, p, d, h, e, Vp, n0, warm);
         if (mid < pred) lo = mid; else hi = mid;
     }
     return (float)((lo + hi) * 0.5);
@@ -547,7 +559,12 @@ BK_DEV float solve_porosity_bisection(float q, float p, float d, float h, float 
 // iteration cannot escape the bracket and converges in a few evaluations. When the bracket's
 // lower end is not below the root (g(0+) >= 0) the reference's bisection runs unchanged. The root
 // is resolved to ~1e-14 relative, far below the float32 rounding of the returned porosity.
-BK_DEV float solve_porosity(float q, float p, float d, float h, float e, double Vp, float n0) {
+// Each evaluation's overstress root starts from the previous one (`warm`, which also returns the
+// last root to the caller); the roots are the reference's to its |residual| < 1e-12 test.
+BK_DEV float solve_porosity(float q, float p, float d, float h, float e, double Vp, float n0,
+                            double* warm = nullptr) {
+    double r_local = 0.0;
+    if (!warm) warm = &r_local;
     double trial = Vp - 1.0 + (double)n0;
     if (trial > 0.0 && trial < 1.0) {
         double a = pressure_coefficient64(trial);
@@ -555,19 +572,27 @@ BK_DEV float solve_porosity(float q, float p, float d, float h, float e, double 
     }
     double lo = 0.0, hi = 1.0 - 1.0e-9;
     // g(0+) = -trial: the root lies above zero only when the elastic prediction is positive.
-    if (!(trial > 0.0)) return solve_porosity_bisection(q, p, d, h, e, Vp, n0);
+    if (!(trial > 0.0)) return solve_porosity_bisection(q, p, d, h, e, Vp, n0, warm);
     double n = trial < hi ? trial : 0.5 * (lo + hi);
     for (int it = 0; it < 100; ++it) {
         double slope;
-        double pred = porosity_prediction_slope(n, q, p, d, h, e, Vp, n0, slope);
+        double pred = porosity_prediction_slope(n, q, p, d, h, e, Vp, n0, slope, warm);
         double g = n - pred;
+        if (g == 0.0) break;  // n is the root
         if (n < pred) lo = n; else hi = n;
         double dg = 1.0 - slope;
         double next = n - g / dg;
+        // A converged Newton step ends the solve before the bracket test: when the root sits on
+        // the end of the bracket that n just became (g at the float64 rounding level, as when the
+        // mean stress vanishes), the step falls on that end, and treating it as a bracket escape
+        // would bisect all the way back to it.
+        if (fabs(next - n) <= 1e-14 * fabs(n)) {
+            if (next > lo && next < hi) n = next;
+            break;
+        }
         if (!(next > lo && next < hi)) next = 0.5 * (lo + hi);
-        double step = fabs(next - n);
         n = next;
-        if (step <= 1e-14 * n || hi - lo <= 1e-15 * hi) break;
+        if (hi - lo <= 1e-15 * hi) break;
     }
     return (float)n;
 }
@@ -581,7 +606,7 @@ struct DingOut {
 
 // Ding return map (ding.py:103-137) given the SVD of the trial gradient (float32 factors).
 BK_DEV DingOut ding_return(const M3& trial, const M3& Um, const float* s, const M3& Vm, float mu, float lam,
-                           float ty, float eta, float a, float dt) {
+                           float ty, float eta, float a, float dt, float r0 = 0.0f) {
     const float* U = Um.m;
     const float* V = Vm.m;
     float eps[3] = {logf(s[0]), logf(s[1]), logf(s[2])};
@@ -596,7 +621,7 @@ BK_DEV DingOut ding_return(const M3& trial, const M3& Um, const float* s, const 
     float p2 = a * mean * mean / ty2;
     float df = 6.0f * mu * dt * ty * ty / eta;
     float mf = 2.0f * a / 3.0f * (2.0f * mu + 3.0f * lam) * dt * ty * ty / eta;
-    float r = solve_overstress(q2, p2, df, mf);
+    float r = solve_overstress(q2, p2, df, mf, r0);
     float cs[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) cs[k] = dev[k] / (1.0f + df * r) + mean / (1.0f + mf * r);
@@ -717,6 +742,7 @@ BK_DEV void ding_exact(const DingParamsDev& P, const DingPrelude& d, float por, 
     const float dt = P.dt, mu = P.mu, lam = P.lam, n0 = P.initial_porosity;
     const float ty = d.ty, eta = d.eta;
     float ret_por = por, consistency = 0.0f;
+    double r_warm = 0.0;  // overstress root carried from one solve to the next
     if (P.coupled_porosity) {
         float st[3] = {logf(d.s[0]), logf(d.s[1]), logf(d.s[2])};
         float tr = st[0] + st[1] + st[2];
@@ -732,12 +758,13 @@ BK_DEV void ding_exact(const DingParamsDev& P, const DingPrelude& d, float por, 
         float ms = 2.0f / 3.0f * (2.0f * mu + 3.0f * lam) * dt * ty * ty / eta;
         float ex = 3.0f * mean / (2.0f * mu + 3.0f * lam);
         double Vp = 1.0 - (double)n0 + (double)por;
-        ret_por = solve_porosity(qv, pv, df, ms, ex, Vp, n0);
-        double pred = porosity_prediction((double)ret_por, qv, pv, df, ms, ex, Vp, n0);
+        ret_por = solve_porosity(qv, pv, df, ms, ex, Vp, n0, &r_warm);
+        double pred = porosity_prediction((double)ret_por, qv, pv, df, ms, ex, Vp, n0, &r_warm);
         consistency = (float)fabs((double)ret_por - pred);
         if (consistency > 1.0e-6f || ret_por <= 0.0f || ret_por >= 1.0f) set_flag(flags, 1);
     }
-    DingOut r = ding_return(d.trial, d.U, d.s, d.V, mu, lam, ty, eta, porosity_coefficient(ret_por), dt);
+    DingOut r = ding_return(d.trial, d.U, d.s, d.V, mu, lam, ty, eta, porosity_coefficient(ret_por), dt,
+                            (float)r_warm);
     ding_close(P, por, F_tot, ret_por, r.Fe, flags, out, need_fp);
     out.tau = r.tau;
     out.residual = r.residual;

@@ -910,9 +910,11 @@ __global__ void __launch_bounds__(128, 6) k_g2p_return(Params P, BkState in, BkS
     }
 }
 
-// G2P + return map with the learned surrogate: each CTA evaluates the network for its 128
-// particles on the tensor cores (bk_mlp.cuh); yielding particles inside the training range take
-// the surrogate's return, all others (elastic, out of range, invalid porosity) the exact map.
+// G2P + return map with the learned surrogate: a persistent CTA walks 128-particle tiles and
+// evaluates the network for each on the tensor cores (bk_mlp.cuh), so the weights are staged,
+// the tensor memory allocated and the mbarrier initialised once per CTA. Yielding particles inside
+// the training range take the surrogate's return; all others (elastic, out of range, invalid
+// porosity) the exact map.
 __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkState in, BkState out, BkConstants cst,
                                                              GridPtrs g, BkDiagnostics diag, BkFlags flags,
                                                              SurrogateDev sg) {
@@ -920,67 +922,71 @@ __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkSta
     __shared__ int s_counts[3];
     mlp::tile_setup(ts, sg.blob);
     if (threadIdx.x < 3) s_counts[threadIdx.x] = 0;
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (blockIdx.x == 0 && threadIdx.x < 6) {
         g.bounds[6 + threadIdx.x] = g.bounds[threadIdx.x];
         g.bounds[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
     }
+    __syncthreads();
     const int64_t pitch = P.pitch;
-    M3 Fn, Cn;
-    bool ding = false, use_mlp = false;
-    DingPrelude d;
-    float T = 0.f, por = 0.f, x[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    int perm[3] = {0, 1, 2};
-    if (i < P.n && g2p_gather(P, in, out, g, flags, i, Fn, Cn) && P.material == 1) {
-        T = P.transport ? (float)out.temperature[i] : in.material_temperature[i];
-        por = in.porosity[i];
-        ding = ding_prelude(P.ding, load_m3(in.Fe, i, pitch), por, in.gelled[i], Cn, T, __ldg(cst.viscosity_parameter),
-                            flags.ding, d);
-        if (ding && !ding_elastic(P.ding, d, por)) {
-            order3(d.s, perm);
-            float f[7];
-            surrogate_features(P, out, cst, i, d, por, det3(Fn), perm, f);
-            use_mlp = true;
-#pragma unroll
-            for (int k = 0; k < 7; ++k) {
-                use_mlp = use_mlp && f[k] >= sg.in_low[k] && f[k] <= sg.in_high[k];
-                x[k] = (f[k] - sg.in_mean[k]) / sg.in_scale[k];
-            }
-        }
-    }
-    __syncthreads();  // s_counts initialised before any thread adds to it
-    float y[3];
     uint32_t phase = 0;
-    const bool tile_ok = mlp::tile_eval(ts, x, use_mlp, y, phase);
-    int path = -1;
-    if (ding) {
-        DingParticleOut o;
-        bool done = false;
-        if (use_mlp && tile_ok) {
-            // y is in the sorted order: singular value j has rank r_j with perm[r_j] = j.
-            float e[3];
+    for (int64_t base = (int64_t)blockIdx.x * 128; base < P.n; base += (int64_t)gridDim.x * 128) {
+        const int64_t i = base + threadIdx.x;
+        M3 Fn, Cn;
+        bool ding = false, use_mlp = false;
+        DingPrelude d;
+        float T = 0.f, por = 0.f, x[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int perm[3] = {0, 1, 2};
+        if (i < P.n && g2p_gather(P, in, out, g, flags, i, Fn, Cn) && P.material == 1) {
+            T = P.transport ? (float)out.temperature[i] : in.material_temperature[i];
+            por = in.porosity[i];
+            ding = ding_prelude(P.ding, load_m3(in.Fe, i, pitch), por, in.gelled[i], Cn, T,
+                                __ldg(cst.viscosity_parameter), flags.ding, d);
+            if (ding && !ding_elastic(P.ding, d, por)) {
+                order3(d.s, perm);
+                float f[7];
+                surrogate_features(P, out, cst, i, d, por, det3(Fn), perm, f);
+                use_mlp = true;
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const int r = perm[0] == j ? 0 : (perm[1] == j ? 1 : 2);
-                e[j] = logf(d.s[j]) + sel3(y, r) * sel3(sg.out_scale, r);
-            }
-            done = ding_surrogate(P.ding, d, por, Fn, e, flags.ding, o, diag.plastic_gradients != nullptr);
-            // Judged in whole warps, so that the exact map's cost falls on 1 warp in judge_stride.
-            if (done && sg.judge_error && sg.judge_stride > 0 && (i >> 5) % sg.judge_stride == 0) {
-                DingParticleOut ex;
-                int32_t scratch[3] = {0, 0, 0};
-                ding_exact(P.ding, d, por, Fn, scratch, ex, false);
-                float err = 0.f;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) err = fmaxf(err, fabsf(ex.e[k] - e[k]));
-                atomic_max_nonneg(sg.judge_error, err);
+                for (int k = 0; k < 7; ++k) {
+                    use_mlp = use_mlp && f[k] >= sg.in_low[k] && f[k] <= sg.in_high[k];
+                    x[k] = (f[k] - sg.in_mean[k]) / sg.in_scale[k];
+                }
             }
         }
-        if (!done) ding_exact(P.ding, d, por, Fn, flags.ding, o, diag.plastic_gradients != nullptr);
-        path = done ? 1 : (o.yielded ? 2 : 0);
-        ding_store(P, out, diag, i, T, o);
+        float y[3];
+        const bool tile_ok = mlp::tile_eval(ts, x, use_mlp, y, phase);
+        int path = -1;
+        if (ding) {
+            DingParticleOut o;
+            bool done = false;
+            if (use_mlp && tile_ok) {
+                // y is in the sorted order: singular value j has rank r_j with perm[r_j] = j.
+                float e[3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const int r = perm[0] == j ? 0 : (perm[1] == j ? 1 : 2);
+                    e[j] = logf(d.s[j]) + sel3(y, r) * sel3(sg.out_scale, r);
+                }
+                done = ding_surrogate(P.ding, d, por, Fn, e, flags.ding, o, diag.plastic_gradients != nullptr);
+                // Judged in whole warps, so that the exact map's cost falls on 1 warp in judge_stride.
+                if (done && sg.judge_error && sg.judge_stride > 0 && (i >> 5) % sg.judge_stride == 0) {
+                    DingParticleOut ex;
+                    int32_t scratch[3] = {0, 0, 0};
+                    ding_exact(P.ding, d, por, Fn, scratch, ex, false);
+                    float err = 0.f;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) err = fmaxf(err, fabsf(ex.e[k] - e[k]));
+                    atomic_max_nonneg(sg.judge_error, err);
+                }
+            }
+            if (!done) ding_exact(P.ding, d, por, Fn, flags.ding, o, diag.plastic_gradients != nullptr);
+            path = done ? 1 : (o.yielded ? 2 : 0);
+            ding_store(P, out, diag, i, T, o);
+        }
+        if (sg.path_counts && path >= 0) atomicAdd(&s_counts[path], 1);
+        __syncthreads();
+        if (ts.failed) break;  // read after a barrier, so every thread takes the same branch
     }
-    if (sg.path_counts && path >= 0) atomicAdd(&s_counts[path], 1);
     mlp::tile_teardown(ts);
     if (sg.path_counts && threadIdx.x < 3 && s_counts[threadIdx.x]) atomicAdd(sg.path_counts + threadIdx.x, s_counts[threadIdx.x]);
 }
@@ -1136,8 +1142,10 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
         const SurrogateDev sg = surrogate_dev(p.surrogate);
         if (sg.blob && p.material == 1) {
             int rec = profile_begin("g2p_return_surrogate", s);
-            k_g2p_return_surrogate<<<blocks_for(p.n, 128), 128, 0, s>>>(P, *in, *out, *constants, g, *diagnostics,
-                                                                     *flags, sg);
+            const unsigned tiles = blocks_for(p.n, 128);
+            const unsigned persistent = (unsigned)sms * 4;
+            k_g2p_return_surrogate<<<tiles < persistent ? tiles : persistent, 128, 0, s>>>(
+                P, *in, *out, *constants, g, *diagnostics, *flags, sg);
             profile_end(rec, s);
         } else {
             int rec = profile_begin("g2p_return", s);

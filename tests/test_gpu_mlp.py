@@ -37,8 +37,9 @@ def test_tensor_core_inference_matches_oracle(n):
     x = omlp.normalise(feats[:n], norm.in_mean, norm.in_scale)
     ref = omlp.forward(params, x) * norm.out_scale
     scale = np.abs(ref).max()
-    # BF16 hidden activations may round differently where FP32 sums differ in their last bits.
-    np.testing.assert_allclose(out, ref, rtol=0, atol=2e-3 * scale)
+    # BF16 hidden activations may round differently where FP32 sums differ in their last bits, and
+    # the inference SiLU uses the hardware tanh approximation (relative error ~2^-11).
+    np.testing.assert_allclose(out, ref, rtol=0, atol=4e-3 * scale)
     assert np.abs(out - ref).mean() < 2e-4 * scale
 
 
