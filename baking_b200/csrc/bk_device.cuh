@@ -423,8 +423,9 @@ BK_DEV Stencil make_stencil(const V3& x, const float* origin, float dx, int R) {
 
 BK_DEV int64_t node_index(int i, int j, int k, int R) { return ((int64_t)i * R + j) * R + k; }
 
+// flags may be NULL (a re-evaluation whose flags are not reported).
 BK_DEV void set_flag(int32_t* flags, int index) {
-    if (flags[index] == 0) atomicMax(flags + index, 1);
+    if (flags && flags[index] == 0) atomicMax(flags + index, 1);
 }
 
 // ------------------------------------------------------- ding.py:56-100

@@ -971,8 +971,7 @@ __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkSta
                 // Judged in whole warps, so that the exact map's cost falls on 1 warp in judge_stride.
                 if (done && sg.judge_error && sg.judge_stride > 0 && (i >> 5) % sg.judge_stride == 0) {
                     DingParticleOut ex;
-                    int32_t scratch[3] = {0, 0, 0};
-                    ding_exact(P.ding, d, por, Fn, scratch, ex, false);
+                    ding_exact(P.ding, d, por, Fn, nullptr, ex, false);  // judge only: no flags
                     float err = 0.f;
 #pragma unroll
                     for (int k = 0; k < 3; ++k) err = fmaxf(err, fabsf(ex.e[k] - e[k]));
