@@ -867,10 +867,11 @@ __device__ bool ding_surrogate(const DingParamsDev& D, const DingPrelude& d, flo
     return true;
 }
 
-// 6 blocks of 128 threads per SM (80 registers): the float64 steps of the return map are latency
-// bound, so the extra resident warps outweigh a few spilled registers. With `sg.samples` set
-// (harvest), yielding particles on the sampling stride append (features, return) rows.
-__global__ void __launch_bounds__(128, 6) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
+// 8 blocks of 128 threads per SM (64 registers): the return map's dependent float64 chains are
+// latency bound, so resident warps outweigh the spilled registers (measured at 3 to 12 blocks per
+// SM: 8 is fastest for both elastic and yielding particles). With `sg.samples` set (harvest),
+// yielding particles on the sampling stride append (features, return) rows.
+__global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
                                                    BkDiagnostics diag, BkFlags flags, SurrogateDev sg) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (blockIdx.x == 0 && threadIdx.x < 6) {
