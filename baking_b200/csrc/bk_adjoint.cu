@@ -15,8 +15,8 @@
 // in the rotated frame use divided differences of g and h. For this model they have closed
 // forms (g_j - g_i and h_j - h_i depend on log(s_j / s_i) alone), evaluated with expm1/log1p so
 // they stay finite as two singular values coincide. The diagonal and parameter derivatives come
-// from forward-mode duals through the principal-space chain, including the implicit overstress
-// solve (derivatives as in the reference's SolveOverstressGradient, ding.py:90-100).
+// from a hand-written reverse sweep through the principal-space chain, including the implicit
+// overstress solve (derivatives as in the reference's SolveOverstressGradient, ding.py:90-100).
 // Differentiable parameters: shear modulus, Lame lambda, the viscosity parameter and the
 // per-particle temperature (through the yield and viscosity factor tables). The gelation latch and
 // the wall and stencil switches are discrete; like the reference, no gradient flows through them.
@@ -26,7 +26,6 @@
 #include "baking_b200.h"
 #include "bk_common.h"
 #include "bk_device.cuh"
-#include "bk_dual.cuh"
 
 using namespace bk;
 
@@ -47,94 +46,173 @@ struct AdjState {
     float *x, *v, *C, *F, *Fe, *tau, *porosity, *temperature;
 };
 
-// Directional-derivative slots of the principal-space duals.
+// Slots of the principal-space derivative vector: the three singular values, then the parameters.
 enum { kS0 = 0, kS1, kS2, kMu, kLam, kTy, kEta, kA, kDirs };
-using D8 = Dual<kDirs>;
 
-struct Principal {
-    float g[3], h[3];          // Fe' = U diag(g) V^T, tau' = U diag(h) U^T
-    float dg[3][kDirs], dh[3][kDirs];
-    float r, df;               // overstress root and deviatoric factor d
-    float iso;                 // common isochoric factor applied to g (1 when a != 0)
+// Forward values of sigma -> (g, h) of the Ding return map (ding.py:103-131), kept for the
+// reverse sweep: Fe' = U diag(g) V^T, tau' = U diag(h = cs) U^T.
+struct PrincipalFwd {
+    float s[3], eps[3], ts[3], dev[3], cs[3], gpre[3], g[3];
+    float tr, mean, ty, ty2, q2, p2, bulk, d, h, r, u, w, cm, c;
+    float mu, lam, eta, a, dt;
+    bool yielded, iso;
 };
 
-// sigma -> (g, h) of the Ding return map (ding.py:103-131) with derivatives.
-__device__ Principal principal(const float* s, float mu, float lam, float ty, float eta, float a, float dt) {
-    D8 S[3] = {D8::seed(s[0], kS0), D8::seed(s[1], kS1), D8::seed(s[2], kS2)};
-    D8 Mu = D8::seed(mu, kMu), Lam = D8::seed(lam, kLam), Ty = D8::seed(ty, kTy), Eta = D8::seed(eta, kEta);
-    D8 Aa = D8::seed(a, kA);
-    D8 eps[3] = {dlog(S[0]), dlog(S[1]), dlog(S[2])};
-    D8 tr = eps[0] + eps[1] + eps[2];
-    D8 two_mu = scale(Mu, 2.f);
-    D8 ts[3];
+__device__ PrincipalFwd principal_forward(const float* s, float mu, float lam, float ty, float eta, float a, float dt) {
+    PrincipalFwd f;
+    f.mu = mu; f.lam = lam; f.ty = ty; f.eta = eta; f.a = a; f.dt = dt;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) ts[k] = two_mu * eps[k] + Lam * tr;
-    D8 mean = scale(ts[0] + ts[1] + ts[2], 1.f / 3.f);
-    D8 dev[3] = {ts[0] - mean, ts[1] - mean, ts[2] - mean};
-    D8 ty2 = Ty * Ty;
-    D8 q2 = scale(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2], 1.5f) / ty2;
-    D8 p2 = Aa * mean * mean / ty2;
-    D8 bulk = two_mu + scale(Lam, 3.f);
-    D8 d = scale(Mu, 6.f * dt) * ty2 / Eta;
-    D8 h = scale(Aa, 2.f / 3.f * dt) * bulk * ty2 / Eta;
-    float r = solve_overstress(q2.v, p2.v, d.v, h.v);
-    D8 R(r);
-    if (q2.v + p2.v > 1.0f) {
-        // R(r) = r + 1 - q2/(1+dr)^2 - p2/(1+hr)^2 = 0: dr = -(R_q2 dq2 + R_p2 dp2 + R_d dd + R_h dh) / R_r.
-        float u = 1.f + d.v * r, w = 1.f + h.v * r;
-        float Rr = 1.f + 2.f * d.v * q2.v / (u * u * u) + 2.f * h.v * p2.v / (w * w * w);
-        float Rq = -1.f / (u * u), Rp = -1.f / (w * w);
-        float Rd = 2.f * q2.v * r / (u * u * u), Rh = 2.f * p2.v * r / (w * w * w);
+    for (int k = 0; k < 3; ++k) { f.s[k] = s[k]; f.eps[k] = logf(s[k]); }
+    f.tr = f.eps[0] + f.eps[1] + f.eps[2];
 #pragma unroll
-        for (int k = 0; k < kDirs; ++k) R.d[k] = -(Rq * q2.d[k] + Rp * p2.d[k] + Rd * d.d[k] + Rh * h.d[k]) / Rr;
-    }
-    D8 one(1.f);
-    D8 cs[3];
+    for (int k = 0; k < 3; ++k) f.ts[k] = 2.f * mu * f.eps[k] + lam * f.tr;
+    f.mean = (f.ts[0] + f.ts[1] + f.ts[2]) / 3.f;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) cs[k] = dev[k] / (one + d * R) + mean / (one + h * R);
-    D8 cm = scale(cs[0] + cs[1] + cs[2], 1.f / 3.f);
-    D8 g[3];
+    for (int k = 0; k < 3; ++k) f.dev[k] = f.ts[k] - f.mean;
+    f.ty2 = ty * ty;
+    f.q2 = 1.5f * (f.dev[0] * f.dev[0] + f.dev[1] * f.dev[1] + f.dev[2] * f.dev[2]) / f.ty2;
+    f.p2 = a * f.mean * f.mean / f.ty2;
+    f.bulk = 2.f * mu + 3.f * lam;
+    f.d = 6.f * mu * dt * f.ty2 / eta;
+    f.h = 2.f / 3.f * dt * a * f.bulk * f.ty2 / eta;
+    f.r = solve_overstress(f.q2, f.p2, f.d, f.h);
+    f.yielded = f.q2 + f.p2 > 1.0f;
+    f.u = 1.f + f.d * f.r;
+    f.w = 1.f + f.h * f.r;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) g[k] = dexp((cs[k] - cm) / two_mu + cm / bulk);
-    Principal out;
-    out.iso = 1.f;
-    if (a == 0.0f) {
+    for (int k = 0; k < 3; ++k) f.cs[k] = f.dev[k] / f.u + f.mean / f.w;
+    f.cm = (f.cs[0] + f.cs[1] + f.cs[2]) / 3.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) f.gpre[k] = expf((f.cs[k] - f.cm) / (2.f * mu) + f.cm / f.bulk);
+    f.iso = a == 0.0f;
+    f.c = 1.f;
+    if (f.iso) {
         // Isochoric correction (ding.py:129-131): Fe' *= cbrt(det trial / det Fe'), a common factor.
-        D8 c = dcbrt((S[0] * S[1] * S[2]) / (g[0] * g[1] * g[2]));
-        out.iso = c.v;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) g[k] = g[k] * c;
+        f.c = cbrtf((s[0] * s[1] * s[2]) / (f.gpre[0] * f.gpre[1] * f.gpre[2]));
     }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) f.g[k] = f.gpre[k] * f.c;
+    return f;
+}
+
+// Reverse sweep of principal_forward: given dL/dg (gb) and dL/dh (hb), the derivatives of L with
+// respect to the slots kS0..kA. The overstress root enters through the implicit function theorem
+// on R(r) = r + 1 - q2/(1+dr)^2 - p2/(1+hr)^2 (the derivatives of the reference's
+// SolveOverstressGradient, ding.py:90-100).
+__device__ void principal_vjp(const PrincipalFwd& f, const float* gb, const float* hb, float* out) {
+    const float mu = f.mu, lam = f.lam;
+    float sb[3] = {0.f, 0.f, 0.f}, gpb[3];
+    float mub = 0.f, lamb = 0.f, etab = 0.f, ab = 0.f, ty2b = 0.f;
+    if (f.iso) {
+        float cb = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            cb += gb[k] * f.gpre[k];
+            gpb[k] = gb[k] * f.c;
+        }
+        // c = cbrt(P), P = s0 s1 s2 / (gp0 gp1 gp2): dc/dP P = c / 3
+        const float cp = cb * f.c / 3.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            sb[k] += cp / f.s[k];
+            gpb[k] -= cp / f.gpre[k];
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) gpb[k] = gb[k];
+    }
+    // gpre_k = exp(z_k), z_k = (cs_k - cm) / (2 mu) + cm / bulk
+    float csb[3], cmb = 0.f, bulkb = 0.f;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        out.g[k] = g[k].v;
-        out.h[k] = cs[k].v;
-#pragma unroll
-        for (int j = 0; j < kDirs; ++j) {
-            out.dg[k][j] = g[k].d[j];
-            out.dh[k][j] = cs[k].d[j];
-        }
+        const float zb = gpb[k] * f.gpre[k];
+        csb[k] = hb[k] + zb / (2.f * mu);
+        cmb += zb * (1.f / f.bulk - 1.f / (2.f * mu));
+        mub -= zb * (f.cs[k] - f.cm) / (2.f * mu * mu);
+        bulkb -= zb * f.cm / (f.bulk * f.bulk);
     }
-    out.r = r;
-    out.df = d.v;
-    return out;
-}
-
-// expm1(x / c) / expm1(x), finite at x = 0.
-__device__ __forceinline__ float ratio_expm1(float x, float c) {
-    if (fabsf(x) < 1e-12f) return 1.f / c;
-    return expm1f(x / c) / expm1f(x);
-}
-
-// x / expm1(x), finite at x = 0.
-__device__ __forceinline__ float x_over_expm1(float x) {
-    if (fabsf(x) < 1e-12f) return 1.f;
-    return x / expm1f(x);
+    // cm = (cs_0 + cs_1 + cs_2) / 3; cs_k = dev_k / u + mean / w
+    float devb[3], meanb = 0.f, ub = 0.f, wb = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        csb[k] += cmb / 3.f;
+        devb[k] = csb[k] / f.u;
+        meanb += csb[k] / f.w;
+        ub -= csb[k] * f.dev[k] / (f.u * f.u);
+        wb -= csb[k] * f.mean / (f.w * f.w);
+    }
+    float db = ub * f.r, hbar = wb * f.r;
+    const float rb = ub * f.d + wb * f.h;
+    float q2b = 0.f, p2b = 0.f;
+    if (f.yielded) {
+        const float u3 = f.u * f.u * f.u, w3 = f.w * f.w * f.w;
+        const float Rr = 1.f + 2.f * f.d * f.q2 / u3 + 2.f * f.h * f.p2 / w3;
+        const float k = -rb / Rr;
+        q2b += k * (-1.f / (f.u * f.u));
+        p2b += k * (-1.f / (f.w * f.w));
+        db += k * (2.f * f.q2 * f.r / u3);
+        hbar += k * (2.f * f.p2 * f.r / w3);
+    }
+    // h = (2/3) dt a bulk ty2 / eta
+    const float kh = 2.f / 3.f * f.dt / f.eta;
+    ab += hbar * kh * f.bulk * f.ty2;
+    bulkb += hbar * kh * f.a * f.ty2;
+    ty2b += hbar * kh * f.a * f.bulk;
+    etab -= hbar * f.h / f.eta;
+    // d = 6 mu dt ty2 / eta
+    mub += db * 6.f * f.dt * f.ty2 / f.eta;
+    ty2b += db * 6.f * mu * f.dt / f.eta;
+    etab -= db * f.d / f.eta;
+    // bulk = 2 mu + 3 lam
+    mub += 2.f * bulkb;
+    lamb += 3.f * bulkb;
+    // p2 = a mean^2 / ty2; q2 = 1.5 |dev|^2 / ty2
+    ab += p2b * f.mean * f.mean / f.ty2;
+    meanb += p2b * 2.f * f.a * f.mean / f.ty2;
+    ty2b -= p2b * f.p2 / f.ty2;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) devb[k] += q2b * 3.f * f.dev[k] / f.ty2;
+    ty2b -= q2b * f.q2 / f.ty2;
+    const float tyb = 2.f * f.ty * ty2b;
+    // dev_k = ts_k - mean; mean = (ts_0 + ts_1 + ts_2) / 3
+    float tsb[3], devsum = devb[0] + devb[1] + devb[2];
+    meanb -= devsum;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) tsb[k] = devb[k] + meanb / 3.f;
+    // ts_k = 2 mu eps_k + lam tr; tr = eps_0 + eps_1 + eps_2; eps_k = log s_k
+    const float tsum = tsb[0] + tsb[1] + tsb[2];
+    lamb += f.tr * tsum;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        mub += 2.f * f.eps[k] * tsb[k];
+        sb[k] += (2.f * mu * tsb[k] + lam * tsum) / f.s[k];
+    }
+    out[kS0] = sb[0]; out[kS1] = sb[1]; out[kS2] = sb[2];
+    out[kMu] = mub; out[kLam] = lamb; out[kTy] = tyb; out[kEta] = etab; out[kA] = ab;
 }
 
 __device__ __forceinline__ void add_m3(float* __restrict__ p, int64_t i, int64_t pitch, const float* a) {
 #pragma unroll
     for (int c = 0; c < 9; ++c) p[c * pitch + i] += a[c];
+}
+
+// a^T b and a b^T for 3x3 row-major matrices.
+__device__ __forceinline__ M3 mul_tn(const M3& a, const M3& b) {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.m[3 * i + j] = a.m[i] * b.m[j] + a.m[3 + i] * b.m[3 + j] + a.m[6 + i] * b.m[6 + j];
+    return r;
+}
+__device__ __forceinline__ M3 mul_nt(const M3& a, const M3& b) {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            r.m[3 * i + j] = a.m[3 * i] * b.m[3 * j] + a.m[3 * i + 1] * b.m[3 * j + 1] + a.m[3 * i + 2] * b.m[3 * j + 2];
+    return r;
 }
 
 // Block-reduce a value into one float64 accumulator (material parameter adjoints).
@@ -162,7 +240,7 @@ __device__ __forceinline__ float qweight_grad(float l, int o) {
 
 // ------------------------------------------------------------ G2P + return
 // params_adj: float64 [0] mu, [1] lambda, [2] viscosity parameter.
-__global__ void __launch_bounds__(kThreads) k_adj_g2p_return(AdjParams P, BkState in, const float4* __restrict__ grid_v,
+__global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkState in, const float4* __restrict__ grid_v,
                                                           const float* __restrict__ eta_param, AdjState out_adj,
                                                           AdjState in_adj, float4* __restrict__ grid_v_adj,
                                                           double* __restrict__ params_adj) {
@@ -248,7 +326,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_g2p_return(AdjParams P, BkStat
                 float s[3];
                 svd3f(trial, U, s, V);
                 float a = porosity_coefficient(por);
-                Principal pr = principal(s, D.mu, D.lam, ty, eta, a, D.dt);
+                PrincipalFwd pr = principal_forward(s, D.mu, D.lam, ty, eta, a, D.dt);
                 // porosity' = det(F') / prod(g) - 1 + n0 (uncoupled; zero when n0 = n = 0)
                 float prod_g = pr.g[0] * pr.g[1] * pr.g[2];
                 bool porosity_free = !(D.initial_porosity == 0.0f && por == 0.0f);
@@ -266,70 +344,58 @@ __global__ void __launch_bounds__(kThreads) k_adj_g2p_return(AdjParams P, BkStat
 #pragma unroll
                     for (int k = 0; k < 3; ++k) gb_por[k] = -por_b * npor / pr.g[k];
                 }
-                // rotated adjoints
-                float Gh[9], Th[9];
+                // rotated adjoints Gh = U^T Fe_bar V, Th = U^T tau_bar U
+                M3 FeB, tauB;
 #pragma unroll
-                for (int p = 0; p < 3; ++p)
-#pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        float gs = 0.f, tsum = 0.f;
-#pragma unroll
-                        for (int r = 0; r < 3; ++r)
-#pragma unroll
-                            for (int c = 0; c < 3; ++c) {
-                                gs += U.m[3 * r + p] * Fe_b[3 * r + c] * V.m[3 * c + q];
-                                tsum += U.m[3 * r + p] * tau_b[3 * r + c] * U.m[3 * c + q];
-                            }
-                        Gh[3 * p + q] = gs;
-                        Th[3 * p + q] = tsum;
-                    }
+                for (int e = 0; e < 9; ++e) { FeB.m[e] = Fe_b[e]; tauB.m[e] = tau_b[e]; }
+                const M3 Ghm = mul_tn(U, matmul(FeB, V)), Thm = mul_tn(U, matmul(tauB, U));
+                const float* Gh = Ghm.m;
+                const float* Th = Thm.m;
                 // diagonal: sbar_j = sum_i (Gh_ii + gb_por_i) dg_i/ds_j + Th_ii dh_i/ds_j; parameters likewise
-                float Ab[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                M3 Abm;
+                float* Ab = Abm.m;
                 float dpar[kDirs];
-#pragma unroll
-                for (int j = 0; j < kDirs; ++j) {
-                    float t = 0.f;
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) t += (Gh[4 * k] + gb_por[k]) * pr.dg[k][j] + Th[4 * k] * pr.dh[k][j];
-                    dpar[j] = t;
+                {
+                    const float gbar[3] = {Gh[0] + gb_por[0], Gh[4] + gb_por[1], Gh[8] + gb_por[2]};
+                    const float hbar[3] = {Th[0], Th[4], Th[8]};
+                    principal_vjp(pr, gbar, hbar, dpar);
                 }
                 Ab[0] = dpar[kS0];
                 Ab[4] = dpar[kS1];
                 Ab[8] = dpar[kS2];
-                // off-diagonal: divided differences in closed form
-                const float one_dr = 1.f + pr.df * pr.r;
+                // Off-diagonal terms, one unordered pair (p, q) at a time. With M = U^T dA V:
+                //   dFe^_pq = P_pq M_pq + Q_pq M_qp, P_pq = (g_q s_q - g_p s_p) / (s_q^2 - s_p^2),
+                //   Q_pq = (g_q s_p - g_p s_q) / (s_q^2 - s_p^2); dtau^_pq = D (s_q M_pq + s_p M_qp),
+                //   D = (h_q - h_p) / (s_q^2 - s_p^2), symmetric in (p, q).
+                // With L = log(s_q / s_p): s_q = s_p (1 + A), g_q = g_p (1 + B), A = expm1(L),
+                // B = expm1(L / (1 + d r)), so the divided difference (g_q - g_p) / (s_q - s_p) is
+                // (g_p / s_p) B / A and h_q - h_p = 2 mu L / (1 + d r): one log1p and two expm1 per pair,
+                // finite as the two singular values coincide.
+                const float one_dr = 1.f + pr.d * pr.r;
 #pragma unroll
-                for (int p = 0; p < 3; ++p)
-#pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        if (p == q) continue;
-                        // pair (i=p, j=q): L = log(s_q / s_p)
-                        float L = log1pf((s[q] - s[p]) / s[p]);
-                        // dFe^_pq = P_pq M_pq + Q_pq M_qp with M = U^T dA V,
-                        //   P_pq = (g_q s_q - g_p s_p) / (s_q^2 - s_p^2), Q_pq = (g_q s_p - g_p s_q) / (s_q^2 - s_p^2);
-                        // dtau^_pq = D_pq (s_q M_pq + s_p M_qp), D_pq = (h_q - h_p) / (s_q^2 - s_p^2).
-                        // g_q / g_p = exp(L / (1 + d r)) and h_q - h_p = 2 mu L / (1 + d r).
-                        float ddg = (pr.g[p] / s[p]) * ratio_expm1(L, one_dr);  // (g_q - g_p) / (s_q - s_p)
-                        float P_pq = (ddg * s[q] + pr.g[p]) / (s[q] + s[p]);
-                        float ddg_r = (pr.g[q] / s[q]) * ratio_expm1(-L, one_dr);  // (g_p - g_q) / (s_p - s_q)
-                        float Q_qp = (ddg_r * s[q] - pr.g[q]) / (s[p] + s[q]);
-                        float D_pq = 2.f * D.mu / (one_dr * (s[q] + s[p]) * s[p]) * x_over_expm1(L);
-                        Ab[3 * p + q] = Gh[3 * p + q] * P_pq + Gh[3 * q + p] * Q_qp +
-                                        (Th[3 * p + q] + Th[3 * q + p]) * D_pq * s[q];
+                for (int k = 0; k < 3; ++k) {
+                    const int p = k == 2 ? 1 : 0;
+                    const int q = k == 0 ? 1 : 2;
+                    const float sp = s[p], sq = s[q], gp = pr.g[p], gq = pr.g[q];
+                    const float L = log1pf((sq - sp) / sp);
+                    float ratio = 1.f / one_dr, xo = 1.f;
+                    if (fabsf(L) >= 1e-12f) {
+                        const float A = expm1f(L), B = expm1f(L / one_dr);
+                        ratio = B / A;
+                        xo = L / A;
                     }
+                    const float ddg = (gp / sp) * ratio;
+                    const float inv_sum = 1.f / (sp + sq);
+                    const float P_pq = (ddg * sq + gp) * inv_sum, Q_qp = (ddg * sq - gq) * inv_sum;
+                    const float P_qp = (ddg * sp + gq) * inv_sum, Q_pq = (ddg * sp - gp) * inv_sum;
+                    const float Dm = 2.f * D.mu * xo * inv_sum / (one_dr * sp);
+                    const float Tsym = Th[3 * p + q] + Th[3 * q + p];
+                    Ab[3 * p + q] = Gh[3 * p + q] * P_pq + Gh[3 * q + p] * Q_qp + Tsym * Dm * sq;
+                    Ab[3 * q + p] = Gh[3 * q + p] * P_qp + Gh[3 * p + q] * Q_pq + Tsym * Dm * sp;
+                }
                 // trial adjoint A_bar = U Ab V^T
-                float Tb_m[9];
-#pragma unroll
-                for (int r = 0; r < 3; ++r)
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        float t = 0.f;
-#pragma unroll
-                        for (int p = 0; p < 3; ++p)
-#pragma unroll
-                            for (int q = 0; q < 3; ++q) t += U.m[3 * r + p] * Ab[3 * p + q] * V.m[3 * c + q];
-                        Tb_m[3 * r + c] = t;
-                    }
+                const M3 Tbm = matmul(U, mul_nt(Abm, V));
+                const float* Tb_m = Tbm.m;
                 // trial = (I + dt C') Fe: Cbar += dt trial_bar Fe^T; Fe_bar_in = (I + dt C')^T trial_bar
 #pragma unroll
                 for (int r = 0; r < 3; ++r)
@@ -448,16 +514,15 @@ __global__ void __launch_bounds__(kThreads) k_adj_g2p_return(AdjParams P, BkStat
 }
 
 // ------------------------------------------------------------- grid update
-__global__ void k_adj_grid(AdjParams P, const float4* __restrict__ pm, const float4* __restrict__ grid_v_adj,
-                           float4* __restrict__ pm_adj, int64_t nodes) {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= nodes) return;
+__device__ __forceinline__ void adj_grid_node(const AdjParams& P, const float4* __restrict__ pm,
+                                              float4* __restrict__ grid_v_adj, float4* __restrict__ pm_adj,
+                                              int64_t i, int c0, int c1, int c2, bool clear) {
     float4 a = grid_v_adj[i];
     float4 q = pm[i];
     float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
     if (q.w > 0.0f && (a.x != 0.f || a.y != 0.f || a.z != 0.f)) {
         const int R = P.R, bc = P.bc;
-        int c[3] = {(int)(i / ((int64_t)R * R)), (int)((i / R) % R), (int)(i % R)};
+        const int c[3] = {c0, c1, c2};
         float p[3] = {q.x, q.y, q.z}, ab[3] = {a.x, a.y, a.z};
         float pb[3], mb = 0.f;
 #pragma unroll
@@ -471,6 +536,38 @@ __global__ void k_adj_grid(AdjParams P, const float4* __restrict__ pm, const flo
         out = make_float4(pb[0], pb[1], pb[2], mb);
     }
     pm_adj[i] = out;
+    if (clear) grid_v_adj[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Every node of the grid (velocity adjoint zeroed beforehand by the caller of the substep).
+__global__ void k_adj_grid(AdjParams P, const float4* __restrict__ pm, float4* __restrict__ grid_v_adj,
+                           float4* __restrict__ pm_adj, int64_t nodes) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nodes) return;
+    const int R = P.R;
+    adj_grid_node(P, pm, grid_v_adj, pm_adj, i, (int)(i / ((int64_t)R * R)), (int)((i / R) % R), (int)(i % R), false);
+}
+
+// The nodes of the forward substep's active box (inclusive lo[3], hi[3] on the device), which holds
+// every stencil node; the velocity adjoint is zeroed behind, so the next call finds it zero.
+__global__ void k_adj_grid_box(AdjParams P, const int32_t* __restrict__ box, const float4* __restrict__ pm,
+                               float4* __restrict__ grid_v_adj, float4* __restrict__ pm_adj) {
+    int lo[3], ext[3];
+    int64_t count = 1;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int l = max(box[a], 0), h = min(box[3 + a], P.R - 1);
+        if (l > h) return;
+        lo[a] = l;
+        ext[a] = h - l + 1;
+        count *= ext[a];
+    }
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+        const int c2 = lo[2] + (int)(t % ext[2]);
+        const int c1 = lo[1] + (int)((t / ext[2]) % ext[1]);
+        const int c0 = lo[0] + (int)(t / ((int64_t)ext[2] * ext[1]));
+        adj_grid_node(P, pm, grid_v_adj, pm_adj, node_index(c0, c1, c2, P.R), c0, c1, c2, true);
+    }
 }
 
 // ---------------------------------------------------------------- P2G
@@ -634,9 +731,9 @@ AdjState adj_state(const BkAdjointState& s) {
 extern "C" {
 
 int bk_substep_adjoint(const BkSubstepParams* params, const BkState* in, const BkConstants* constants,
-                       const float* node_pm, const float* node_v, const BkAdjointState* out_adjoint,
-                       BkAdjointState* in_adjoint, float* node_v_adjoint, float* node_pm_adjoint,
-                       double* parameter_adjoint, void* stream) {
+                       const float* node_pm, const float* node_v, const int32_t* node_box,
+                       const BkAdjointState* out_adjoint, BkAdjointState* in_adjoint, float* node_v_adjoint,
+                       float* node_pm_adjoint, double* parameter_adjoint, void* stream) {
     if (!params || !in || !constants || !node_pm || !node_v || !out_adjoint || !in_adjoint || !node_v_adjoint ||
         !node_pm_adjoint)
         return bk::fail(BK_ERR_ARGUMENT, "bk_substep_adjoint: null argument");
@@ -653,16 +750,25 @@ int bk_substep_adjoint(const BkSubstepParams* params, const BkState* in, const B
     AdjParams a = adj_params(p);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int64_t nodes = (int64_t)p.resolution * p.resolution * p.resolution;
-    cudaMemsetAsync(node_v_adjoint, 0, nodes * sizeof(float4), s);
+    if (!node_box) cudaMemsetAsync(node_v_adjoint, 0, nodes * sizeof(float4), s);
     unsigned blocks = (unsigned)((p.n + kThreads - 1) / kThreads);
     k_adj_g2p_return<<<blocks, kThreads, 0, s>>>(a, *in, reinterpret_cast<const float4*>(node_v),
                                                  constants->viscosity_parameter, adj_state(*out_adjoint),
                                                  adj_state(*in_adjoint), reinterpret_cast<float4*>(node_v_adjoint),
                                                  parameter_adjoint);
     if (int rc = bk::check_launch("bk_substep_adjoint/g2p_return")) return rc;
-    k_adj_grid<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(a, reinterpret_cast<const float4*>(node_pm),
-                                                              reinterpret_cast<const float4*>(node_v_adjoint),
-                                                              reinterpret_cast<float4*>(node_pm_adjoint), nodes);
+    if (node_box) {
+        int device = 0, sms = 148;
+        cudaGetDevice(&device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        k_adj_grid_box<<<(unsigned)sms * 4, 256, 0, s>>>(a, node_box, reinterpret_cast<const float4*>(node_pm),
+                                                          reinterpret_cast<float4*>(node_v_adjoint),
+                                                          reinterpret_cast<float4*>(node_pm_adjoint));
+    } else {
+        k_adj_grid<<<(unsigned)((nodes + 255) / 256), 256, 0, s>>>(a, reinterpret_cast<const float4*>(node_pm),
+                                                                  reinterpret_cast<float4*>(node_v_adjoint),
+                                                                  reinterpret_cast<float4*>(node_pm_adjoint), nodes);
+    }
     if (int rc = bk::check_launch("bk_substep_adjoint/grid")) return rc;
     k_adj_p2g<<<blocks, kThreads, 0, s>>>(a, *in, constants->mass, constants->volume,
                                           reinterpret_cast<const float4*>(node_pm_adjoint), adj_state(*in_adjoint),

@@ -39,7 +39,7 @@ class BkAdjointState(C.Structure):
                 ("temperature", P)]
 
 
-_SIGNATURE = [P] * 10 + [P]
+_SIGNATURE = [P] * 11 + [P]
 
 # (keyword, state attribute, material-state attribute); outputs follow the same order.
 _KINEMATIC = (("positions", "particle_positions"), ("velocities", "particle_velocities"),
@@ -117,9 +117,21 @@ class _Runner:
         self.fn = _declare(self.lib)
         self.checkpoints = []
 
+    # ------------------------------------------------------------- buffers
+    def _pool(self):
+        """Buffers kept on the simulator between Rollout calls (states, grids, adjoint arrays)."""
+        return self.sim._buffers.setdefault("rollout", {"snapshots": [], "work": [], "grids": []})
+
+    def _states(self, key, count):
+        lst = self._pool()[key]
+        while len(lst) < count:
+            lst.append(self.sim._allocate_like_current())
+        return lst
+
     # ----------------------------------------------------------------- forward
     def _snapshot(self, state):
-        snap = self.sim._allocate_like_current()
+        snaps = self._states("snapshots", len(self.checkpoints) + 1)
+        snap = snaps[len(self.checkpoints)]
         _copy_state(snap, state, self.is_ding)
         return snap
 
@@ -144,7 +156,8 @@ class _Runner:
             self._set_young_modulus(inputs["young_modulus"].detach().reshape(()).item())
         if self.is_ding and sim.material.ding_config.gas_enabled:
             raise NotImplementedError("the gas (coupled porosity) return map has no adjoint here")
-        self.checkpoints = [self._snapshot(state)]
+        self.checkpoints = []
+        self.checkpoints.append(self._snapshot(state))
         for k in range(self.steps):
             sim._substep(check=False)
             if (k + 1) % self.every == 0 and k + 1 < self.steps:
@@ -164,32 +177,42 @@ class _Runner:
     def backward(self, grads):
         sim, eng = self.sim, self.engine
         n, pitch, dev = eng.n, eng.pitch, sim.device
-        adj = _AdjointBuffers(n, pitch, dev, self.is_ding)
+        pool = self._pool()
+        if pool.get("adjoint") is None:
+            R = sim.simulation_config.grid_resolution
+            pool["adjoint"] = _AdjointBuffers(n, pitch, dev, self.is_ding)
+            # node_v_adj must be zero before the first call; each call leaves it zero (node box mode).
+            pool["node_v_adj"] = torch.zeros(R ** 3, 4, dtype=torch.float32, device=dev)
+            pool["node_pm_adj"] = torch.empty(R ** 3, 4, dtype=torch.float32, device=dev)
+        adj, node_v_adj, node_pm_adj = pool["adjoint"], pool["node_v_adj"], pool["node_pm_adj"]
         for buf, g in zip(adj.tensors(), grads):
-            if g is not None:
+            if g is None:
+                buf.zero_()
+            else:
                 buf.copy_(g.reshape(buf.shape))
-        R = sim.simulation_config.grid_resolution
-        node_v_adj = torch.empty(R ** 3, 4, dtype=torch.float32, device=dev)
-        node_pm_adj = torch.empty(R ** 3, 4, dtype=torch.float32, device=dev)
         params_adj = torch.zeros(3, dtype=torch.float64, device=dev)
         p = eng.params(False)
         cst = eng.constants(False)
         stream = _lib.stream_handle()
-        grid, grid_tensors = eng.mechanics_grid()
-        work = [sim._allocate_like_current() for _ in range(min(self.every, self.steps) + 1)]
+        span = min(self.every, self.steps)
+        # One grid per substep of a segment: the forward run of substep t leaves its grid (and, in
+        # bounds[6:12], its active box) for the adjoint of substep t.
+        grids = pool["grids"]
+        while len(grids) < span:
+            grids.append(eng.mechanics_grid())
+        work = self._states("work", span + 1)
         adj_struct = adj.struct()
         for seg in range(len(self.checkpoints) - 1, -1, -1):
             first = seg * self.every
             length = min(self.every, self.steps - first)
             _copy_state(work[0], self.checkpoints[seg], self.is_ding)
-            for t in range(length - 1):
-                eng.run(work[t], work[t + 1], False, PHASE_MECHANICS, False, grid=grid)
+            for t in range(length):
+                eng.run(work[t], work[t + 1], False, PHASE_MECHANICS, False, grid=grids[t][0])
             for t in range(length - 1, -1, -1):
-                # Restore substep t's grid (P2G + grid update); its particle outputs are not used.
-                eng.run(work[t], work[length], False, PHASE_MECHANICS, False, grid=grid)
+                g = grids[t][1]
                 sin = state_struct(work[t], self.is_ding, False, False)
-                rc = self.fn(C.byref(p), C.byref(sin), C.byref(cst), _p(grid_tensors["node_pm"]),
-                             _p(grid_tensors["node_v"]), C.byref(adj_struct), C.byref(adj_struct),
+                rc = self.fn(C.byref(p), C.byref(sin), C.byref(cst), _p(g["node_pm"]), _p(g["node_v"]),
+                             g["bounds"].data_ptr() + 6 * 4, C.byref(adj_struct), C.byref(adj_struct),
                              _p(node_v_adj), _p(node_pm_adj), _p(params_adj), stream)
                 if rc != 0:
                     raise RuntimeError(f"bk_substep_adjoint failed ({rc}): "

@@ -198,6 +198,7 @@ class MpmSimulator:
         return state
 
     def Reset(self):
+        self._buffers.pop("rollout", None)  # reverse-mode buffers belong to the previous engine
         if isinstance(self.material, DingMaterial):
             self.material.Reset()
         self._stale = False

@@ -248,7 +248,8 @@ class SubstepEngine:
         empty = [2 ** 31 - 1] * 3 + [-2 ** 31] * 3
         tensors = dict(node_pm=torch.zeros(R ** 3, 4, dtype=torch.float32, device=dev),
                        node_v=torch.zeros(R ** 3, 4, dtype=torch.float32, device=dev),
-                       bounds=torch.tensor(empty + empty, dtype=torch.int32, device=dev))
+                       bounds=torch.tensor(empty + empty, dtype=torch.int32, device=dev),
+                       fields=self.fields, node_dT_ratio=self.node_dT_ratio)  # kept alive with the grid
         grid = BkGrid()
         grid.node_pm, grid.node_v, grid.bounds = (_p(tensors[k]) for k in ("node_pm", "node_v", "bounds"))
         grid.node_dT_ratio = _p(self.node_dT_ratio)

@@ -350,14 +350,17 @@ typedef struct BkAdjointState {
    Inputs: the substep's input state `in`, the grid that bk_substep left after running from `in`
    (node_pm, node_v: R^3 float4), and `out_adjoint` = dL/d(output state). Writes
    `in_adjoint` = dL/d(input state); `in_adjoint` may be the same arrays as `out_adjoint`.
-   `node_v_adjoint` and `node_pm_adjoint` are R^3 float4 scratch arrays. `parameter_adjoint`
+   `node_v_adjoint` and `node_pm_adjoint` are R^3 float4 scratch arrays. `node_box` (device, may be
+   NULL): that substep's active node box, BkGrid.bounds + 6 after bk_substep returned (inclusive
+   lo[3], hi[3]); with it only the box is visited and node_v_adjoint is left zero, so it must be
+   zero before the first call; without it node_v_adjoint is cleared and the whole grid visited. `parameter_adjoint`
    (device, float64, may be NULL) accumulates dL/d(shear modulus), dL/d(Lame lambda) and
    dL/d(viscosity parameter). Transport, gas and the coupled porosity solve are not covered
    (BK_ERR_UNSUPPORTED). */
 BK_API int bk_substep_adjoint(const BkSubstepParams *params, const BkState *in, const BkConstants *constants,
-                              const float *node_pm, const float *node_v, const BkAdjointState *out_adjoint,
-                              BkAdjointState *in_adjoint, float *node_v_adjoint, float *node_pm_adjoint,
-                              double *parameter_adjoint, void *stream);
+                              const float *node_pm, const float *node_v, const int32_t *node_box,
+                              const BkAdjointState *out_adjoint, BkAdjointState *in_adjoint, float *node_v_adjoint,
+                              float *node_pm_adjoint, double *parameter_adjoint, void *stream);
 
 /* ---- Return-map surrogate MLP (7 -> 64 -> 64 -> 3, SiLU; BF16 weights, FP32 accumulation) ----
    The reference has no learned component; these entry points serve the surrogate that may replace
