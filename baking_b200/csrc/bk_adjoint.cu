@@ -38,12 +38,13 @@ struct AdjParams {
     int R, bc;
     float origin[3], dx, dt, gravity[3];
     int material;  // 0 neo-Hookean, 1 Ding
+    int transport; // temperature is a transport field: its adjoint here is that of this substep's T_mat
     DingParamsDev ding;
 };
 
 // Adjoint of a particle state: same planes as BkState.
 struct AdjState {
-    float *x, *v, *C, *F, *Fe, *tau, *porosity, *temperature;
+    float *x, *v, *C, *F, *Fe, *tau, *porosity, *temperature, *mass;
 };
 
 // Slots of the principal-space derivative vector: the three singular values, then the parameters.
@@ -291,7 +292,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
 #pragma unroll
                 for (int c = 0; c < 9; ++c) { Fe_b[c] = out_adj.Fe[c * pitch + i]; tau_b[c] = out_adj.tau[c * pitch + i]; }
                 float por_b = out_adj.porosity[i];
-                Tb = out_adj.temperature[i];
+                Tb = P.transport ? 0.f : out_adj.temperature[i];
                 float por = in.porosity[i];
                 int gel = in.gelled[i];
                 float T = in.material_temperature[i];
@@ -502,7 +503,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
 #pragma unroll
                 for (int c = 0; c < 9; ++c) in_adj.Fe[c * pitch + i] = 0.f;
                 in_adj.porosity[i] = 0.f;
-                in_adj.temperature[i] = out_adj.temperature[i];
+                in_adj.temperature[i] = P.transport ? 0.f : out_adj.temperature[i];
             }
         }
     }
@@ -606,7 +607,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_p2g(AdjParams P, BkState in, c
 #pragma unroll
             for (int e = 0; e < 9; ++e) A[e] = m * Cm.m[e] - scale * tau.m[e];
             float vb[3] = {0.f, 0.f, 0.f}, Ab[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            float xg[3] = {0.f, 0.f, 0.f};
+            float xg[3] = {0.f, 0.f, 0.f}, mb = 0.f;
             const float inv_dx = 1.f / P.dx;
 #pragma unroll
             for (int ox = 0; ox < 3; ++ox)
@@ -632,6 +633,11 @@ __global__ void __launch_bounds__(kThreads) k_adj_p2g(AdjParams P, BkState in, c
                         }
                         float sdot = g.w * m + pb[0] * (m * vel.v[0] + Ad[0]) + pb[1] * (m * vel.v[1] + Ad[1]) +
                                      pb[2] * (m * vel.v[2] + Ad[2]);
+                        // node mass w m and momentum w m (v + C d): the particle-mass adjoint
+                        float Cd[3];
+#pragma unroll
+                        for (int r = 0; r < 3; ++r) Cd[r] = Cm.m[3 * r] * d[0] + Cm.m[3 * r + 1] * d[1] + Cm.m[3 * r + 2] * d[2];
+                        mb += w * (g.w + pb[0] * (vel.v[0] + Cd[0]) + pb[1] * (vel.v[1] + Cd[1]) + pb[2] * (vel.v[2] + Cd[2]));
 #pragma unroll
                         for (int a = 0; a < 3; ++a) {
                             float dw = qweight_grad(st.l[a], o[a]) * inv_dx;
@@ -649,6 +655,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_p2g(AdjParams P, BkState in, c
                 in_adj.x[c * pitch + i] += xg[c];
                 in_adj.v[c * pitch + i] = vb[c];
             }
+            if (in_adj.mass) in_adj.mass[i] = mb;
             // A = m C - scale tau
             float Cb[9], taub[9];
 #pragma unroll
@@ -685,6 +692,7 @@ __global__ void __launch_bounds__(kThreads) k_adj_p2g(AdjParams P, BkState in, c
                 acc_lam = trb * lj;
             }
         } else {
+            if (in_adj.mass) in_adj.mass[i] = 0.f;
 #pragma unroll
             for (int c = 0; c < 3; ++c) in_adj.v[c * pitch + i] = 0.f;
 #pragma unroll
@@ -707,6 +715,7 @@ AdjParams adj_params(const BkSubstepParams& p) {
     for (int k = 0; k < 3; ++k) { a.origin[k] = p.origin[k]; a.gravity[k] = p.gravity[k]; }
     a.dx = p.spacing; a.dt = p.time_step;
     a.material = p.material;
+    a.transport = p.transport;
     const BkDingParams& d = p.ding;
     a.ding.coupled_porosity = d.coupled_porosity; a.ding.temperature_enabled = d.temperature_enabled;
     a.ding.mu = d.shear_modulus; a.ding.lam = d.lame_lambda; a.ding.yield_stress = d.yield_stress;
@@ -723,6 +732,7 @@ AdjState adj_state(const BkAdjointState& s) {
     AdjState a;
     a.x = s.x; a.v = s.v; a.C = s.C; a.F = s.F; a.Fe = s.Fe; a.tau = s.tau; a.porosity = s.porosity;
     a.temperature = s.temperature;
+    a.mass = s.mass;
     return a;
 }
 
@@ -738,8 +748,10 @@ int bk_substep_adjoint(const BkSubstepParams* params, const BkState* in, const B
         !node_pm_adjoint)
         return bk::fail(BK_ERR_ARGUMENT, "bk_substep_adjoint: null argument");
     const BkSubstepParams& p = *params;
-    if (p.transport || p.gas)
-        return bk::fail(BK_ERR_UNSUPPORTED, "bk_substep_adjoint: the adjoint covers the mechanics substep (no transport/gas)");
+    if (p.gas || p.ding.coupled_porosity)
+        return bk::fail(BK_ERR_UNSUPPORTED, "bk_substep_adjoint: the gas (coupled porosity) substep has no adjoint");
+    if (p.transport && p.material != 1)
+        return bk::fail(BK_ERR_UNSUPPORTED, "bk_substep_adjoint: with transport the adjoint needs the Ding model");
     if (p.n < 0 || p.pitch < p.n || p.resolution < 4) return bk::fail(BK_ERR_ARGUMENT, "bk_substep_adjoint: bad sizes");
     if (p.material == 1 && (p.ding.coupled_porosity || !in->Fe || !in->tau || !in->porosity || !in->gelled ||
                             !in->material_temperature || !out_adjoint->Fe || !in_adjoint->Fe ||

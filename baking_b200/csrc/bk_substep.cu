@@ -53,6 +53,7 @@ struct Params {
     int water_enabled;
     float conductivity, diffusivity, s0, water_stress;
     float ambient, density, elastic_modulus, cfl, peak, width;
+    int keep_fields;
 };
 
 Params to_params(const BkSubstepParams& p) {
@@ -79,6 +80,7 @@ Params to_params(const BkSubstepParams& p) {
     k.water_stress = p.water_stress;
     k.ambient = p.gas_ambient_pressure; k.density = p.density; k.elastic_modulus = p.elastic_modulus;
     k.cfl = p.cfl_limit; k.peak = p.gas_peak; k.width = p.gas_width;
+    k.keep_fields = p.keep_transport_fields;
     return k;
 }
 
@@ -460,7 +462,7 @@ __global__ void k_grid_update(Params P, GridPtrs g) {
             out = make_float4(vel[0], vel[1], vel[2], 0.f);
         }
         g.v[i] = out;
-        if (P.transport) {
+        if (P.transport && !P.keep_fields) {
 #pragma unroll
             for (int k = 0; k < 7; ++k) g.f[k][i] = 0.0;
         }

@@ -64,7 +64,8 @@ class BkSubstepParams(C.Structure):
                 ("conductivity", C.c_float), ("diffusivity", C.c_float), ("initial_saturation", C.c_float),
                 ("water_stress", C.c_float), ("gas_ambient_pressure", C.c_float), ("density", C.c_float),
                 ("elastic_modulus", C.c_float), ("cfl_limit", C.c_float), ("gas_peak", C.c_float),
-                ("gas_width", C.c_float), ("surrogate", C.POINTER(BkReturnSurrogate))]
+                ("gas_width", C.c_float), ("surrogate", C.POINTER(BkReturnSurrogate)),
+                ("keep_transport_fields", C.c_int32)]
 
 
 PHASE_TRANSPORT = 1
@@ -240,26 +241,32 @@ class SubstepEngine:
             c.gas_rate_per_particle = int(rates.shape[0] == self.n and self.n > 1)
         return c
 
-    def mechanics_grid(self):
-        """A second grid for mechanics-only substeps (its own node arrays and active boxes), so that
-        recomputed substeps leave the simulator's grid holding its last substep."""
+    def mechanics_grid(self, own_transport=False):
+        """A second grid (its own node arrays and active boxes), so that recomputed substeps leave
+        the simulator's grid holding its last substep. With ``own_transport`` it also has its own
+        transport fields and node (dT, dW/W), which a run with keep_fields leaves in place."""
         R = self.sim.simulation_config.grid_resolution
         dev = self.sim.device
         empty = [2 ** 31 - 1] * 3 + [-2 ** 31] * 3
+        fields, dTr = self.fields, self.node_dT_ratio
+        if own_transport and self.transport:
+            fields = [torch.zeros(R ** 3, dtype=torch.float64, device=dev) for _ in range(7)]
+            dTr = torch.zeros(R ** 3, 2, dtype=torch.float64, device=dev)
         tensors = dict(node_pm=torch.zeros(R ** 3, 4, dtype=torch.float32, device=dev),
                        node_v=torch.zeros(R ** 3, 4, dtype=torch.float32, device=dev),
                        bounds=torch.tensor(empty + empty, dtype=torch.int32, device=dev),
-                       fields=self.fields, node_dT_ratio=self.node_dT_ratio)  # kept alive with the grid
+                       fields=fields, node_dT_ratio=dTr)  # kept alive with the grid
         grid = BkGrid()
         grid.node_pm, grid.node_v, grid.bounds = (_p(tensors[k]) for k in ("node_pm", "node_v", "bounds"))
-        grid.node_dT_ratio = _p(self.node_dT_ratio)
+        grid.node_dT_ratio = _p(dTr)
         for k in range(7):
-            grid.fields[k] = _p(self.fields[k])
+            grid.fields[k] = _p(fields[k])
         return grid, tensors
 
     # ---------------------------------------------------------------- launch
-    def run(self, state_in, state_out, settling, phases, full_diagnostics, grid=None):
+    def run(self, state_in, state_out, settling, phases, full_diagnostics, grid=None, keep_fields=False):
         p = self.params(settling)
+        p.keep_transport_fields = int(keep_fields)
         cst = self.constants(settling)
         sin = state_struct(state_in, self.is_ding, self.transport, self.gas)
         sout = state_struct(state_out, self.is_ding, self.transport, self.gas)

@@ -287,6 +287,8 @@ typedef struct BkSubstepParams {
     float conductivity, diffusivity, initial_saturation, water_stress;
     float gas_ambient_pressure, density, elastic_modulus, cfl_limit, gas_peak, gas_width;
     const BkReturnSurrogate *surrogate;  /* NULL: exact return map */
+    int32_t keep_transport_fields;  /* 1: the grid update leaves the transport node fields in place
+                                       (for bk_transport_adjoint, which clears them) */
 } BkSubstepParams;
 
 #define BK_PHASE_TRANSPORT 1       /* surface terms, scalar P2G, diffusion */
@@ -338,9 +340,11 @@ BK_API int bk_materialize(const BkSubstepParams *params, const BkState *state, c
    substep's contribution to the incoming value. */
 typedef struct BkAdjointState {
     float *x, *v, *C, *F;          /* 3, 3, 9, 9 planes */
-    float *Fe, *tau;               /* Ding, 9 planes */
+    float *Fe, *tau;               /* Ding, 9 planes; with transport tau is dL/d(the stress P2G used) */
     float *porosity;               /* Ding */
-    float *temperature;            /* Ding, accumulated over substeps */
+    float *temperature;            /* Ding material temperature: accumulated over substeps without
+                                      transport; with transport, dL/d(this substep's T_mat), written */
+    float *mass;                   /* may be NULL: dL/d(particle mass P2G used), written */
 } BkAdjointState;
 
 /* Reverse sweep of one mechanics substep (P2G, grid update, G2P, neo-Hookean stress or the
@@ -387,6 +391,35 @@ BK_API int bk_mlp_adam(const float *grads, float *params, float *first_moment, f
                        float learning_rate, float beta1, float beta2, float epsilon, void *stream);
 /* FP32 parameters -> packed BF16 operands + FP32 biases for bk_mlp_infer and the fused substep. */
 BK_API int bk_mlp_pack(const float *params, void *packed, void *stream);
+
+/* Transport half of the reverse sweep of one substep (Ding with thermal-water transport, gas off):
+   the surface heat/loss terms with their face areas, the scalar P2G, the diffusion stencil, the
+   scalar G2P, the water stress and the water-dependent mass (physics/thermal_water.py:77-253),
+   reversed. Node arrays are R^3 (node_dT_ratio: double2); all start at zero and are left at zero;
+   vertices: 3 planes of the surface's vertex_pitch, zero on entry, left zero. */
+typedef struct BkAdjointTransport {
+    const double *temperature_out, *water_out;  /* dL/d(T', W') of the substep's output */
+    double *temperature_in, *water_in;          /* dL/d(T, W) of its input (may alias the above) */
+    double *node_dT_ratio;                      /* node adjoint scratch of (dT, dW/W) */
+    double *node_fields[6];                     /* node adjoint scratch: volume, capacity, energy, water,
+                                                   heat, loss */
+    double *vertices;                           /* surface-vertex adjoint scratch */
+    double *heat_parameter;                     /* device [1], may be NULL: += dL/d(heat transfer) */
+} BkAdjointTransport;
+
+/* Before bk_substep_adjoint on a transport substep: the material temperature T + sum w dT, the
+   particle mass dry + W', and the stress tau - J c (s - s0) I that the forward P2G and return map
+   used, from the substep's input state and node (dT, dW/W) (n entries; stress: 9 planes). */
+BK_API int bk_transport_adjoint_prepare(const BkSubstepParams *params, const BkState *in,
+                                        const BkConstants *constants, const double *node_dT_ratio,
+                                        float *material_temperature, float *mass, float *stress, void *stream);
+/* After bk_substep_adjoint (whose tau, mass and temperature outputs are `mechanics`' inputs here,
+   and whose x and F outputs receive the transport terms): `grid` is the substep's forward grid run
+   with keep_transport_fields = 1, whose transport fields this call clears over the box in
+   grid->bounds + 6; `surface` the BkSurface of that substep. */
+BK_API int bk_transport_adjoint(const BkSubstepParams *params, const BkState *in, const BkConstants *constants,
+                                const BkGrid *grid, const BkSurface *surface, const BkAdjointState *mechanics,
+                                BkAdjointTransport *adjoint, void *stream);
 
 #ifdef __cplusplus
 }

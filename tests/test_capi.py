@@ -41,7 +41,7 @@ def test_bindings_match_declared_arity():
     bindings = dict(_lib.SIGNATURES)
     bindings.update(substep._SIGS)
     bindings.update(surrogate.SIGNATURES)
-    bindings["bk_substep_adjoint"] = adjoint._SIGNATURE
+    bindings.update(adjoint._SIGNATURES)
     for name, argtypes in bindings.items():
         assert name in funcs, f"{name} bound but not declared"
         assert len(argtypes) == funcs[name], f"{name}: {len(argtypes)} bound vs {funcs[name]} declared"

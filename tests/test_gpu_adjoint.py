@@ -1,5 +1,6 @@
 """Hand-written adjoint of the mechanics substep against finite differences and the reference's
-autodiff known answers (tests/test_warp_autodiff.py:27-58, tests/test_ding.py:140-171).
+autodiff known answers (tests/test_warp_autodiff.py:27-58, tests/test_ding.py:140-171). The
+transport substep's adjoint is checked in test_gpu_adjoint_transport.py with the same helpers.
 
 Every gradient is checked as a directional derivative: <dL/dtheta, delta> against the central
 difference (L(theta + eps delta) - L(theta - eps delta)) / (2 eps) of the float32 forward run.
@@ -123,16 +124,21 @@ def directional_check(make_sim, steps, name, delta, eps, checkpoint_every=2, rto
             return sim.material.viscosity_parameter.clone()
         if name == "young_modulus":
             return torch.tensor([sim.material.material_config.young_modulus], dtype=torch.float32, device="cuda")
+        if name == "heat_transfer_parameter":
+            return sim.transport.heat_transfer_parameter.clone()
         attr = {"positions": "particle_positions", "velocities": "particle_velocities",
                 "affine_velocities": "affine_velocities", "deformation_gradients": "deformation_gradients"}
         if name in attr:
             return getattr(st, attr[name]).clone()
+        transport = {"transport_temperatures": "temperatures", "water_masses": "water_masses"}
+        if name in transport:
+            return getattr(st.transport_state, transport[name]).clone()
         return getattr(st.material_state, name).clone()
 
     def run(scale, grad):
         sim = make_sim()
         theta = base_value(sim)
-        param = (theta.double() + scale * delta.double()).float().detach().requires_grad_(grad)
+        param = (theta.double() + scale * delta.double()).to(theta.dtype).detach().requires_grad_(grad)
         return param, Rollout(sim, steps, checkpoint_every=checkpoint_every, **{name: param})
 
     _, out0 = run(0.0, False)
@@ -244,11 +250,11 @@ def test_temperature_directional():
     directional_check(make, 5, "temperatures", _delta((n,), 19, 2.0), 0.5)
 
 
-def test_rollout_rejects_transport_and_unknown_inputs():
+def test_rollout_rejects_gas_and_unknown_inputs():
     from baking_b200.physics.adjoint import Rollout
-    from tests.scenes import build_transport
+    from tests.scenes import build_gas
     with pytest.raises(NotImplementedError):
-        Rollout(build_transport("cuda"), 1)
+        Rollout(build_gas("cuda"), 1)
     with pytest.raises(TypeError):
         Rollout(velocity_sim(), 1, gravity=1.0)
 
