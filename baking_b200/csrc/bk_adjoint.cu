@@ -17,6 +17,9 @@
 // they stay finite as two singular values coincide. The diagonal and parameter derivatives come
 // from a hand-written reverse sweep through the principal-space chain, including the implicit
 // overstress solve (derivatives as in the reference's SolveOverstressGradient, ding.py:90-100).
+// In gas mode the end-state porosity of the coupled solve (porous_return.py:43-61) is reversed
+// through its converged consistency equation, and the volume rescaling of Fe (ding.py:200-205)
+// as a common factor of its principal values.
 // Differentiable parameters: shear modulus, Lame lambda, the viscosity parameter and the
 // per-particle temperature (through the yield and viscosity factor tables). The gelation latch and
 // the wall and stencil switches are discrete; like the reference, no gradient flows through them.
@@ -192,6 +195,124 @@ __device__ void principal_vjp(const PrincipalFwd& f, const float* gb, const floa
     out[kMu] = mub; out[kLam] = lamb; out[kTy] = tyb; out[kEta] = etab; out[kA] = ab;
 }
 
+// End-state porosity of gas mode for the trial singular values s (ding.py:183-197); `r_warm`
+// returns the last overstress root. Out of line: the adjoint kernel's other paths keep their registers.
+struct CoupledFwd;
+__device__ __noinline__ float coupled_solve(const float* s, float mu, float lam, float ty, float eta, float dt,
+                                            float n0, float por, double* r_warm);
+
+// Inputs of the end-state porosity solve of gas mode (ding.py:183-196), computed from the trial
+// singular values in the forward's order of operations.
+struct CoupledFwd {
+    float eps[3], dev[3], tr, mean, ty, ty2, q, p, df, ms, ex, bulk, mu, lam, eta, dt;
+    double Vp;
+};
+
+__device__ CoupledFwd coupled_forward(const float* s, float mu, float lam, float ty, float eta, float dt, float n0,
+                                      float por) {
+    CoupledFwd c;
+    c.mu = mu; c.lam = lam; c.ty = ty; c.eta = eta; c.dt = dt;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) c.eps[k] = logf(s[k]);
+    c.tr = c.eps[0] + c.eps[1] + c.eps[2];
+    float ts[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ts[k] = 2.0f * mu * c.eps[k] + lam * c.tr;
+    c.mean = (ts[0] + ts[1] + ts[2]) / 3.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) c.dev[k] = ts[k] - c.mean;
+    c.ty2 = ty * ty;
+    c.q = 1.5f * (c.dev[0] * c.dev[0] + c.dev[1] * c.dev[1] + c.dev[2] * c.dev[2]) / c.ty2;
+    c.p = c.mean * c.mean / c.ty2;
+    c.df = 6.0f * mu * dt * ty * ty / eta;
+    c.bulk = 2.0f * mu + 3.0f * lam;
+    c.ms = 2.0f / 3.0f * c.bulk * dt * ty * ty / eta;
+    c.ex = 3.0f * c.mean / c.bulk;
+    c.Vp = 1.0 - (double)n0 + (double)por;
+    return c;
+}
+
+__device__ __noinline__ float coupled_solve(const float* s, float mu, float lam, float ty, float eta, float dt,
+                                            float n0, float por, double* r_warm) {
+    const CoupledFwd c = coupled_forward(s, mu, lam, ty, eta, dt, n0, por);
+    return solve_porosity(c.q, c.p, c.df, c.ms, c.ex, c.Vp, n0, r_warm);
+}
+
+// Reverse of n = solve_porosity(q, p, d, h, e, Vp): n is the root of n = pred(n; q, p, d, h, e, Vp)
+// with pred = Vp exp(e (1 - 1/v)) - 1 + n0, v = 1 + h a(n) r and r the overstress root of
+// r + 1 - q/(1+dr)^2 - a p/(1+h a r)^2 = 0. The implicit function theorem on the converged
+// equation (the derivatives of the reference's SolvePorosityGradient, porous_return.py:64-100)
+// gives theta_bar = nb dpred/dtheta / (1 - dpred/dn); the elastic early exit is the case r = 0.
+// Adds the result to the principal slots (singular values, mu, lambda, yield stress, viscosity)
+// and returns dL/d(old porosity) through Vp = 1 - n0 + n_old.
+__device__ __noinline__ float coupled_vjp(const float* s, float mu, float lam, float ty, float eta, float dt, float n0,
+                                          float por, double n, double nb, double r_warm, float* dpar) {
+    const CoupledFwd c = coupled_forward(s, mu, lam, ty, eta, dt, n0, por);
+    const double q = c.q, p = c.p, d = c.df, h = c.ms, e = c.ex, Vp = c.Vp;
+    const double a = pressure_coefficient64(n);
+    double r = r_warm;
+    r = overstress64(q, a * p, d, h * a, &r);
+    const double v = 1.0 + h * a * r;
+    const double E = exp(e * (1.0 - 1.0 / v));
+    const double K = Vp * E * e / (v * v);  // dpred/dv
+    double da = 0.0;
+    if (n > 0.0) {
+        const double lg = log(1.0 / n);
+        da = a * (2.0 / (n * lg) - 3.5 / (3.5 * n + 1.0));
+    }
+    double rq = 0.0, rp = 0.0, rd = 0.0, rh = 0.0;  // dr/d(q, a p, d, h a)
+    if (q + a * p > 1.0) {
+        const double u = 1.0 + d * r;
+        const double Fr = 1.0 + 2.0 * d * q / (u * u * u) + 2.0 * h * a * a * p / (v * v * v);
+        rq = 1.0 / (u * u * Fr);
+        rp = 1.0 / (v * v * Fr);
+        rd = -2.0 * q * r / (u * u * u * Fr);
+        rh = -2.0 * a * p * r / (v * v * v * Fr);
+    }
+    const double slope = K * h * da * (r + a * (rp * p + rh * h));
+    const double lm = nb / (1.0 - slope);
+    const float qb = (float)(lm * K * h * a * rq);
+    const float pb = (float)(lm * K * h * a * a * rp);
+    const float db = (float)(lm * K * h * a * rd);
+    const float hb = (float)(lm * K * (a * r + h * a * a * rh));
+    const float eb = (float)(lm * Vp * E * (1.0 - 1.0 / v));
+    // q = 1.5 |dev|^2 / ty2, p = mean^2 / ty2, d = 6 mu dt ty2 / eta, h = (2/3) bulk dt ty2 / eta,
+    // e = 3 mean / bulk
+    float devb[3], meanb = 0.f, ty2b = 0.f, mub = 0.f, lamb = 0.f, etab = 0.f, bulkb = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) devb[k] = qb * 3.f * c.dev[k] / c.ty2;
+    ty2b -= qb * c.q / c.ty2;
+    meanb += pb * 2.f * c.mean / c.ty2;
+    ty2b -= pb * c.p / c.ty2;
+    mub += db * 6.f * c.dt * c.ty2 / c.eta;
+    ty2b += db * 6.f * c.mu * c.dt / c.eta;
+    etab -= db * c.df / c.eta;
+    bulkb += hb * (2.f / 3.f) * c.dt * c.ty2 / c.eta;
+    ty2b += hb * (2.f / 3.f) * c.bulk * c.dt / c.eta;
+    etab -= hb * c.ms / c.eta;
+    meanb += eb * 3.f / c.bulk;
+    bulkb -= eb * c.ex / c.bulk;
+    mub += 2.f * bulkb;
+    lamb += 3.f * bulkb;
+    // dev_k = ts_k - mean, mean = sum ts / 3, ts_k = 2 mu eps_k + lam tr, eps_k = log s_k
+    meanb -= devb[0] + devb[1] + devb[2];
+    float tsb[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) tsb[k] = devb[k] + meanb / 3.f;
+    const float tsum = tsb[0] + tsb[1] + tsb[2];
+    lamb += c.tr * tsum;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        mub += 2.f * c.eps[k] * tsb[k];
+        dpar[kS0 + k] += (2.f * c.mu * tsb[k] + c.lam * tsum) * expf(-c.eps[k]);
+    }
+    dpar[kMu] += mub;
+    dpar[kLam] += lamb;
+    dpar[kTy] += 2.f * c.ty * ty2b;
+    dpar[kEta] += etab;
+    return (float)(lm * E);
+}
+
 __device__ __forceinline__ void add_m3(float* __restrict__ p, int64_t i, int64_t pitch, const float* a) {
 #pragma unroll
     for (int c = 0; c < 9; ++c) p[c * pitch + i] += a[c];
@@ -241,6 +362,8 @@ __device__ __forceinline__ float qweight_grad(float l, int o) {
 
 // ------------------------------------------------------------ G2P + return
 // params_adj: float64 [0] mu, [1] lambda, [2] viscosity parameter.
+// kCoupled: gas mode's coupled porosity (a separate instance, so the other modes keep their registers).
+template <bool kCoupled>
 __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkState in, const float4* __restrict__ grid_v,
                                                           const float* __restrict__ eta_param, AdjState out_adj,
                                                           AdjState in_adj, float4* __restrict__ grid_v_adj,
@@ -326,15 +449,29 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                 M3 U, V;
                 float s[3];
                 svd3f(trial, U, s, V);
-                float a = porosity_coefficient(por);
+                // Gas mode: the end-state porosity n_ret of the coupled solve sets a(n) of the
+                // return, and the returned Fe is rescaled to det F' / (1 - n0 + n_ret) (ding.py:183-205).
+                constexpr bool coupled = kCoupled;
+                float n_ret = por;
+                double r_warm = 0.0;
+                if (coupled) n_ret = coupled_solve(s, D.mu, D.lam, ty, eta, D.dt, D.initial_porosity, por, &r_warm);
+                float a = porosity_coefficient(n_ret);
                 PrincipalFwd pr = principal_forward(s, D.mu, D.lam, ty, eta, a, D.dt);
-                // porosity' = det(F') / prod(g) - 1 + n0 (uncoupled; zero when n0 = n = 0)
-                float prod_g = pr.g[0] * pr.g[1] * pr.g[2];
                 bool porosity_free = !(D.initial_porosity == 0.0f && por == 0.0f);
                 float detFn = det3(Fn);
+                float gv[3] = {pr.g[0], pr.g[1], pr.g[2]};  // principal values of the stored Fe'
                 float gb_por[3] = {0.f, 0.f, 0.f};
-                if (porosity_free && por_b != 0.f) {
-                    float npor = detFn / prod_g;
+                double nret_b = 0.0;
+                float cg = 1.f, target = 1.f;
+                if (coupled) {
+                    target = (float)(1.0 - (double)D.initial_porosity + (double)n_ret);
+                    cg = (float)cbrt((double)detFn / ((double)target * ((double)pr.g[0] * pr.g[1] * pr.g[2])));
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) gv[k] *= cg;
+                    if (porosity_free) nret_b += por_b;  // porosity' = n_ret
+                } else if (porosity_free && por_b != 0.f) {
+                    // porosity' = det(F') / prod(g) - 1 + n0 (uncoupled; zero when n0 = n = 0)
+                    float npor = detFn / (pr.g[0] * pr.g[1] * pr.g[2]);
                     // d/dF' det(F') = det(F') F'^-T
                     M3 inv = inverse3(Fn);
                     float scale_f = por_b * npor;
@@ -357,9 +494,33 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                 float* Ab = Abm.m;
                 float dpar[kDirs];
                 {
-                    const float gbar[3] = {Gh[0] + gb_por[0], Gh[4] + gb_por[1], Gh[8] + gb_por[2]};
+                    float gbar[3] = {Gh[0] + gb_por[0], Gh[4] + gb_por[1], Gh[8] + gb_por[2]};
+                    if (coupled) {
+                        // g'_k = cg g_k, cg = cbrt(det F' / (target prod g)): a common factor
+                        const float cgb = (Gh[0] * pr.g[0] + Gh[4] * pr.g[1] + Gh[8] * pr.g[2]) * (1.f / 3.f);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) gbar[k] = cg * (gbar[k] - cgb / pr.g[k]);
+                        const float lb = cgb * cg;  // dL/d log(det F' / target)
+                        M3 inv = inverse3(Fn);
+#pragma unroll
+                        for (int r = 0; r < 3; ++r)
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) Fb[3 * r + c] += lb * inv.m[3 * c + r];
+                        nret_b -= (double)(lb / target);
+                    }
                     const float hbar[3] = {Th[0], Th[4], Th[8]};
                     principal_vjp(pr, gbar, hbar, dpar);
+                }
+                float porb_coupled = 0.f;
+                if (coupled) {
+                    // a = a(n_ret), then the solve's inputs (s, mu, lambda, yield, viscosity, old n)
+                    if (n_ret > 0.0f) {
+                        const float lg = logf(1.0f / n_ret);
+                        nret_b += (double)(dpar[kA] * a * (2.0f / (n_ret * lg) - 3.5f / (3.5f * n_ret + 1.0f)));
+                    }
+                    if (nret_b != 0.0)
+                        porb_coupled = coupled_vjp(s, D.mu, D.lam, ty, eta, D.dt, D.initial_porosity, por,
+                                                   (double)n_ret, nret_b, r_warm, dpar);
                 }
                 Ab[0] = dpar[kS0];
                 Ab[4] = dpar[kS1];
@@ -377,7 +538,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                 for (int k = 0; k < 3; ++k) {
                     const int p = k == 2 ? 1 : 0;
                     const int q = k == 0 ? 1 : 2;
-                    const float sp = s[p], sq = s[q], gp = pr.g[p], gq = pr.g[q];
+                    const float sp = s[p], sq = s[q], gp = gv[p], gq = gv[q];
                     const float L = log1pf((sq - sp) / sp);
                     float ratio = 1.f / one_dr, xo = 1.f;
                     if (fabsf(L) >= 1e-12f) {
@@ -416,8 +577,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                 acc_lam = dpar[kLam];
                 acc_eta = dpar[kEta] * eta_factor;
                 Tb += dpar[kTy] * dty_dT + dpar[kEta] * deta_dT;
-                // porosity -> a(n) (zero at n = 0)
-                if (por > 0.0f) {
+                // porosity -> a(n) (zero at n = 0); in gas mode through the coupled solve
+                if (coupled) {
+                    porb_in = porb_coupled;
+                } else if (por > 0.0f) {
                     float lg = logf(1.0f / por);
                     float da = a * (2.0f / (por * lg) - 3.5f / (3.5f * por + 1.0f));
                     porb_in = dpar[kA] * da;
@@ -748,12 +911,12 @@ int bk_substep_adjoint(const BkSubstepParams* params, const BkState* in, const B
         !node_pm_adjoint)
         return bk::fail(BK_ERR_ARGUMENT, "bk_substep_adjoint: null argument");
     const BkSubstepParams& p = *params;
-    if (p.gas || p.ding.coupled_porosity)
-        return bk::fail(BK_ERR_UNSUPPORTED, "bk_substep_adjoint: the gas (coupled porosity) substep has no adjoint");
+    if (p.gas && !p.transport)
+        return bk::fail(BK_ERR_UNSUPPORTED, "bk_substep_adjoint: gas mode runs with transport");
     if (p.transport && p.material != 1)
         return bk::fail(BK_ERR_UNSUPPORTED, "bk_substep_adjoint: with transport the adjoint needs the Ding model");
     if (p.n < 0 || p.pitch < p.n || p.resolution < 4) return bk::fail(BK_ERR_ARGUMENT, "bk_substep_adjoint: bad sizes");
-    if (p.material == 1 && (p.ding.coupled_porosity || !in->Fe || !in->tau || !in->porosity || !in->gelled ||
+    if (p.material == 1 && (!in->Fe || !in->tau || !in->porosity || !in->gelled ||
                             !in->material_temperature || !out_adjoint->Fe || !in_adjoint->Fe ||
                             !constants->viscosity_parameter))
         return bk::fail(BK_ERR_ARGUMENT, "bk_substep_adjoint: missing Ding arrays");
@@ -764,10 +927,16 @@ int bk_substep_adjoint(const BkSubstepParams* params, const BkState* in, const B
     const int64_t nodes = (int64_t)p.resolution * p.resolution * p.resolution;
     if (!node_box) cudaMemsetAsync(node_v_adjoint, 0, nodes * sizeof(float4), s);
     unsigned blocks = (unsigned)((p.n + kThreads - 1) / kThreads);
-    k_adj_g2p_return<<<blocks, kThreads, 0, s>>>(a, *in, reinterpret_cast<const float4*>(node_v),
-                                                 constants->viscosity_parameter, adj_state(*out_adjoint),
-                                                 adj_state(*in_adjoint), reinterpret_cast<float4*>(node_v_adjoint),
-                                                 parameter_adjoint);
+    if (p.material == 1 && p.ding.coupled_porosity)
+        k_adj_g2p_return<true><<<blocks, kThreads, 0, s>>>(a, *in, reinterpret_cast<const float4*>(node_v),
+                                                         constants->viscosity_parameter, adj_state(*out_adjoint),
+                                                         adj_state(*in_adjoint), reinterpret_cast<float4*>(node_v_adjoint),
+                                                         parameter_adjoint);
+    else
+        k_adj_g2p_return<false><<<blocks, kThreads, 0, s>>>(a, *in, reinterpret_cast<const float4*>(node_v),
+                                                          constants->viscosity_parameter, adj_state(*out_adjoint),
+                                                          adj_state(*in_adjoint), reinterpret_cast<float4*>(node_v_adjoint),
+                                                          parameter_adjoint);
     if (int rc = bk::check_launch("bk_substep_adjoint/g2p_return")) return rc;
     if (node_box) {
         int device = 0, sms = 148;

@@ -1,15 +1,17 @@
-// Adjoint of the thermal-water transport part of one substep (gas off), the companion of
+// Adjoint of the thermal-water transport part of one substep, the companion of
 // bk_substep_adjoint: the forward transport phase (physics/thermal_water.py:77-190 -- surface
 // areas, scalar P2G, diffusion) and the scalar G2P with its water stress and mass
-// (thermal_water.py:193-229, 248-253) reversed, given the substep's grid with its transport fields
+// (thermal_water.py:193-229, 248-253) and, in gas mode, its local gas source and gas-pressure
+// stress (thermal_water.py:232-245, physics/materials/gas.py:16-35) reversed, given the substep's
+// grid with its transport fields
 // kept (BkSubstepParams.keep_transport_fields) and the adjoints the mechanics adjoint produced for
 // the stress, particle mass and material temperature that P2G and the return map used.
 //
 // Order, all per substep:
-//   prepare          T_mat = T + sum w dT, mass = dry + W', stress tau - J c (s - s0) I: the
-//                    inputs bk_substep_adjoint needs (call before it)
-//   scalar_chain     dL/d(T', W', T_mat, mass, stress) -> dL/d(T, W, F, x) and the node adjoints
-//                    of (dT, dW/W)
+//   prepare          T_mat = T + sum w dT, mass = dry + W', stress tau + J (p_amb - p) I
+//                    - J c (s - s0) I: the inputs bk_substep_adjoint needs (call before it)
+//   scalar_chain     dL/d(T', W', N', T_mat, mass, stress) -> dL/d(T, W, N, n, F, x, alpha) and
+//                    the node adjoints of (dT, dW/W)
 //   diffuse          node gather: dL/d(dT, dW/W) -> dL/d(volume, capacity, energy, water, heat, loss)
 //   scatter          particle gather of the node-field adjoints -> dL/d(F, T, W, x)
 //   owners           surface heat/loss of face-owning particles -> dL/d(T, W, F, x, h) and the
@@ -47,6 +49,8 @@ struct TParams {
     int water_enabled;
     double oven, tray, tray_transfer, surface_loss, latent;
     double contact_limit;  // floor height + contact distance, summed in float as the forward does
+    int gas, settling;
+    double ambient, peak, width, source_scale;  // gas: ambient pressure, source peak/width, dt * density
 };
 
 __device__ __forceinline__ float qgrad(float l, int o) {
@@ -80,6 +84,22 @@ __device__ __forceinline__ void add_det_grad(float* Fb, int64_t i, int64_t pitch
         for (int c = 0; c < 3; ++c) Fb[(3 * r + c) * pitch + i] += scale * J * inv.m[3 * c + r];
 }
 
+// Gas content after this substep's local source (thermal_water.py:238-245):
+// N' = N + dt rho alpha exp(-z^2), z = ((T + T')/2 - T_peak) / width; no source while settling.
+// `ez`, `z` (may be NULL) return exp(-z^2) and z.
+__device__ __forceinline__ double source_moles(const TParams& P, const BkState& in, const BkConstants& cst, int64_t i,
+                                               double T, double Tn, double* ez, double* z) {
+    double N = in.gas_moles[i];
+    if (!P.settling) {
+        const double zz = (0.5 * (T + Tn) - P.peak) / P.width;
+        const double e = exp(-(zz * zz));
+        N += P.source_scale * (double)cst.gas_rate[cst.gas_rate_per_particle ? i : 0] * e;
+        if (ez) *ez = e;
+        if (z) *z = zz;
+    }
+    return N;
+}
+
 // ------------------------------------------------------------------ prepare
 __global__ void k_tadj_prepare(TParams P, BkState in, BkConstants cst, const double2* __restrict__ dTr,
                                float* __restrict__ T_mat, float* __restrict__ mass, float* __restrict__ tau_eff) {
@@ -98,14 +118,24 @@ __global__ void k_tadj_prepare(TParams P, BkState in, BkConstants cst, const dou
         dTp += w * d.x;
         ratio += w * d.y;
     }
-    const double Tn = in.temperature[i] + dTp, Wn = in.water[i] * (1.0 + ratio);
+    const double T = in.temperature[i];
+    const double Tn = T + dTp, Wn = in.water[i] * (1.0 + ratio);
     T_mat[i] = (float)Tn;
     mass[i] = (float)(cst.dry_mass[i] + Wn);
     const M3 F = load_m3(in.F, i, pitch);
     const float J = det3(F);
+    M3 tau = load_m3(in.tau, i, pitch);
+    if (P.gas) {
+        const float n = in.porosity[i];
+        if (n > 0.0f && n < 1.0f && isfinite(n) && J > 0.0f) {
+            const float p = (float)gas_pressure(source_moles(P, in, cst, i, T, Tn, nullptr, nullptr), (float)Tn, J, n);
+            const float iso = J * ((float)P.ambient - p);
+#pragma unroll
+            for (int e = 0; e < 9; ++e) tau.m[e] += (e % 4) == 0 ? iso : 0.0f;
+        }
+    }
     const double sat = Wn / (P.rho_w * (double)cst.volume[i] * (double)J);
     const float iso = J * (float)P.c_water * ((float)sat - (float)P.s0);
-    M3 tau = load_m3(in.tau, i, pitch);
 #pragma unroll
     for (int e = 0; e < 9; ++e) tau.m[e] -= (e % 4) == 0 ? iso : 0.0f;
     store_m3(tau_eff, i, pitch, tau);
@@ -116,62 +146,103 @@ __global__ void __launch_bounds__(kThreads) k_tadj_scalar(TParams P, BkState in,
                                                         const double2* __restrict__ dTr, BkAdjointTransport a,
                                                         const BkAdjointState adj, double2* __restrict__ dTr_bar) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
     const int64_t pitch = P.pitch;
-    Stencil st = make_stencil(load_v3(in.x, i, pitch), P.origin, P.dx, P.R);
-    if (!st.valid) {
+    double rate_b = 0.0;  // dL/d(gas source rate) through this particle
+    Stencil st;
+    st.valid = false;
+    if (i < P.n) st = make_stencil(load_v3(in.x, i, pitch), P.origin, P.dx, P.R);
+    if (i < P.n && !st.valid) {
         a.temperature_in[i] = 0.0;
         a.water_in[i] = 0.0;
-        return;
-    }
-    double dTp = 0.0, ratio = 0.0;
+        if (P.gas) a.gas_moles_in[i] = 0.0;
+    } else if (i < P.n) {
+        double dTp = 0.0, ratio = 0.0;
 #pragma unroll
-    for (int j = 0; j < 27; ++j) {
-        int ox, oy, oz;
-        node_offset(j, ox, oy, oz);
-        const double w = (double)(st.w[0][ox] * st.w[1][oy] * st.w[2][oz]);
-        const double2 d = dTr[node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R)];
-        dTp += w * d.x;
-        ratio += w * d.y;
-    }
-    const double W = in.water[i], Wn = W * (1.0 + ratio);
-    const M3 F = load_m3(in.F, i, pitch);
-    const double J = (double)det3(F);
-    const double V0 = (double)cst.volume[i];
-    const double sat = Wn / (P.rho_w * V0 * J);
-    // adjoints arriving at T', W', T_mat, mass and the P2G stress
-    double Tnb = a.temperature_out[i] + (double)adj.temperature[i];
-    double Wnb = a.water_out[i] + (double)adj.mass[i];
-    const double trace = (double)adj.tau[i] + (double)adj.tau[4 * pitch + i] + (double)adj.tau[8 * pitch + i];
-    // stress -= iso I, iso = J c (s - s0)
-    const double isob = -trace;
-    double Jb = isob * P.c_water * (sat - P.s0);
-    const double satb = isob * J * P.c_water;
-    Wnb += satb / (P.rho_w * V0 * J);
-    Jb -= satb * sat / J;
-    // W' = W (1 + sum w r), T' = T + sum w dT
-    const double ratiob = Wnb * W;
-    a.water_in[i] = Wnb * (1.0 + ratio);
-    a.temperature_in[i] = Tnb;
-    const float inv_dx = 1.f / P.dx;
-    float xg[3] = {0.f, 0.f, 0.f};
+        for (int j = 0; j < 27; ++j) {
+            int ox, oy, oz;
+            node_offset(j, ox, oy, oz);
+            const double w = (double)(st.w[0][ox] * st.w[1][oy] * st.w[2][oz]);
+            const double2 d = dTr[node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R)];
+            dTp += w * d.x;
+            ratio += w * d.y;
+        }
+        const double T = in.temperature[i], Tn = T + dTp;
+        const double W = in.water[i], Wn = W * (1.0 + ratio);
+        const M3 F = load_m3(in.F, i, pitch);
+        const float Jf = det3(F);
+        const double J = (double)Jf;
+        const double V0 = (double)cst.volume[i];
+        const double sat = Wn / (P.rho_w * V0 * J);
+        // adjoints arriving at T', W', T_mat, mass and the P2G stress
+        double Tnb = a.temperature_out[i] + (double)adj.temperature[i];
+        double Wnb = a.water_out[i] + (double)adj.mass[i];
+        const double trace = (double)adj.tau[i] + (double)adj.tau[4 * pitch + i] + (double)adj.tau[8 * pitch + i];
+        // stress -= iso I, iso = J c (s - s0)
+        const double isob = -trace;
+        double Jb = isob * P.c_water * (sat - P.s0);
+        const double satb = isob * J * P.c_water;
+        Wnb += satb / (P.rho_w * V0 * J);
+        Jb -= satb * sat / J;
+        double Tb_direct = 0.0;  // through the source's mean temperature, besides T'
+        if (P.gas) {
+            double ez = 0.0, z = 0.0;
+            const double Np = source_moles(P, in, cst, i, T, Tn, &ez, &z);
+            double Npb = a.gas_moles_out[i];
+            const float n = in.porosity[i];
+            if (n > 0.0f && n < 1.0f && isfinite(n) && Jf > 0.0f) {
+                // stress += J (p_amb - p) I, p = N' R T_mat / (J n) (gas.py:11-13, 27-29)
+                const float Tm = (float)Tn;
+                const double pg = (double)(float)gas_pressure(Np, Tm, Jf, n);
+                Jb += trace * (P.ambient - pg);
+                const double pb = -trace * J;
+                Npb += pb * kGasConstant * (double)Tm / (J * (double)n);
+                Tnb += pb * pg / (double)Tm;
+                Jb -= pb * pg / J;
+                adj.porosity[i] += (float)(-pb * pg / (double)n);
+            }
+            a.gas_moles_in[i] = Npb;
+            if (!P.settling) {
+                const double rate = (double)cst.gas_rate[cst.gas_rate_per_particle ? i : 0];
+                rate_b = Npb * P.source_scale * ez;
+                const double zb = Npb * P.source_scale * rate * ez * (-2.0 * z);
+                Tnb += zb * 0.5 / P.width;
+                Tb_direct = zb * 0.5 / P.width;
+            }
+        }
+        // W' = W (1 + sum w r), T' = T + sum w dT
+        const double ratiob = Wnb * W;
+        a.water_in[i] = Wnb * (1.0 + ratio);
+        a.temperature_in[i] = Tnb + Tb_direct;
+        const float inv_dx = 1.f / P.dx;
+        float xg[3] = {0.f, 0.f, 0.f};
 #pragma unroll 1
-    for (int j = 0; j < 27; ++j) {
-        int ox, oy, oz;
-        node_offset(j, ox, oy, oz);
-        float dw[3];
-        const double w = (double)weight_and_grad(st, ox, oy, oz, inv_dx, dw);
-        const int64_t node = node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R);
-        const double2 d = dTr[node];
-        atomicAdd(&dTr_bar[node].x, w * Tnb);
-        atomicAdd(&dTr_bar[node].y, w * ratiob);
-        const float s = (float)(d.x * Tnb + d.y * ratiob);
+        for (int j = 0; j < 27; ++j) {
+            int ox, oy, oz;
+            node_offset(j, ox, oy, oz);
+            float dw[3];
+            const double w = (double)weight_and_grad(st, ox, oy, oz, inv_dx, dw);
+            const int64_t node = node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R);
+            const double2 d = dTr[node];
+            atomicAdd(&dTr_bar[node].x, w * Tnb);
+            atomicAdd(&dTr_bar[node].y, w * ratiob);
+            const float s = (float)(d.x * Tnb + d.y * ratiob);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) xg[c] += dw[c] * s;
+            for (int c = 0; c < 3; ++c) xg[c] += dw[c] * s;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) adj.x[c * pitch + i] += xg[c];
+        add_det_grad(adj.F, i, pitch, F, (float)Jb);
     }
+    if (P.gas && a.gas_rate) {
+        if (cst.gas_rate_per_particle) {
+            if (i < P.n) a.gas_rate[i] += rate_b;
+        } else {
+            // one shared rate: a warp sum, then one atomic per warp
 #pragma unroll
-    for (int c = 0; c < 3; ++c) adj.x[c * pitch + i] += xg[c];
-    add_det_grad(adj.F, i, pitch, F, (float)Jb);
+            for (int o = 16; o > 0; o >>= 1) rate_b += __shfl_xor_sync(0xffffffffu, rate_b, o);
+            if ((threadIdx.x & 31) == 0 && rate_b != 0.0) atomicAdd(a.gas_rate, rate_b);
+        }
+    }
 }
 
 // ------------------------------------------------------------------ diffuse
@@ -514,6 +585,12 @@ TParams tparams(const BkSubstepParams& p, const BkSurface* sf) {
     t.oven = p.scalar.oven_temperature; t.tray = p.scalar.tray_temperature;
     t.tray_transfer = p.scalar.tray_transfer; t.surface_loss = p.scalar.surface_loss; t.latent = p.scalar.latent_heat;
     t.contact_limit = sf ? (double)(sf->floor_height + sf->contact_distance) : 0.0;
+    t.gas = p.gas;
+    t.settling = p.settling;
+    t.ambient = p.gas_ambient_pressure;
+    t.peak = p.gas_peak;
+    t.width = p.gas_width;
+    t.source_scale = (double)(p.time_step * p.density);
     return t;
 }
 
@@ -531,6 +608,8 @@ int bk_transport_adjoint_prepare(const BkSubstepParams* params, const BkState* i
     const BkSubstepParams& p = *params;
     if (!p.transport || p.material != 1 || !in->temperature || !in->water || !in->tau || !constants->dry_mass)
         return fail(BK_ERR_ARGUMENT, "bk_transport_adjoint_prepare: needs the Ding model with transport");
+    if (p.gas && (!in->gas_moles || !in->porosity || !constants->gas_rate))
+        return fail(BK_ERR_ARGUMENT, "bk_transport_adjoint_prepare: gas mode needs the gas arrays");
     if (p.n == 0) return BK_OK;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     k_tadj_prepare<<<blocks(p.n, 256), 256, 0, s>>>(tparams(p, nullptr), *in, *constants,
@@ -545,8 +624,11 @@ int bk_transport_adjoint(const BkSubstepParams* params, const BkState* in, const
     if (!params || !in || !constants || !grid || !surface || !mechanics || !adjoint)
         return fail(BK_ERR_ARGUMENT, "bk_transport_adjoint: null argument");
     const BkSubstepParams& p = *params;
-    if (!p.transport || p.material != 1 || p.gas)
-        return fail(BK_ERR_UNSUPPORTED, "bk_transport_adjoint: the Ding model with transport and without gas");
+    if (!p.transport || p.material != 1)
+        return fail(BK_ERR_UNSUPPORTED, "bk_transport_adjoint: the Ding model with transport");
+    if (p.gas && (!in->gas_moles || !in->porosity || !constants->gas_rate || !adjoint->gas_moles_out ||
+                  !adjoint->gas_moles_in || !mechanics->porosity))
+        return fail(BK_ERR_ARGUMENT, "bk_transport_adjoint: gas mode needs the gas arrays and their adjoints");
     const BkAdjointTransport& a = *adjoint;
     if (!a.temperature_out || !a.water_out || !a.temperature_in || !a.water_in || !a.node_dT_ratio || !a.vertices ||
         !mechanics->tau || !mechanics->mass || !mechanics->temperature || !mechanics->x || !mechanics->F)

@@ -11,16 +11,18 @@ tests/test_ding_thermal.py:160-190). Here :func:`Rollout` runs ``steps`` substep
 * backward: per checkpoint segment, latest first, the segment's substeps are re-run from its
   checkpoint, each on a grid of its own so that the grid (with transport, also its node fields)
   stays for its reverse step; each substep is then reversed by ``bk_substep_adjoint`` (G2P +
-  return map, grid update, P2G) and, with transport, by ``bk_transport_adjoint`` (scalar G2P with
-  the water stress and particle mass, diffusion, scalar P2G, surface heat and loss through the
+  return map with, in gas mode, the coupled end-state porosity solve, grid update, P2G) and, with
+  transport, by ``bk_transport_adjoint`` (scalar G2P with the water stress and particle mass, the
+  gas source and gas-pressure stress, diffusion, scalar P2G, surface heat and loss through the
   mesh face areas).
 
 Memory is one state per checkpoint plus ``checkpoint_every`` states and grids, instead of one
-state and one grid per substep. Covered: neo-Hookean and Ding (uncoupled porosity) materials,
-with or without thermal-water transport, gas off, after settling. Gradients reach the initial
-positions, velocities, affine velocities, deformation gradients, Ding elastic gradients, stresses
-and porosities, the material temperatures without transport or the transport temperatures and
-water masses with it, the viscosity parameter, Young's modulus and the heat-transfer parameter.
+state and one grid per substep. Covered: neo-Hookean and Ding materials, with or without
+thermal-water transport and gas, after settling. Gradients reach the initial positions,
+velocities, affine velocities, deformation gradients, Ding elastic gradients, stresses and
+porosities, the material temperatures without transport or the transport temperatures and water
+masses with it, the gas content, the viscosity parameter, Young's modulus, the heat-transfer
+parameter and the gas source rates (one shared or one per particle).
 Discrete switches (gelation latch, wall clamping, stencil validity, tray contact, nodes without
 capacity) carry no gradient, as in the reference.
 """
@@ -46,7 +48,8 @@ class BkAdjointState(C.Structure):
 
 class BkAdjointTransport(C.Structure):
     _fields_ = [("temperature_out", P), ("water_out", P), ("temperature_in", P), ("water_in", P),
-                ("node_dT_ratio", P), ("node_fields", P * 6), ("vertices", P), ("heat_parameter", P)]
+                ("node_dT_ratio", P), ("node_fields", P * 6), ("vertices", P), ("heat_parameter", P),
+                ("gas_moles_out", P), ("gas_moles_in", P), ("gas_rate", P)]
 
 
 _SIGNATURE = [P] * 11 + [P]
@@ -62,6 +65,7 @@ _KINEMATIC = (("positions", "particle_positions"), ("velocities", "particle_velo
 _DING = (("elastic_gradients", "elastic_gradients"), ("kirchhoff_stresses", "kirchhoff_stresses"),
          ("porosities", "porosities"), ("temperatures", "temperatures"))
 _DING_DISCRETE = ("gelled",)
+_GAS = (("gas_moles", "gas_moles"),)
 _TRANSPORT = (("transport_temperatures", "temperatures"), ("water_masses", "water_masses"))
 
 
@@ -78,38 +82,40 @@ def _p(t):
     return None if t is None else t.data_ptr()
 
 
-def _keys(is_ding, transport):
+def _keys(is_ding, transport, gas=False):
     return [k for k, _ in _KINEMATIC] + ([k for k, _ in _DING] if is_ding else []) + \
-        ([k for k, _ in _TRANSPORT] if transport else [])
+        ([k for k, _ in _GAS] if gas else []) + ([k for k, _ in _TRANSPORT] if transport else [])
 
 
-def _arrays_of(state, is_ding, transport):
-    """The primary arrays of a state: kinematic, Ding (the gelation latch last), transport."""
+def _arrays_of(state, is_ding, transport, gas=False):
+    """The primary arrays of a state: kinematic, Ding (then the gelation latch), gas, transport."""
     out = [getattr(state, attr) for _, attr in _KINEMATIC]
     if is_ding:
         m = state.material_state
         out += [getattr(m, attr) for _, attr in _DING] + [getattr(m, a) for a in _DING_DISCRETE]
+        if gas:
+            out += [getattr(m, attr) for _, attr in _GAS]
     if transport:
         t = state.transport_state
         out += [getattr(t, attr) for _, attr in _TRANSPORT]
     return out
 
 
-def _outputs_of(state, is_ding, transport):
+def _outputs_of(state, is_ding, transport, gas=False):
     """The differentiable arrays of a state, in the order of ``_keys``."""
-    arrs = _arrays_of(state, is_ding, transport)
+    arrs = _arrays_of(state, is_ding, transport, gas)
     return arrs[:8] + arrs[9:] if is_ding else arrs
 
 
-def _copy_state(dst, src, is_ding, transport):
-    for d, s in zip(_arrays_of(dst, is_ding, transport), _arrays_of(src, is_ding, transport)):
+def _copy_state(dst, src, is_ding, transport, gas=False):
+    for d, s in zip(_arrays_of(dst, is_ding, transport, gas), _arrays_of(src, is_ding, transport, gas)):
         d.copy_(s)
 
 
 class _AdjointBuffers:
     """Adjoint state in the plane layout (updated in place, substep by substep)."""
 
-    def __init__(self, n, pitch, device, is_ding, transport):
+    def __init__(self, n, pitch, device, is_ding, transport, gas=False):
         self.x = arrays.vec3s(n, device=device, pitch=pitch)
         self.v = arrays.vec3s(n, device=device, pitch=pitch)
         self.C = arrays.mat33s(n, device=device, pitch=pitch)
@@ -119,6 +125,7 @@ class _AdjointBuffers:
         self.porosity = arrays.scalars(n, device=device, pitch=pitch) if is_ding else None
         self.temperature = arrays.scalars(n, device=device, pitch=pitch) if is_ding else None
         self.mass = arrays.scalars(n, device=device, pitch=pitch) if transport else None
+        self.N = arrays.scalars(n, torch.float64, device) if gas else None
         self.T = arrays.scalars(n, torch.float64, device) if transport else None
         self.W = arrays.scalars(n, torch.float64, device) if transport else None
 
@@ -127,6 +134,8 @@ class _AdjointBuffers:
         out = [self.x, self.v, self.C, self.F]
         if self.Fe is not None:
             out += [self.Fe, self.tau, self.porosity, self.temperature]
+        if self.N is not None:
+            out.append(self.N)
         if self.T is not None:
             out += [self.T, self.W]
         return out
@@ -145,8 +154,7 @@ class _Runner:
     def __init__(self, sim, steps, checkpoint_every):
         self.is_ding = isinstance(sim.material, DingMaterial)
         self.transport = sim.transport is not None
-        if self.is_ding and sim.material.ding_config.gas_enabled:
-            raise NotImplementedError("the gas (coupled porosity) substep has no adjoint here")
+        self.gas = bool(self.is_ding and sim.material.ding_config.gas_enabled)
         if self.transport and not self.is_ding:
             raise NotImplementedError("with transport the adjoint needs the ding2019 material")
         if sim.IsSettling:
@@ -176,7 +184,7 @@ class _Runner:
     def _snapshot(self, state):
         snaps = self._states("snapshots", len(self.checkpoints) + 1)
         snap = snaps[len(self.checkpoints)]
-        _copy_state(snap, state, self.is_ding, self.transport)
+        _copy_state(snap, state, self.is_ding, self.transport, self.gas)
         return snap
 
     def _set_young_modulus(self, E):
@@ -188,8 +196,8 @@ class _Runner:
         if self.transport and inputs.get("temperatures") is not None:
             raise ValueError("with transport set transport_temperatures (the material temperature follows them)")
         state = sim.current_state
-        for name, target in zip(_keys(self.is_ding, self.transport),
-                                _outputs_of(state, self.is_ding, self.transport)):
+        for name, target in zip(_keys(self.is_ding, self.transport, self.gas),
+                                _outputs_of(state, self.is_ding, self.transport, self.gas)):
             value = inputs.get(name)
             if value is not None:
                 target.copy_(value.detach().reshape(target.shape))
@@ -197,6 +205,10 @@ class _Runner:
             if not self.is_ding:
                 raise ValueError("viscosity_parameter needs the ding2019 material")
             sim.material.viscosity_parameter.copy_(inputs["viscosity_parameter"].detach().reshape(1))
+        if inputs.get("gas_source_rates") is not None:
+            if not self.gas:
+                raise ValueError("gas_source_rates needs gas mode")
+            sim.SetGasSourceRates(inputs["gas_source_rates"].detach().reshape(-1).cpu().numpy())
         if inputs.get("heat_transfer_parameter") is not None:
             if not self.transport:
                 raise ValueError("heat_transfer_parameter needs transport")
@@ -217,7 +229,7 @@ class _Runner:
         if messages:
             raise RuntimeError(messages[0] + " (during Rollout)")
         final = sim.current_state  # with transport this also fills the material temperature from T
-        return tuple(t.detach().clone() for t in _outputs_of(final, self.is_ding, self.transport))
+        return tuple(t.detach().clone() for t in _outputs_of(final, self.is_ding, self.transport, self.gas))
 
     # ---------------------------------------------------------------- backward
     def _check(self, rc, name):
@@ -244,7 +256,10 @@ class _Runner:
             t["owner_loss"] = torch.zeros_like(src["owner_loss"])
             surface.owner_heat, surface.owner_loss = _p(t["owner_heat"]), _p(t["owner_loss"])
         if eng.surface.vertex_count > 0:
-            t["surface_vertices"] = torch.empty_like(self.sim.surface_vertices_buffer())
+            # Plane layout with the surface's vertex pitch, as the vertex kernels index it
+            # (empty_like of the strided view would return a row-major n x 3 buffer).
+            verts = self.sim.surface_vertices_buffer()
+            t["surface_vertices"] = arrays.vec3s(verts.shape[0], device=dev, pitch=int(eng.surface.vertex_pitch))
             surface.vertices = _p(t["surface_vertices"])
         t["surface"] = surface
         pool["transport"] = t
@@ -266,7 +281,7 @@ class _Runner:
         n, pitch, dev = eng.n, eng.pitch, sim.device
         R = sim.simulation_config.grid_resolution
         if pool.get("adjoint") is None:
-            pool["adjoint"] = _AdjointBuffers(n, pitch, dev, self.is_ding, self.transport)
+            pool["adjoint"] = _AdjointBuffers(n, pitch, dev, self.is_ding, self.transport, self.gas)
             # node_v_adj must be zero before the first call; each call leaves it zero (node box mode).
             pool["node_v_adj"] = torch.zeros(R ** 3, 4, dtype=torch.float32, device=dev)
             pool["node_pm_adj"] = torch.empty(R ** 3, 4, dtype=torch.float32, device=dev)
@@ -281,6 +296,9 @@ class _Runner:
             adj.T += adj.temperature.double()
             adj.temperature.zero_()
         params_adj = torch.zeros(4, dtype=torch.float64, device=dev)  # mu, lambda, eta, heat parameter
+        rate_adj = None
+        if self.gas:
+            rate_adj = torch.zeros(sim.material.production_parameter.shape[0], dtype=torch.float64, device=dev)
         p = eng.params(False)
         cst = eng.constants(False)
         stream = _lib.stream_handle()
@@ -306,23 +324,26 @@ class _Runner:
                 tadj.node_fields[k] = _p(tb["node_fields"][k])
             tadj.vertices = _p(tb["vertices"])
             tadj.heat_parameter = params_adj.data_ptr() + 3 * 8
+            if self.gas:
+                tadj.gas_moles_out = tadj.gas_moles_in = _p(adj.N)
+                tadj.gas_rate = _p(rate_adj)
             # P2G of a transport substep uses T', dry + W' and the water-stressed stress.
             cst_mech = BkConstants.from_buffer_copy(cst)
             cst_mech.mass = _p(tb["mass"])
         for seg in range(len(self.checkpoints) - 1, -1, -1):
             first = seg * self.every
             length = min(self.every, self.steps - first)
-            _copy_state(work[0], self.checkpoints[seg], self.is_ding, self.transport)
+            _copy_state(work[0], self.checkpoints[seg], self.is_ding, self.transport, self.gas)
             for t in range(length):
                 self._run(work[t], work[t + 1], phases, grids[t][0], surface)
             for t in range(length - 1, -1, -1):
                 grid, g = grids[t]
-                sin = state_struct(work[t], self.is_ding, self.transport, False)
+                sin = state_struct(work[t], self.is_ding, self.transport, self.gas)
                 if self.transport:
                     self._check(self.lib.bk_transport_adjoint_prepare(
                         C.byref(p), C.byref(sin), C.byref(cst), _p(g["node_dT_ratio"]), _p(tb["T_mat"]),
                         _p(tb["mass"]), _p(tb["tau"]), stream), "bk_transport_adjoint_prepare")
-                    smech = state_struct(work[t], self.is_ding, self.transport, False)
+                    smech = state_struct(work[t], self.is_ding, self.transport, self.gas)
                     smech.tau, smech.material_temperature = _p(tb["tau"]), _p(tb["T_mat"])
                     self._check(self.fn(C.byref(p), C.byref(smech), C.byref(cst_mech), _p(g["node_pm"]),
                                         _p(g["node_v"]), g["bounds"].data_ptr() + 6 * 4, C.byref(adj_struct),
@@ -337,7 +358,7 @@ class _Runner:
                                         _p(node_v_adj), _p(node_pm_adj), _p(params_adj), stream),
                                 "bk_substep_adjoint")
         self.checkpoints = []
-        return adj, params_adj
+        return adj, params_adj, rate_adj
 
     def _run(self, state_in, state_out, phases, grid, surface):
         eng = self.engine
@@ -363,8 +384,8 @@ class _RolloutFunction(torch.autograd.Function):
     @staticmethod
     def backward(ctx, *grads):
         runner = ctx.runner
-        adj, params_adj = runner.backward(grads)
-        state_grads = dict(zip(_keys(runner.is_ding, runner.transport), adj.tensors()))
+        adj, params_adj, rate_adj = runner.backward(grads)
+        state_grads = dict(zip(_keys(runner.is_ding, runner.transport, runner.gas), adj.tensors()))
         nu = runner.sim.material.material_config.poisson_ratio
         mu_bar, lam_bar, eta_bar, h_bar = params_adj.tolist()
         dev = runner.sim.device
@@ -376,6 +397,8 @@ class _RolloutFunction(torch.autograd.Function):
                 out.append(state_grads[name].clone().reshape(shape))
             elif name == "viscosity_parameter":
                 out.append(torch.full(shape, eta_bar, dtype=torch.float32, device=dev))
+            elif name == "gas_source_rates":
+                out.append(rate_adj.float().reshape(shape).clone())
             elif name == "heat_transfer_parameter":
                 out.append(torch.full(shape, h_bar, dtype=torch.float32, device=dev))
             elif name == "young_modulus":
@@ -386,8 +409,9 @@ class _RolloutFunction(torch.autograd.Function):
         return (None, None, *out)
 
 
-_INPUTS = tuple(k for k, _ in _KINEMATIC) + tuple(k for k, _ in _DING) + tuple(k for k, _ in _TRANSPORT) + \
-    ("viscosity_parameter", "young_modulus", "heat_transfer_parameter")
+_INPUTS = tuple(k for k, _ in _KINEMATIC) + tuple(k for k, _ in _DING) + tuple(k for k, _ in _GAS) + \
+    tuple(k for k, _ in _TRANSPORT) + ("viscosity_parameter", "young_modulus", "heat_transfer_parameter",
+                                      "gas_source_rates")
 
 
 def Rollout(sim, steps, checkpoint_every=16, **inputs):
@@ -399,10 +423,11 @@ def Rollout(sim, steps, checkpoint_every=16, **inputs):
     ``kirchhoff_stresses`` (n, 3, 3), ``porosities`` (n,), ``temperatures`` (n,; the material
     temperature, without transport only) and ``viscosity_parameter`` (1,); with transport
     ``transport_temperatures``, ``water_masses`` (n,, float64) and ``heat_transfer_parameter`` (1,);
-    ``young_modulus`` (scalar or (1,)). Returns a dict of the final state's arrays (detached copies
-    joined to the autograd graph): the four kinematic arrays; for Ding ``elastic_gradients``,
-    ``kirchhoff_stresses``, ``porosities``, ``temperatures``; with transport
-    ``transport_temperatures`` and ``water_masses``. The simulator advances by ``steps`` substeps
+    in gas mode ``gas_moles`` (n,, float64) and ``gas_source_rates`` ((1,) or (n,), as
+    ``SetGasSourceRates``); ``young_modulus`` (scalar or (1,)). Returns a dict of the final state's
+    arrays (detached copies joined to the autograd graph): the four kinematic arrays; for Ding
+    ``elastic_gradients``, ``kirchhoff_stresses``, ``porosities``, ``temperatures``; in gas mode
+    ``gas_moles``; with transport ``transport_temperatures`` and ``water_masses``. The simulator advances by ``steps`` substeps
     as ``AdvanceUnchecked`` would, and its parameters keep the values given. Device flags raised
     during the run raise ``RuntimeError``.
     """
@@ -413,4 +438,4 @@ def Rollout(sim, steps, checkpoint_every=16, **inputs):
     names = tuple(k for k in _INPUTS if k in inputs)
     values = tuple(inputs[k] for k in names)
     outputs = _RolloutFunction.apply(runner, names, *values)
-    return dict(zip(_keys(runner.is_ding, runner.transport), outputs))
+    return dict(zip(_keys(runner.is_ding, runner.transport, runner.gas), outputs))

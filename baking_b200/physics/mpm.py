@@ -232,8 +232,13 @@ class MpmSimulator:
         self.settling_quiet_steps = 0
         self.settling_reference_step = 0
         self.settling_plastic_rate = 0.0
-        self.settling_reference_plastic = (self.current_state.material_state.plastic_gradients.clone()
-                                           if isinstance(self.material, DingMaterial) else None)
+        self.settling_reference_plastic = None
+        if isinstance(self.material, DingMaterial):
+            # A plane-layout copy: bk_settling_metrics reads it with the state's pitch (a clone of
+            # the strided view would be row-major unless n fills the pitch).
+            plastic = self.current_state.material_state.plastic_gradients
+            self.settling_reference_plastic = arrays.mat33s(n, device=self.device, pitch=arrays.layout_pitch(plastic))
+            self.settling_reference_plastic.copy_(plastic)
         self.settling_reason = "pending" if self._baking_start_step is None else "disabled"
         self.settling_diagnostics = dict(max_speed_m_s=0.0, max_strain_rate_per_s=0.0, max_plastic_rate_per_s=0.0)
         self.settling_metrics = torch.zeros(3, dtype=torch.float32, device=self.device)

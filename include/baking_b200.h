@@ -348,8 +348,8 @@ typedef struct BkAdjointState {
 } BkAdjointState;
 
 /* Reverse sweep of one mechanics substep (P2G, grid update, G2P, neo-Hookean stress or the
-   uncoupled Ding return map; physics/mpm.py:163-205 with transfer.py:37-105, grid.py:20-38,
-   elastic.py:4-26, ding.py:103-221). The reference gets these derivatives from Warp's tape replaying
+   Ding return map with its uncoupled or coupled (gas mode) porosity; physics/mpm.py:163-205 with
+   transfer.py:37-105, grid.py:20-38, elastic.py:4-26, ding.py:103-221, porous_return.py:43-100). The reference gets these derivatives from Warp's tape replaying
    its kernels' generated adjoints; this entry point replaces that replay for one substep.
    Inputs: the substep's input state `in`, the grid that bk_substep left after running from `in`
    (node_pm, node_v: R^3 float4), and `out_adjoint` = dL/d(output state). Writes
@@ -359,8 +359,12 @@ typedef struct BkAdjointState {
    lo[3], hi[3]); with it only the box is visited and node_v_adjoint is left zero, so it must be
    zero before the first call; without it node_v_adjoint is cleared and the whole grid visited. `parameter_adjoint`
    (device, float64, may be NULL) accumulates dL/d(shear modulus), dL/d(Lame lambda) and
-   dL/d(viscosity parameter). Transport, gas and the coupled porosity solve are not covered
-   (BK_ERR_UNSUPPORTED). */
+   dL/d(viscosity parameter). The coupled porosity solve is reversed through its converged
+   consistency equation (the derivative of the reference's SolvePorosityGradient). On a transport
+   substep `in` carries the stress and material temperature, and `constants` the particle mass,
+   that bk_transport_adjoint_prepare produced; `in_adjoint->mass` receives dL/d(particle mass) and
+   `in_adjoint->temperature` dL/d(material temperature); bk_transport_adjoint then finishes the
+   substep. */
 BK_API int bk_substep_adjoint(const BkSubstepParams *params, const BkState *in, const BkConstants *constants,
                               const float *node_pm, const float *node_v, const int32_t *node_box,
                               const BkAdjointState *out_adjoint, BkAdjointState *in_adjoint, float *node_v_adjoint,
@@ -392,11 +396,13 @@ BK_API int bk_mlp_adam(const float *grads, float *params, float *first_moment, f
 /* FP32 parameters -> packed BF16 operands + FP32 biases for bk_mlp_infer and the fused substep. */
 BK_API int bk_mlp_pack(const float *params, void *packed, void *stream);
 
-/* Transport half of the reverse sweep of one substep (Ding with thermal-water transport, gas off):
-   the surface heat/loss terms with their face areas, the scalar P2G, the diffusion stencil, the
-   scalar G2P, the water stress and the water-dependent mass (physics/thermal_water.py:77-253),
-   reversed. Node arrays are R^3 (node_dT_ratio: double2); all start at zero and are left at zero;
-   vertices: 3 planes of the surface's vertex_pitch, zero on entry, left zero. */
+/* Transport half of the reverse sweep of one substep (Ding with thermal-water transport, with or
+   without gas): the surface heat/loss terms with their face areas, the scalar P2G, the diffusion
+   stencil, the scalar G2P, the water stress and the water-dependent mass
+   (physics/thermal_water.py:77-253) and, with gas, the local gas source and the gas-pressure
+   stress (thermal_water.py:232-245, physics/materials/gas.py:16-35), reversed. Node arrays are R^3
+   (node_dT_ratio: double2); all start at zero and are left at zero; vertices: 3 planes of the
+   surface's vertex_pitch, zero on entry, left zero. */
 typedef struct BkAdjointTransport {
     const double *temperature_out, *water_out;  /* dL/d(T', W') of the substep's output */
     double *temperature_in, *water_in;          /* dL/d(T, W) of its input (may alias the above) */
@@ -405,11 +411,16 @@ typedef struct BkAdjointTransport {
                                                    heat, loss */
     double *vertices;                           /* surface-vertex adjoint scratch */
     double *heat_parameter;                     /* device [1], may be NULL: += dL/d(heat transfer) */
+    const double *gas_moles_out;                /* gas mode: dL/dN' of the substep's output */
+    double *gas_moles_in;                       /* gas mode: dL/dN of its input (may alias the above) */
+    double *gas_rate;                           /* gas mode, may be NULL: += dL/d(gas source rate), one
+                                                   entry per entry of BkConstants.gas_rate */
 } BkAdjointTransport;
 
 /* Before bk_substep_adjoint on a transport substep: the material temperature T + sum w dT, the
-   particle mass dry + W', and the stress tau - J c (s - s0) I that the forward P2G and return map
-   used, from the substep's input state and node (dT, dW/W) (n entries; stress: 9 planes). */
+   particle mass dry + W', and the stress tau + J (p_amb - p_gas) I - J c (s - s0) I (the gas term
+   in gas mode) that the forward P2G and return map used, from the substep's input state and node
+   (dT, dW/W) (n entries; stress: 9 planes). */
 BK_API int bk_transport_adjoint_prepare(const BkSubstepParams *params, const BkState *in,
                                         const BkConstants *constants, const double *node_dT_ratio,
                                         float *material_temperature, float *mass, float *stress, void *stream);

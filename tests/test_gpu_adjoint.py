@@ -126,6 +126,8 @@ def directional_check(make_sim, steps, name, delta, eps, checkpoint_every=2, rto
             return torch.tensor([sim.material.material_config.young_modulus], dtype=torch.float32, device="cuda")
         if name == "heat_transfer_parameter":
             return sim.transport.heat_transfer_parameter.clone()
+        if name == "gas_source_rates":
+            return sim.material.production_parameter.clone()
         attr = {"positions": "particle_positions", "velocities": "particle_velocities",
                 "affine_velocities": "affine_velocities", "deformation_gradients": "deformation_gradients"}
         if name in attr:
@@ -250,13 +252,12 @@ def test_temperature_directional():
     directional_check(make, 5, "temperatures", _delta((n,), 19, 2.0), 0.5)
 
 
-def test_rollout_rejects_gas_and_unknown_inputs():
+def test_rollout_rejects_unknown_inputs():
     from baking_b200.physics.adjoint import Rollout
-    from tests.scenes import build_gas
-    with pytest.raises(NotImplementedError):
-        Rollout(build_gas("cuda"), 1)
     with pytest.raises(TypeError):
         Rollout(velocity_sim(), 1, gravity=1.0)
+    with pytest.raises(ValueError):
+        Rollout(velocity_sim(), 1, gas_source_rates=_torch().ones(1, device="cuda"))
 
 
 def test_checkpoint_interval_does_not_change_gradients():

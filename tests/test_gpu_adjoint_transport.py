@@ -169,3 +169,78 @@ def test_backward_leaves_the_simulator_state():
                        st.transport_state.water_masses.clone(), st.transport_state.heat_exchanges.clone()])
     for a, b in zip(*finals):  # float atomics may sum in another order between the two runs
         torch.testing.assert_close(a, b, rtol=1e-5, atol=1e-6 * float(a.abs().max()))
+
+
+# ------------------------------------------------------------------- gas mode
+def gassy_sim(per_particle=True):
+    """The heated cube in gas mode: coupled end-state porosity, gas source around its reaction
+    temperature (per-particle rates), gas-pressure stress, water transport."""
+    from baking_b200.physics.mpm import MpmSimulator
+    from tests.scenes import assign, to_np
+    mesh = CreateDemoMesh(2)
+    transport = TransportConfig(enabled=True, initial_temperature_k=325.0, oven_temperature_k=480.0,
+                                heat_transfer=2000.0, conductivity=20.0, specific_heat=100.0,
+                                water_diffusivity=1e-8, surface_water_loss=1e-5)
+    ding = DingConfig(yield_stress=50.0, viscosity=1000.0, porosity=0.3, temperature_enabled=True, gas_enabled=True,
+                      gas_initial_pressure_pa=1000.0, gas_ambient_pressure_pa=1000.0, gas_production_rate=0.005)
+    sim = MpmSimulator(mesh, SampleParticles(mesh, 1000.0, 4),
+                       replace(SimulationConfig(), device_name="cuda:0", time_step=0.001, gravity=(0.0, 0.0, 0.0)),
+                       MaterialConfig(model="ding2019"), ding_config=ding, transport_config=transport)
+    rng = np.random.default_rng(7)
+    n = sim.particle_data.particle_count
+    st = sim.current_state
+    x = to_np(st.particle_positions)
+    assign(st.particle_velocities, ((x - np.array([0.5, 0.6, 0.5], np.float32)) @ STRAIN_RATES.T).astype(np.float32))
+    assign(st.affine_velocities, np.tile(STRAIN_RATES, (n, 1, 1)))
+    Q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+    Q *= np.sign(np.linalg.det(Q))
+    Fe = (Q @ np.diag([1.01, 0.995, 1.003]) @ Q.T)[None] + 0.003 * rng.standard_normal((n, 3, 3))
+    assign(st.material_state.elastic_gradients, Fe.astype(np.float32))
+    assign(st.deformation_gradients, Fe.astype(np.float32))
+    tau = 20.0 * rng.standard_normal((n, 3, 3))
+    assign(st.material_state.kirchhoff_stresses, (tau + tau.transpose(0, 2, 1)).astype(np.float32))
+    assign(st.transport_state.temperatures, 320.0 + 10.0 * rng.random(n))
+    if per_particle:
+        sim.SetGasSourceRates((0.003 + 0.004 * rng.random(n)).astype(np.float32))
+    return sim
+
+
+def _gas_shape(sim, name):
+    n = sim.particle_data.particle_count
+    return {"velocities": (n, 3), "deformation_gradients": (n, 3, 3), "elastic_gradients": (n, 3, 3),
+            "porosities": (n,), "transport_temperatures": (n,), "viscosity_parameter": (1,),
+            "young_modulus": (1,), "gas_source_rates": (n,)}[name]
+
+
+@pytest.mark.parametrize("name,scale,eps", [
+    ("gas_source_rates", 0.002, 0.5), ("transport_temperatures", 2.0, 0.5), ("porosities", 0.01, 0.5),
+    ("elastic_gradients", 0.002, 0.5), ("deformation_gradients", 0.002, 0.5), ("velocities", 0.02, 0.5),
+    ("viscosity_parameter", 100.0, 0.5), ("young_modulus", 1000.0, 1.0)])
+def test_gas_directional(name, scale, eps):
+    sim = gassy_sim()
+    directional_check(gassy_sim, 5, name, _delta(_gas_shape(sim, name), 37, scale), eps)
+
+
+def test_gas_moles_directional():
+    sim = gassy_sim()
+    N0 = sim.current_state.material_state.gas_moles.clone()
+    directional_check(gassy_sim, 5, "gas_moles", 0.2 * N0 * _coherent(tuple(N0.shape), 41), 0.5)
+
+
+def test_shared_gas_rate_directional():
+    """One production parameter for every particle (the reference's scalar)."""
+    make = lambda: gassy_sim(per_particle=False)  # noqa: E731
+    directional_check(make, 5, "gas_source_rates", _delta((1,), 43, 0.002), 0.5)
+
+
+def test_private_surface_buffers_use_the_vertex_pitch():
+    """The reverse sweep's own vertex buffer is written by the vertex kernel in plane layout with
+    the surface's vertex pitch; a row-major buffer would be written past its end."""
+    from baking_b200 import arrays
+    from baking_b200.physics.adjoint import Rollout
+    sim = heated_sim()
+    T = sim.current_state.transport_state.temperatures.clone().requires_grad_(True)
+    Rollout(sim, 2, transport_temperatures=T)["transport_temperatures"].sum().backward()
+    verts = sim._buffers["rollout"]["transport"]["surface_vertices"]
+    assert arrays.layout_pitch(verts) == sim._engine.surface.vertex_pitch
+    assert verts.shape == sim.surface_vertices_buffer().shape
