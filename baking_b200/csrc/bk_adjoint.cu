@@ -195,12 +195,6 @@ __device__ void principal_vjp(const PrincipalFwd& f, const float* gb, const floa
     out[kMu] = mub; out[kLam] = lamb; out[kTy] = tyb; out[kEta] = etab; out[kA] = ab;
 }
 
-// End-state porosity of gas mode for the trial singular values s (ding.py:183-197); `r_warm`
-// returns the last overstress root. Out of line: the adjoint kernel's other paths keep their registers.
-struct CoupledFwd;
-__device__ __noinline__ float coupled_solve(const float* s, float mu, float lam, float ty, float eta, float dt,
-                                            float n0, float por, double* r_warm);
-
 // Inputs of the end-state porosity solve of gas mode (ding.py:183-196), computed from the trial
 // singular values in the forward's order of operations.
 struct CoupledFwd {
@@ -232,25 +226,22 @@ __device__ CoupledFwd coupled_forward(const float* s, float mu, float lam, float
     return c;
 }
 
-__device__ __noinline__ float coupled_solve(const float* s, float mu, float lam, float ty, float eta, float dt,
-                                            float n0, float por, double* r_warm) {
-    const CoupledFwd c = coupled_forward(s, mu, lam, ty, eta, dt, n0, por);
-    return solve_porosity(c.q, c.p, c.df, c.ms, c.ex, c.Vp, n0, r_warm);
-}
-
-// Reverse of n = solve_porosity(q, p, d, h, e, Vp): n is the root of n = pred(n; q, p, d, h, e, Vp)
-// with pred = Vp exp(e (1 - 1/v)) - 1 + n0, v = 1 + h a(n) r and r the overstress root of
-// r + 1 - q/(1+dr)^2 - a p/(1+h a r)^2 = 0. The implicit function theorem on the converged
+// End-state porosity of gas mode, n = solve_porosity(q, p, d, h, e, Vp) for the trial singular
+// values s (ding.py:183-197), and its gradient G = dn/d(s0, s1, s2, mu, lambda, yield stress,
+// viscosity, old porosity). n is the root of n = pred(n; q, p, d, h, e, Vp) with
+// pred = Vp exp(e (1 - 1/v)) - 1 + n0, v = 1 + h a(n) r and r the overstress root of
+// r + 1 - q/(1+dr)^2 - a p/(1+h a r)^2 = 0; the implicit function theorem on the converged
 // equation (the derivatives of the reference's SolvePorosityGradient, porous_return.py:64-100)
-// gives theta_bar = nb dpred/dtheta / (1 - dpred/dn); the elastic early exit is the case r = 0.
-// Adds the result to the principal slots (singular values, mu, lambda, yield stress, viscosity)
-// and returns dL/d(old porosity) through Vp = 1 - n0 + n_old.
-__device__ __noinline__ float coupled_vjp(const float* s, float mu, float lam, float ty, float eta, float dt, float n0,
-                                          float por, double n, double nb, double r_warm, float* dpar) {
+// gives dn/dtheta = dpred/dtheta / (1 - dpred/dn); the elastic early exit is the case r = 0.
+// Out of line, called before the rest of the reverse sweep needs its registers.
+__device__ __noinline__ float coupled_solve_grad(const float* s, float mu, float lam, float ty, float eta, float dt,
+                                                 float n0, float por, float* G) {
     const CoupledFwd c = coupled_forward(s, mu, lam, ty, eta, dt, n0, por);
+    double r = 0.0;
+    const float nf = solve_porosity(c.q, c.p, c.df, c.ms, c.ex, c.Vp, n0, &r);
+    const double n = (double)nf;
     const double q = c.q, p = c.p, d = c.df, h = c.ms, e = c.ex, Vp = c.Vp;
     const double a = pressure_coefficient64(n);
-    double r = r_warm;
     r = overstress64(q, a * p, d, h * a, &r);
     const double v = 1.0 + h * a * r;
     const double E = exp(e * (1.0 - 1.0 / v));
@@ -270,7 +261,7 @@ __device__ __noinline__ float coupled_vjp(const float* s, float mu, float lam, f
         rh = -2.0 * a * p * r / (v * v * v * Fr);
     }
     const double slope = K * h * da * (r + a * (rp * p + rh * h));
-    const double lm = nb / (1.0 - slope);
+    const double lm = 1.0 / (1.0 - slope);
     const float qb = (float)(lm * K * h * a * rq);
     const float pb = (float)(lm * K * h * a * a * rp);
     const float db = (float)(lm * K * h * a * rd);
@@ -304,13 +295,14 @@ __device__ __noinline__ float coupled_vjp(const float* s, float mu, float lam, f
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         mub += 2.f * c.eps[k] * tsb[k];
-        dpar[kS0 + k] += (2.f * c.mu * tsb[k] + c.lam * tsum) * expf(-c.eps[k]);
+        G[k] = (2.f * c.mu * tsb[k] + c.lam * tsum) / s[k];
     }
-    dpar[kMu] += mub;
-    dpar[kLam] += lamb;
-    dpar[kTy] += 2.f * c.ty * ty2b;
-    dpar[kEta] += etab;
-    return (float)(lm * E);
+    G[3] = mub;
+    G[4] = lamb;
+    G[5] = 2.f * c.ty * ty2b;
+    G[6] = etab;
+    G[7] = (float)(lm * E);  // through Vp = 1 - n0 + n_old
+    return nf;
 }
 
 __device__ __forceinline__ void add_m3(float* __restrict__ p, int64_t i, int64_t pitch, const float* a) {
@@ -453,8 +445,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                 // return, and the returned Fe is rescaled to det F' / (1 - n0 + n_ret) (ding.py:183-205).
                 constexpr bool coupled = kCoupled;
                 float n_ret = por;
-                double r_warm = 0.0;
-                if (coupled) n_ret = coupled_solve(s, D.mu, D.lam, ty, eta, D.dt, D.initial_porosity, por, &r_warm);
+                float nG[8];  // dn_ret/d(s0, s1, s2, mu, lambda, yield, viscosity, old porosity)
+                if (coupled) n_ret = coupled_solve_grad(s, D.mu, D.lam, ty, eta, D.dt, D.initial_porosity, por, nG);
                 float a = porosity_coefficient(n_ret);
                 PrincipalFwd pr = principal_forward(s, D.mu, D.lam, ty, eta, a, D.dt);
                 bool porosity_free = !(D.initial_porosity == 0.0f && por == 0.0f);
@@ -518,9 +510,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                         const float lg = logf(1.0f / n_ret);
                         nret_b += (double)(dpar[kA] * a * (2.0f / (n_ret * lg) - 3.5f / (3.5f * n_ret + 1.0f)));
                     }
-                    if (nret_b != 0.0)
-                        porb_coupled = coupled_vjp(s, D.mu, D.lam, ty, eta, D.dt, D.initial_porosity, por,
-                                                   (double)n_ret, nret_b, r_warm, dpar);
+                    const float nb = (float)nret_b;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) dpar[kS0 + k] += nb * nG[k];
+                    dpar[kMu] += nb * nG[3];
+                    dpar[kLam] += nb * nG[4];
+                    dpar[kTy] += nb * nG[5];
+                    dpar[kEta] += nb * nG[6];
+                    porb_coupled = nb * nG[7];
                 }
                 Ab[0] = dpar[kS0];
                 Ab[4] = dpar[kS1];

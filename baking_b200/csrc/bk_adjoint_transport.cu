@@ -142,20 +142,42 @@ __global__ void k_tadj_prepare(TParams P, BkState in, BkConstants cst, const dou
 }
 
 // ------------------------------------------------------------- scalar chain
+// Node adjoints of (dT, dW/W) are scattered like the forward's scalar P2G: a block stages the node
+// box its particles touch in shared memory (when it fits kTileNodes), and within a warp each run
+// of particles with the same stencil base is summed by 27 lanes, one node each, before one atomic
+// per node.
+constexpr int kTileNodes = 512;
+
+struct ScalarSmem {
+    float w[kThreads][9];
+    double val[kThreads][2];
+    double tile[2][kTileNodes];
+    int box[6];
+};
+
+__device__ __forceinline__ long long pack_base(const int* b) {
+    return ((long long)b[0] << 42) | ((long long)b[1] << 21) | (long long)b[2];
+}
+
 __global__ void __launch_bounds__(kThreads) k_tadj_scalar(TParams P, BkState in, BkConstants cst,
                                                         const double2* __restrict__ dTr, BkAdjointTransport a,
                                                         const BkAdjointState adj, double2* __restrict__ dTr_bar) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    __shared__ ScalarSmem sm;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + tid;
     const int64_t pitch = P.pitch;
     double rate_b = 0.0;  // dL/d(gas source rate) through this particle
+    double Tnb = 0.0, ratiob = 0.0;
     Stencil st;
     st.valid = false;
+    st.b[0] = st.b[1] = st.b[2] = 0;
     if (i < P.n) st = make_stencil(load_v3(in.x, i, pitch), P.origin, P.dx, P.R);
+    const bool valid = i < P.n && st.valid;
     if (i < P.n && !st.valid) {
         a.temperature_in[i] = 0.0;
         a.water_in[i] = 0.0;
         if (P.gas) a.gas_moles_in[i] = 0.0;
-    } else if (i < P.n) {
+    } else if (valid) {
         double dTp = 0.0, ratio = 0.0;
 #pragma unroll
         for (int j = 0; j < 27; ++j) {
@@ -167,14 +189,15 @@ __global__ void __launch_bounds__(kThreads) k_tadj_scalar(TParams P, BkState in,
             ratio += w * d.y;
         }
         const double T = in.temperature[i], Tn = T + dTp;
-        const double W = in.water[i], Wn = W * (1.0 + ratio);
+        const double W = in.water[i];
+        const double Wn = W * (1.0 + ratio);
         const M3 F = load_m3(in.F, i, pitch);
         const float Jf = det3(F);
         const double J = (double)Jf;
         const double V0 = (double)cst.volume[i];
         const double sat = Wn / (P.rho_w * V0 * J);
         // adjoints arriving at T', W', T_mat, mass and the P2G stress
-        double Tnb = a.temperature_out[i] + (double)adj.temperature[i];
+        Tnb = a.temperature_out[i] + (double)adj.temperature[i];
         double Wnb = a.water_out[i] + (double)adj.mass[i];
         const double trace = (double)adj.tau[i] + (double)adj.tau[4 * pitch + i] + (double)adj.tau[8 * pitch + i];
         // stress -= iso I, iso = J c (s - s0)
@@ -210,9 +233,10 @@ __global__ void __launch_bounds__(kThreads) k_tadj_scalar(TParams P, BkState in,
             }
         }
         // W' = W (1 + sum w r), T' = T + sum w dT
-        const double ratiob = Wnb * W;
+        ratiob = Wnb * W;
         a.water_in[i] = Wnb * (1.0 + ratio);
         a.temperature_in[i] = Tnb + Tb_direct;
+        // weight gradients: x_bar += sum_j grad w_j (dT_j T'_bar + r_j ratio_bar)
         const float inv_dx = 1.f / P.dx;
         float xg[3] = {0.f, 0.f, 0.f};
 #pragma unroll 1
@@ -220,11 +244,8 @@ __global__ void __launch_bounds__(kThreads) k_tadj_scalar(TParams P, BkState in,
             int ox, oy, oz;
             node_offset(j, ox, oy, oz);
             float dw[3];
-            const double w = (double)weight_and_grad(st, ox, oy, oz, inv_dx, dw);
-            const int64_t node = node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R);
-            const double2 d = dTr[node];
-            atomicAdd(&dTr_bar[node].x, w * Tnb);
-            atomicAdd(&dTr_bar[node].y, w * ratiob);
+            weight_and_grad(st, ox, oy, oz, inv_dx, dw);
+            const double2 d = dTr[node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R)];
             const float s = (float)(d.x * Tnb + d.y * ratiob);
 #pragma unroll
             for (int c = 0; c < 3; ++c) xg[c] += dw[c] * s;
@@ -233,6 +254,80 @@ __global__ void __launch_bounds__(kThreads) k_tadj_scalar(TParams P, BkState in,
         for (int c = 0; c < 3; ++c) adj.x[c * pitch + i] += xg[c];
         add_det_grad(adj.F, i, pitch, F, (float)Jb);
     }
+    // ---- scatter w (T'_bar, ratio_bar) into the node adjoints
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax)
+#pragma unroll
+        for (int o = 0; o < 3; ++o) sm.w[tid][3 * ax + o] = valid ? st.w[ax][o] : 0.f;
+    sm.val[tid][0] = Tnb;
+    sm.val[tid][1] = ratiob;
+    if (tid < 6) sm.box[tid] = tid < 3 ? INT_MAX : INT_MIN;
+    __syncthreads();
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const int lo = __reduce_min_sync(0xffffffffu, valid ? st.b[ax] : INT_MAX);
+        const int hi = __reduce_max_sync(0xffffffffu, valid ? st.b[ax] + 2 : INT_MIN);
+        if (lane == 0 && lo != INT_MAX) {
+            atomicMin(&sm.box[ax], lo);
+            atomicMax(&sm.box[3 + ax], hi);
+        }
+    }
+    __syncthreads();
+    int lo[3] = {0, 0, 0}, ext[3] = {1, 1, 1};
+    int count = 0;
+    bool tiled = false;
+    if (sm.box[0] != INT_MAX) {
+        long long c = 1;
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            lo[ax] = sm.box[ax];
+            ext[ax] = sm.box[3 + ax] - sm.box[ax] + 1;
+            c *= ext[ax];
+        }
+        tiled = c <= kTileNodes;
+        count = tiled ? (int)c : 0;
+    }
+    for (int t = tid; t < count; t += kThreads) sm.tile[0][t] = sm.tile[1][t] = 0.0;
+    __syncthreads();
+    const long long key = valid ? pack_base(st.b) : -1;
+    const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
+    unsigned starts = __ballot_sync(0xffffffffu, valid && (lane == 0 || prev != key));
+    const int warp_base = tid & ~31;
+    int ox, oy, oz;
+    node_offset(lane < 27 ? lane : 0, ox, oy, oz);
+    while (starts) {
+        const int s0 = __ffs(starts) - 1;
+        starts &= starts - 1;
+        const int e = starts ? __ffs(starts) - 1 : 32;
+        const int b0 = __shfl_sync(0xffffffffu, st.b[0], s0), b1 = __shfl_sync(0xffffffffu, st.b[1], s0),
+                  b2 = __shfl_sync(0xffffffffu, st.b[2], s0);
+        if (lane < 27) {
+            double acc0 = 0.0, acc1 = 0.0;
+            for (int k = warp_base + s0; k < warp_base + e; ++k) {
+                const double w = (double)(sm.w[k][ox] * sm.w[k][3 + oy] * sm.w[k][6 + oz]);
+                acc0 += w * sm.val[k][0];
+                acc1 += w * sm.val[k][1];
+            }
+            if (tiled) {
+                const int t = ((b0 + ox - lo[0]) * ext[1] + (b1 + oy - lo[1])) * ext[2] + (b2 + oz - lo[2]);
+                atomicAdd(&sm.tile[0][t], acc0);
+                atomicAdd(&sm.tile[1][t], acc1);
+            } else {
+                double2* d = dTr_bar + node_index(b0 + ox, b1 + oy, b2 + oz, P.R);
+                atomicAdd(&d->x, acc0);
+                atomicAdd(&d->y, acc1);
+            }
+        }
+    }
+    __syncthreads();
+    for (int t = tid; t < count; t += kThreads) {
+        const double v0 = sm.tile[0][t], v1 = sm.tile[1][t];
+        if (v0 == 0.0 && v1 == 0.0) continue;
+        const int z = t % ext[2], y = (t / ext[2]) % ext[1], x = t / (ext[2] * ext[1]);
+        double2* d = dTr_bar + node_index(lo[0] + x, lo[1] + y, lo[2] + z, P.R);
+        atomicAdd(&d->x, v0);
+        atomicAdd(&d->y, v1);
+    }
     if (P.gas && a.gas_rate) {
         if (cst.gas_rate_per_particle) {
             if (i < P.n) a.gas_rate[i] += rate_b;
@@ -240,7 +335,7 @@ __global__ void __launch_bounds__(kThreads) k_tadj_scalar(TParams P, BkState in,
             // one shared rate: a warp sum, then one atomic per warp
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) rate_b += __shfl_xor_sync(0xffffffffu, rate_b, o);
-            if ((threadIdx.x & 31) == 0 && rate_b != 0.0) atomicAdd(a.gas_rate, rate_b);
+            if (lane == 0 && rate_b != 0.0) atomicAdd(a.gas_rate, rate_b);
         }
     }
 }
@@ -387,36 +482,55 @@ __global__ void __launch_bounds__(kThreads) k_tadj_scatter(TParams P, BkState in
 }
 
 // ---------------------------------------------------------------- surface
-// Vertex position of the mesh (geometry/mesh_tracking.py:13-38): anchor + sum_b w_b (pred_b - anchor),
-// pred_b = x_p + F_p o_b, anchor = pred of the first binding.
-__device__ void vertex_position(const BkSurface& sf, const float* __restrict__ x, const float* __restrict__ F,
-                                int64_t pitch, int vid, double* out) {
+// Mesh vertex positions of this substep (geometry/mesh_tracking.py:13-38) into surface.vertices,
+// as the forward's transport phase computed them: one warp per boundary vertex,
+// anchor + sum_b w_b (pred_b - anchor) with pred_b = x_p + F_p o_b and the first binding's
+// prediction as the anchor, summed lane-strided and reduced in the same order.
+__global__ void k_tadj_vertex_positions(TParams P, const float* __restrict__ x, const float* __restrict__ F,
+                                        BkSurface sf) {
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= sf.vertex_count) return;
+    const int vid = sf.vertex_ids[w];
     const int b0 = sf.binding_offsets[vid], b1 = sf.binding_offsets[vid + 1];
-    const int64_t vp = sf.vertex_pitch, bp = sf.binding_pitch;
+    const int64_t vp = sf.vertex_pitch, bp = sf.binding_pitch, pitch = P.pitch;
     if (b0 == b1) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) out[k] = (double)sf.reference_vertices[k * vp + vid];
+        if (lane < 3) sf.vertices[lane * vp + vid] = sf.reference_vertices[lane * vp + vid];
         return;
     }
-    float anchor[3], disp[3] = {0.f, 0.f, 0.f};
-    for (int b = b0; b < b1; ++b) {
+    auto predict = [&](int b, float* r) {
         const int p = sf.binding_particles[b];
         const M3 f = load_m3(F, p, pitch);
         const V3 xp = load_v3(x, p, pitch);
         const float o[3] = {sf.reference_offsets[b], sf.reference_offsets[bp + b], sf.reference_offsets[2 * bp + b]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) r[a] = xp.v[a] + (f.m[3 * a] * o[0] + f.m[3 * a + 1] * o[1] + f.m[3 * a + 2] * o[2]);
+    };
+    float anchor[3];
+    predict(b0, anchor);
+    float disp[3] = {0.f, 0.f, 0.f};
+    for (int b = b0 + lane; b < b1; b += 32) {
         float pr[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) pr[k] = xp.v[k] + (f.m[3 * k] * o[0] + f.m[3 * k + 1] * o[1] + f.m[3 * k + 2] * o[2]);
-        if (b == b0) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) anchor[k] = pr[k];
-        }
+        predict(b, pr);
         const float wgt = sf.binding_weights[b];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) disp[k] += wgt * (pr[k] - anchor[k]);
+        for (int a = 0; a < 3; ++a) disp[a] += wgt * (pr[a] - anchor[a]);
     }
 #pragma unroll
-    for (int k = 0; k < 3; ++k) out[k] = (double)(anchor[k] + disp[k]);
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) disp[a] += __shfl_xor_sync(0xffffffffu, disp[a], o);
+    if (lane < 3) sf.vertices[lane * vp + vid] = anchor[lane] + disp[lane];
+}
+
+__device__ __forceinline__ void face_vertices(const BkSurface& sf, int f, double q[3][3], int vid[3]) {
+    const int64_t vp = sf.vertex_pitch;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        vid[k] = sf.faces[3 * f + k];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) q[k][a] = (double)sf.vertices[a * vp + vid[k]];
+    }
 }
 
 __global__ void k_tadj_owners(TParams P, BkState in, BkConstants cst, BkSurface sf, BkGridFields g,
@@ -432,8 +546,8 @@ __global__ void k_tadj_owners(TParams P, BkState in, BkConstants cst, BkSurface 
     const int f0 = sf.owner_face_offsets[o], f1 = sf.owner_face_offsets[o + 1];
     for (int f = f0; f < f1; ++f) {
         double q[3][3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) vertex_position(sf, in.x, in.F, pitch, sf.faces[3 * f + k], q[k]);
+        int vid[3];
+        face_vertices(sf, f, q, vid);
         const double e1[3] = {q[1][0] - q[0][0], q[1][1] - q[0][1], q[1][2] - q[0][2]};
         const double e2[3] = {q[2][0] - q[0][0], q[2][1] - q[0][1], q[2][2] - q[0][2]};
         const double nr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
@@ -487,11 +601,7 @@ __global__ void k_tadj_owners(TParams P, BkState in, BkConstants cst, BkSurface 
     for (int f = f0; f < f1; ++f) {
         double q[3][3];
         int vid[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            vid[k] = sf.faces[3 * f + k];
-            vertex_position(sf, in.x, in.F, pitch, vid[k], q[k]);
-        }
+        face_vertices(sf, f, q, vid);
         const double e1[3] = {q[1][0] - q[0][0], q[1][1] - q[0][1], q[1][2] - q[0][2]};
         const double e2[3] = {q[2][0] - q[0][0], q[2][1] - q[0][1], q[2][2] - q[0][2]};
         const double nr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
@@ -657,6 +767,10 @@ int bk_transport_adjoint(const BkSubstepParams* params, const BkState* in, const
     if (int rc = check_launch("bk_transport_adjoint/diffuse")) return rc;
     k_tadj_scatter<<<blocks(p.n, kThreads), kThreads, 0, s>>>(P, *in, *constants, g, a, *mechanics);
     if (int rc = check_launch("bk_transport_adjoint/scatter")) return rc;
+    if (surface->vertex_count > 0) {
+        k_tadj_vertex_positions<<<blocks(surface->vertex_count * 32, 128), 128, 0, s>>>(P, in->x, in->F, *surface);
+        if (int rc = check_launch("bk_transport_adjoint/vertex_positions")) return rc;
+    }
     if (surface->owner_count > 0) {
         k_tadj_owners<<<blocks(surface->owner_count, 64), 64, 0, s>>>(P, *in, *constants, *surface, g, a, *mechanics);
         if (int rc = check_launch("bk_transport_adjoint/owners")) return rc;

@@ -362,6 +362,44 @@ def batched(args, rank, dist, net, count=64, steps=200):
             "scene": "dough balls (loaf dough: Ding + gas + thermal-water), dt 5e-5, one CUDA graph per 2 substeps"}
 
 
+def rollout_variant(sim, dist, stream, world, scene, fb_steps=64, every=8):
+    """Forward + hand-written adjoint of ``fb_steps`` substeps with a checkpoint every ``every``
+    (Rollout): loss = mean squared distance of the final positions to the initial cloud scaled by
+    1.2 about its centre; gradients with respect to the per-particle initial temperatures and gas
+    source rates and Young's modulus."""
+    import torch
+    from baking_b200.physics.adjoint import Rollout
+    n = sim.particle_data.particle_count
+    sim.AdvanceUnchecked(2)
+    st = sim.current_state
+    x0 = st.particle_positions.clone()
+    center = x0.mean(0)
+    target = 1.2 * (x0 - center) + center
+    T0 = st.transport_state.temperatures.clone().requires_grad_(True)
+    rates = sim.material.production_parameter.clone().requires_grad_(True)
+    E0 = torch.tensor([sim.material.material_config.young_modulus], device="cuda", requires_grad=True)
+
+    def fwd_bwd():
+        res = Rollout(sim, fb_steps, checkpoint_every=every, transport_temperatures=T0, gas_source_rates=rates,
+                      young_modulus=E0)
+        loss = ((res["positions"] - target) ** 2).sum(1).mean()
+        loss.backward()
+        return loss
+
+    fwd_bwd()  # warm-up: first-call set-up of the reverse-mode buffers and kernels
+    for t in (T0, rates, E0):
+        t.grad = None
+    t_fb, _ = _timed(fwd_bwd, dist, stream)
+    t_f, _ = _timed(lambda: sim.AdvanceUnchecked(fb_steps), dist, stream)
+    finite = all(bool(torch.isfinite(t.grad).all()) for t in (T0, rates, E0))
+    out = {"value": world * n * fb_steps / t_fb, "unit": UNIT, "forward_only": world * n * fb_steps / t_f,
+           "ms_per_substep": 1e3 * t_fb / fb_steps, "steps": fb_steps, "checkpoint_every": every,
+           "gradients": ["transport_temperatures", "gas_source_rates", "young_modulus"],
+           "finite_gradients": finite, "scene": scene}
+    del sim
+    return out
+
+
 def variants(args, rank, dist):
     """The metric's other two forms at the same particle count and grid.
 
@@ -370,14 +408,12 @@ def variants(args, rank, dist):
     the same substeps from the same state; the plain loaf of the headline never yields in the timed
     window, so the surrogate has nothing to replace there.
     fwd_bwd: forward + hand-written adjoint of 64 substeps with a checkpoint every 8 (Rollout) on the
-    loaf without transport or gas (the adjoint's scope), loss = mean squared distance of the final
-    positions to the initial cloud scaled by 1.2 about its centre, gradients with respect to the
-    per-particle velocities and temperatures and Young's modulus."""
+    headline loaf (Ding + gas + thermal-water), loss = mean squared distance of the final positions
+    to the initial cloud scaled by 1.2 about its centre, gradients with respect to the per-particle
+    initial temperatures and gas source rates and Young's modulus; also on a 100k-particle dough
+    sphere on a 64^3 grid."""
     import torch
-    from dataclasses import replace
-    from baking_b200.config import TransportConfig
-    from baking_b200.physics.adjoint import Rollout
-    from baking_b200.scenes import box_loaf, make_simulator
+    from baking_b200.scenes import box_loaf, dough_ball, make_simulator
     from baking_b200.surrogate import LoadReturnSurrogate, ReturnMapSurrogate
     world = int(os.environ.get("WORLD_SIZE", "1"))
     stream = torch.cuda.current_stream()
@@ -407,37 +443,13 @@ def variants(args, rank, dist):
                         "scene": f"box loaf {n} particles, {args.resolution}^3, 318 K, prestrain 0.08, gas + transport"}
     del results, xe, xs
     # forward + backward
-    fb_steps, every = 64, 8
-    mech = replace(loaf, transport=TransportConfig(enabled=False), gas_source_rates=None,
-                   ding=replace(loaf.ding, gas_enabled=False), initial_log_strain=(0.0, 0.0, 0.0))
-    sim = make_simulator(mech, diagnostics="lean")
-    sim.AdvanceUnchecked(2)
-    st = sim.current_state
-    x0 = st.particle_positions.clone()
-    center = x0.mean(0)
-    target = 1.2 * (x0 - center) + center
-    v0 = st.particle_velocities.clone().requires_grad_(True)
-    T0 = st.material_state.temperatures.clone().requires_grad_(True)
-    E0 = torch.tensor([sim.material.material_config.young_modulus], device="cuda", requires_grad=True)
-
-    def fwd_bwd():
-        res = Rollout(sim, fb_steps, checkpoint_every=every, velocities=v0, temperatures=T0, young_modulus=E0)
-        loss = ((res["positions"] - target) ** 2).sum(1).mean()
-        loss.backward()
-        return loss
-
-    fwd_bwd()  # warm-up: first-call set-up of the reverse-mode buffers and kernels
-    v0.grad = None
-    T0.grad = None
-    E0.grad = None
-    t_fb, _ = _timed(fwd_bwd, dist, stream)
-    t_f, _ = _timed(lambda: sim.AdvanceUnchecked(fb_steps), dist, stream)
-    out["fwd_bwd"] = {"value": world * n * fb_steps / t_fb, "unit": UNIT, "forward_only": world * n * fb_steps / t_f,
-                      "steps": fb_steps, "checkpoint_every": every,
-                      "finite_gradients": bool(torch.isfinite(v0.grad).all() and torch.isfinite(T0.grad).all()
-                                               and torch.isfinite(E0.grad).all()),
-                      "scene": f"box loaf {n} particles, {args.resolution}^3, Ding without transport/gas"}
-    del sim, v0, T0, E0
+    out["fwd_bwd"] = rollout_variant(make_simulator(box_loaf(args.resolution, args.particles, seed=rank),
+                                                    diagnostics="lean"), dist, stream, world,
+                                     f"box loaf {n} particles, {args.resolution}^3, Ding + gas + thermal-water")
+    sphere = dough_ball(64, 100_000, seed=rank, initial_temperature=298.15)
+    out["fwd_bwd"]["sphere_64"] = rollout_variant(
+        make_simulator(sphere, diagnostics="lean"), dist, stream, world,
+        f"dough sphere {sphere.particle_count} particles, 64^3, Ding + gas + thermal-water")
     out["batched"] = batched(args, rank, dist, net)
     return out
 

@@ -427,7 +427,8 @@ BK_API int bk_transport_adjoint_prepare(const BkSubstepParams *params, const BkS
 /* After bk_substep_adjoint (whose tau, mass and temperature outputs are `mechanics`' inputs here,
    and whose x and F outputs receive the transport terms): `grid` is the substep's forward grid run
    with keep_transport_fields = 1, whose transport fields this call clears over the box in
-   grid->bounds + 6; `surface` the BkSurface of that substep. */
+   grid->bounds + 6; `surface` the BkSurface of that substep, whose `vertices` this call rewrites
+   with the substep's mesh vertex positions (as the forward transport phase computed them). */
 BK_API int bk_transport_adjoint(const BkSubstepParams *params, const BkState *in, const BkConstants *constants,
                                 const BkGrid *grid, const BkSurface *surface, const BkAdjointState *mechanics,
                                 BkAdjointTransport *adjoint, void *stream);
