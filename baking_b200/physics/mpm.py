@@ -280,6 +280,9 @@ class MpmSimulator:
             self.UpdateSettling(original)
         if getattr(self, "result_recorder", None) is not None:
             self.result_recorder.Record()
+            if was_settling and not self.IsSettling:
+                self.result_recorder.settled_measurement = dict(self.result_recorder.last_measurement)
+                self.result_recorder.QueueSnapshot()
 
     def MaxReturnResiduals(self):
         """(max return residual, max porosity residual) of the last substep, on the host."""

@@ -50,6 +50,9 @@ def parse():
     p.add_argument("--resolution", type=int, default=128)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-variants", action="store_true", help="skip the surrogate and fwd+bwd forms")
+    p.add_argument("--rollout-only", type=int, nargs=2, metavar=("STEPS", "EVERY"), default=None,
+                   help="time only forward + adjoint of STEPS substeps, a checkpoint every EVERY, on the "
+                        "headline loaf (for profiling the reverse sweep)")
     return p.parse_args()
 
 
@@ -208,6 +211,16 @@ def main():
     scene = box_loaf(args.resolution, args.particles, seed=rank)
     sim = make_simulator(scene, diagnostics="lean")
     n = scene.particle_count
+    if args.rollout_only:
+        steps, every = args.rollout_only
+        out = rollout_variant(sim, dist, torch.cuda.current_stream(), world,
+                              f"box loaf {n} particles, {args.resolution}^3, Ding + gas + thermal-water",
+                              fb_steps=steps, every=every)
+        if rank == 0:
+            print(json.dumps(dict(out, metric="forward + adjoint particle-substeps/s", n_gpus=world)))
+        if dist:
+            dist.destroy_process_group()
+        return
     for _ in range(args.warmup):
         sim.AdvanceUnchecked(1)
     torch.cuda.synchronize()

@@ -433,6 +433,54 @@ BK_API int bk_transport_adjoint(const BkSubstepParams *params, const BkState *in
                                 const BkGrid *grid, const BkSurface *surface, const BkAdjointState *mechanics,
                                 BkAdjointTransport *adjoint, void *stream);
 
+/* The recorder's per-step measurements (experiments/recording.py:46-112, SimulationRecorder.Measure)
+   as one device reduction over the particles, mesh vertices and tets, in place of pulling every
+   array to the host. Arrays are in plane layout with `pitch` (vertices: `vertex_pitch`); groups
+   whose pointers are NULL are skipped and their slots left 0. `regions` marks particles: bit 0 a
+   surface-face owner, bit 1 the initial core. */
+typedef struct BkMeasureInputs {
+    int64_t n, pitch;
+    const float *F;                              /* 9 planes */
+    const float *reference_volume;               /* n */
+    const float *material_temperature, *porosity; /* Ding */
+    const int32_t *gelled;                       /* Ding */
+    const double *gas_moles, *gas_pressure;      /* gas mode */
+    const double *temperature, *water, *saturation, *water_losses, *heat_exchanges, *capacity; /* transport */
+    const uint8_t *regions;                      /* transport */
+    int64_t vertex_count, vertex_pitch;
+    const float *vertices;                       /* 3 planes */
+    int64_t tet_count;
+    const int32_t *tets;                         /* tet_count x 4 */
+} BkMeasureInputs;
+
+/* Slots of bk_measure_state's output (float64). */
+enum {
+    BK_MEASURE_PARTICLE_VOLUME = 0,  /* sum V0 det F */
+    BK_MEASURE_INVALID_PARTICLES,    /* count det F <= 0 */
+    BK_MEASURE_NONFINITE,            /* count of particles or vertices with a nonfinite F or position */
+    BK_MEASURE_MATERIAL_T_SUM,       /* Ding: sum of the material temperatures */
+    BK_MEASURE_POROSITY_SUM, BK_MEASURE_POROSITY_MIN, BK_MEASURE_POROSITY_MAX,
+    BK_MEASURE_GELLED,               /* count of gelled particles */
+    BK_MEASURE_GAS_TOTAL,            /* sum V0 N */
+    BK_MEASURE_PRESSURE_SUM, BK_MEASURE_PRESSURE_MIN, BK_MEASURE_PRESSURE_MAX,
+    BK_MEASURE_PORE_VOLUME,          /* sum V0 det F n */
+    BK_MEASURE_T_MIN, BK_MEASURE_T_MAX,
+    BK_MEASURE_ENERGY,               /* sum c T */
+    BK_MEASURE_CAPACITY,             /* sum c */
+    BK_MEASURE_SURFACE_T_SUM, BK_MEASURE_SURFACE_COUNT, BK_MEASURE_CORE_T_SUM, BK_MEASURE_CORE_COUNT,
+    BK_MEASURE_WATER, BK_MEASURE_WATER_LOST, BK_MEASURE_HEAT_EXCHANGE,
+    BK_MEASURE_SATURATION_SUM, BK_MEASURE_SATURATION_MIN, BK_MEASURE_SATURATION_MAX,
+    BK_MEASURE_X_MIN, BK_MEASURE_Y_MIN, BK_MEASURE_Z_MIN, BK_MEASURE_X_MAX, BK_MEASURE_Y_MAX, BK_MEASURE_Z_MAX,
+    BK_MEASURE_MESH_VOLUME,          /* sum |signed tet volume| */
+    BK_MEASURE_INVERTED_TETS,        /* count signed volume <= 0 */
+    BK_MEASURE_SLOTS
+};
+#define BK_MEASURE_BLOCKS 296        /* partial results per slot held in `scratch` */
+
+/* out: BK_MEASURE_SLOTS doubles (device); scratch: BK_MEASURE_BLOCKS * BK_MEASURE_SLOTS doubles
+   (device). Deterministic: fixed grid, per-block partials reduced in a fixed order. */
+BK_API int bk_measure_state(const BkMeasureInputs *in, double *out, double *scratch, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

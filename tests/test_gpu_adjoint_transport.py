@@ -23,17 +23,18 @@ def _torch():
 
 
 # ----------------------------------------------------------------- known answer
-def thermal_sim(viscosity):
-    """BuildThermalSimulator(short_curve=True): demo cube, Ding with temperature and porosity 0.2,
-    yield 5 Pa, dt 1 ms, transport with water off from 300 K, strain-rate field."""
+def thermal_sim(viscosity, short_curve=True):
+    """BuildThermalSimulator: demo cube, Ding with temperature and porosity 0.2, transport with water
+    off from 300 K, strain-rate field; short_curve: yield 5 Pa and dt 1 ms, else 100 Pa and 0.1 ms."""
     from baking_b200.physics.mpm import MpmSimulator
     from tests.scenes import assign, to_np
     mesh = CreateDemoMesh(1)
     sim = MpmSimulator(mesh, SampleParticles(mesh, 1000.0, 4),
-                       replace(SimulationConfig(), device_name="cuda:0", time_step=0.001, gravity=(0.0, 0.0, 0.0)),
+                       replace(SimulationConfig(), device_name="cuda:0", time_step=0.001 if short_curve else 0.0001,
+                               gravity=(0.0, 0.0, 0.0)),
                        MaterialConfig(model="ding2019"),
-                       ding_config=DingConfig(temperature_enabled=True, porosity=0.2, yield_stress=5.0,
-                                              viscosity=viscosity),
+                       ding_config=DingConfig(temperature_enabled=True, porosity=0.2,
+                                              yield_stress=5.0 if short_curve else 100.0, viscosity=viscosity),
                        transport_config=TransportConfig(enabled=True, water_enabled=False,
                                                         initial_temperature_k=300.0))
     st = sim.current_state
