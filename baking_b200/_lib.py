@@ -53,6 +53,7 @@ SIGNATURES = {
     "bk_saturations": [I64, I64, P, P, P, P, F32, P],
     "bk_settling_metrics": [I64, I64, P, P, P, P, P, F32, P],
     "bk_measure_state": [P, P, P, P],
+    "bk_step_summary": [P, P, P, P, P, P, P],
     "bk_solve_porosity": [I64, P, P, P, P, P, P, F32, P, P, P],
     "bk_porosity_coefficient": [I64, P, P, P],
     "bk_profile_start": [],

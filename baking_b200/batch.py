@@ -85,6 +85,103 @@ class BatchedSimulators:
         return [sim.CheckState() for sim in self.sims]
 
 
+class SubstepGraphs:
+    """One simulator's substep as two captured CUDA graphs, state A -> B and B -> A, each followed
+    by the step-result reduction (``MpmSimulator.StepSummary``): ``Advance(1)`` is one graph launch.
+    For callers that read a result back after every substep, where the per-kernel host launch cost
+    would otherwise sit between the substeps.
+
+    ``inputs``: device tensors the caller refills before every substep (per-particle gas source
+    rates, say). Each graph starts by copying them from a staging buffer of its own, so ``load``
+    can upload the inputs of the substep after the next one from pinned host memory, on a copy
+    stream, while the next one runs. The graphs hold the simulator's arrays and parameters at
+    capture time: refill parameter tensors in place between steps, and capture again after
+    replacing one."""
+
+    def __init__(self, sim, inputs=()):
+        if sim.IsSettling:
+            raise ValueError("captured substeps start after settling (settling_duration_s = 0)")
+        if sim.retain_history:
+            raise ValueError("captured substeps keep no history")
+        self.sim = sim
+        self.summary = torch.zeros(2, dtype=torch.float64, device=sim.device)
+        self.inputs = list(inputs)
+        self.staging = [[torch.empty_like(t) for t in self.inputs] for _ in range(2)]
+        self.loaded = [None, None]     # events: staging set k filled
+        self.consumed = [None, None]   # events: the last graph that read staging set k finished
+        self.graphs = None
+        self._first = None
+
+    def _record(self, state_in, state_out, parity):
+        for t, staged in zip(self.inputs, self.staging[parity]):
+            t.copy_(staged)
+        BatchedSimulators._substep(self.sim, state_in, state_out)
+        self.sim._engine.step_summary(state_out, self.summary)
+
+    def _parity(self, ahead=0):
+        """Staging set read by the substep ``ahead`` substeps after the next one."""
+        return ((0 if self.sim._current is self._first else 1) + ahead) % 2
+
+    def capture(self):
+        """Build both graphs. The substeps run once outside capture first (which advances the
+        simulator by two substeps); the staging buffers then hold the inputs' current values."""
+        sim = self.sim
+        a, b = sim._current, sim.next_state
+        self._first = a
+        for k in range(2):
+            for t, staged in zip(self.inputs, self.staging[k]):
+                staged.copy_(t)
+        torch.cuda.synchronize()
+        self._record(a, b, 0)
+        self._record(b, a, 1)
+        torch.cuda.synchronize()
+        sim.step_count += 2
+        sim._stale = True
+        graphs = {}
+        for parity, (src, dst) in enumerate(((a, b), (b, a))):
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._record(src, dst, parity)
+            graphs[id(src)] = (g, dst, parity)
+        self.graphs = graphs
+        return self
+
+    def load(self, host_tensors, ahead=0, stream=None):
+        """Copy ``host_tensors`` (pinned, one per input) into the staging set of the substep
+        ``ahead`` substeps after the next ``Advance`` step, on ``stream`` (default: current)."""
+        parity = self._parity(ahead)
+        stream = stream or torch.cuda.current_stream()
+        with torch.cuda.stream(stream):
+            if self.consumed[parity] is not None:
+                stream.wait_event(self.consumed[parity])
+            for staged, host in zip(self.staging[parity], host_tensors):
+                staged.copy_(host, non_blocking=True)
+            event = torch.cuda.Event()
+            event.record(stream)
+        self.loaded[parity] = event
+
+    def Advance(self, steps=1):
+        """Advance by ``steps`` substeps; returns the device tensor (grid mass, kinetic energy) of
+        the last one."""
+        if self.graphs is None:
+            self.capture()
+        sim = self.sim
+        main = torch.cuda.current_stream()
+        for _ in range(steps):
+            graph, nxt, parity = self.graphs[id(sim._current)]
+            if self.loaded[parity] is not None:
+                main.wait_event(self.loaded[parity])
+                self.loaded[parity] = None
+            graph.replay()
+            done = torch.cuda.Event()
+            done.record(main)
+            self.consumed[parity] = done
+            sim.next_state, sim._current = sim._current, nxt
+            sim.step_count += 1
+            sim._stale = True
+        return self.summary
+
+
 def _state_tensors(sim):
     from dataclasses import fields
     st = sim._current

@@ -180,7 +180,83 @@ __global__ void k_measure_finish(const double* __restrict__ partial, double* __r
     out[s] = v;
 }
 
+// Step result: the grid mass of the last substep (node masses over its active box, the only
+// nonzero nodes) and the particles' kinetic energy sum 1/2 m |v|^2 with m = dry + W under
+// transport, in two deterministic passes like k_measure.
+__global__ void __launch_bounds__(kThreads) k_step_summary(int64_t n, int64_t pitch, const float* __restrict__ v,
+                                                         const float* __restrict__ mass, const double* __restrict__ dry,
+                                                         const double* __restrict__ water, const float4* __restrict__ pm,
+                                                         const int32_t* __restrict__ box, int R,
+                                                         double* __restrict__ partial) {
+    double grid = 0.0, kinetic = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t first = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (int64_t i = first; i < n; i += stride) {
+        const double m = water ? dry[i] + water[i] : (double)mass[i];
+        const double a = v[i], b = v[pitch + i], c = v[2 * pitch + i];
+        kinetic += 0.5 * m * (a * a + b * b + c * c);
+    }
+    int lo[3], ext[3];
+    int64_t count = 1;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int l = max(box[k], 0), h = min(box[3 + k], R - 1);
+        lo[k] = l;
+        ext[k] = h >= l ? h - l + 1 : 0;
+        count *= ext[k];
+    }
+    for (int64_t t = first; t < count; t += stride) {
+        const int z = lo[2] + (int)(t % ext[2]);
+        const int y = lo[1] + (int)((t / ext[2]) % ext[1]);
+        const int x = lo[0] + (int)(t / ((int64_t)ext[2] * ext[1]));
+        grid += (double)pm[node_index(x, y, z, R)].w;
+    }
+    __shared__ double s_warp[2][kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        grid += __shfl_xor_sync(0xffffffffu, grid, o);
+        kinetic += __shfl_xor_sync(0xffffffffu, kinetic, o);
+    }
+    if (lane == 0) {
+        s_warp[0][warp] = grid;
+        s_warp[1][warp] = kinetic;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        double b = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w) b += s_warp[threadIdx.x][w];
+        partial[2 * (int64_t)blockIdx.x + threadIdx.x] = b;
+    }
+}
+
+__global__ void k_step_summary_finish(const double* __restrict__ partial, double* __restrict__ out, int blocks) {
+    const int k = threadIdx.x;
+    if (k >= 2) return;
+    double v = 0.0;
+    for (int b = 0; b < blocks; ++b) v += partial[2 * b + k];
+    out[k] = v;
+}
+
 }  // namespace
+
+extern "C" int bk_step_summary(const BkSubstepParams* params, const BkState* state, const BkConstants* constants,
+                               const BkGrid* grid, double* out, double* scratch, void* stream) {
+    if (!params || !state || !constants || !grid || !out || !scratch)
+        return fail(BK_ERR_ARGUMENT, "bk_step_summary: null argument");
+    const BkSubstepParams& p = *params;
+    if (!state->v || !grid->node_pm || !grid->bounds || (p.transport ? (!constants->dry_mass || !state->water)
+                                                                      : !constants->mass))
+        return fail(BK_ERR_ARGUMENT, "bk_step_summary: missing arrays");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    k_step_summary<<<BK_MEASURE_BLOCKS, kThreads, 0, s>>>(p.n, p.pitch, state->v, constants->mass, constants->dry_mass,
+                                                          p.transport ? state->water : nullptr,
+                                                          reinterpret_cast<const float4*>(grid->node_pm),
+                                                          grid->bounds + 6, p.resolution, scratch);
+    if (int rc = check_launch("bk_step_summary")) return rc;
+    k_step_summary_finish<<<1, 32, 0, s>>>(scratch, out, BK_MEASURE_BLOCKS);
+    return check_launch("bk_step_summary/finish");
+}
 
 extern "C" int bk_measure_state(const BkMeasureInputs* in, double* out, double* scratch, void* stream) {
     if (!in || !out || !scratch) return fail(BK_ERR_ARGUMENT, "bk_measure_state: null argument");

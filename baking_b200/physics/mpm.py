@@ -319,11 +319,11 @@ class MpmSimulator:
         for _ in range(step_count):
             self._substep(check=False)
 
-    def StepSummary(self):
-        """Device tensor (grid mass, particle kinetic energy) of the current state, float64."""
-        masses = self.Masses().double()
-        v = self.current_state.particle_velocities.double()
-        return torch.stack([self.grid_state.node_masses.double().sum(), 0.5 * (masses * (v * v).sum(1)).sum()])
+    def StepSummary(self, out=None):
+        """Device tensor (grid mass of the last substep, particle kinetic energy of the current
+        state), float64, from one fused reduction (``bk_step_summary``); ``out`` (2 doubles) may
+        be given to write into."""
+        return self._engine.step_summary(self._current, out)
 
     def AlgorithmicBytes(self, kernel, active_nodes):
         """Bytes one launch of ``kernel`` must move (each input and output array once), or None."""

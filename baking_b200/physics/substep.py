@@ -291,6 +291,20 @@ class SubstepEngine:
         if rc != 0:
             raise RuntimeError(f"bk_substep failed ({rc}): {self.lib.bk_last_error().decode(errors='replace')}")
 
+    def step_summary(self, state, out=None):
+        """(grid mass of the last substep, kinetic energy of ``state``) as a float64 device tensor."""
+        dev = self.sim.device
+        if out is None:
+            out = torch.empty(2, dtype=torch.float64, device=dev)
+        if getattr(self, "_summary_scratch", None) is None:
+            self._summary_scratch = torch.empty(2 * 296, dtype=torch.float64, device=dev)
+        p = self.params(False)
+        cst = self.constants(False)
+        s = state_struct(state, self.is_ding, self.transport, self.gas)
+        _lib.call_raw(self.lib.bk_step_summary, "bk_step_summary", C.byref(p), C.byref(s), C.byref(cst),
+                      C.byref(self.grid), out.data_ptr(), self._summary_scratch.data_ptr(), _lib.stream_handle())
+        return out
+
     def accumulate_surface(self, transport_state):
         if not self.transport or self.surface.owner_count == 0:
             return

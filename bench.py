@@ -249,10 +249,14 @@ def main():
     active = active_node_count(sim)
 
     # End to end through the public API: pinned host inputs (the per-particle gas source rates) uploaded
-    # every substep, the substep, and the step's result (grid mass, kinetic energy) read back to the host.
+    # for every substep, the substep (SubstepGraphs: one graph launch per substep, with the step-result
+    # reduction), and the step's result (grid mass, kinetic energy) read back to the host. Each
+    # substep's upload runs on a copy stream while the substep before it computes.
+    from baking_b200.batch import SubstepGraphs
     host_rates = torch.from_numpy(scene.gas_source_rates).pin_memory()
-    device_rates = sim.material.production_parameter
     e2e_steps = max(1, min(args.steps, 100))
+    stepper = SubstepGraphs(sim, inputs=[sim.material.production_parameter]).capture()
+    copy_stream = torch.cuda.Stream()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -260,10 +264,12 @@ def main():
     e1 = torch.cuda.Event(enable_timing=True)
     wall0 = time.perf_counter()
     e0.record(stream)
-    for _ in range(e2e_steps):
-        device_rates.copy_(host_rates, non_blocking=True)
-        sim.AdvanceUnchecked(1)
-        result = sim.StepSummary().cpu()
+    stepper.load([host_rates], 0, copy_stream)
+    for k in range(e2e_steps):
+        out = stepper.Advance(1)
+        if k + 1 < e2e_steps:
+            stepper.load([host_rates], 0, copy_stream)  # the next substep's inputs, during this one
+        result = out.cpu()
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_elapsed = max(e0.elapsed_time(e1) / 1e3, time.perf_counter() - wall0)
@@ -271,7 +277,7 @@ def main():
         t = torch.tensor([e2e_elapsed], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_elapsed = float(t.item())
-    del result
+    del result, stepper
 
     peak, peak_kind = load_peaks()
     traffic = load_traffic(n)

@@ -481,6 +481,14 @@ enum {
    (device). Deterministic: fixed grid, per-block partials reduced in a fixed order. */
 BK_API int bk_measure_state(const BkMeasureInputs *in, double *out, double *scratch, void *stream);
 
+/* A substep's result for a caller that reads one back per step (no counterpart in the reference,
+   whose callers pull whole arrays): out[0] = grid mass of the last substep (node masses over the
+   active box in grid->bounds + 6), out[1] = particle kinetic energy sum 1/2 m |v|^2 of `state`
+   (m = dry + W with transport, else constants->mass). out: 2 doubles, scratch: 2 *
+   BK_MEASURE_BLOCKS doubles (device). Deterministic. */
+BK_API int bk_step_summary(const BkSubstepParams *params, const BkState *state, const BkConstants *constants,
+                           const BkGrid *grid, double *out, double *scratch, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
