@@ -483,44 +483,14 @@ __global__ void __launch_bounds__(kThreads) k_tadj_scatter(TParams P, BkState in
 
 // ---------------------------------------------------------------- surface
 // Mesh vertex positions of this substep (geometry/mesh_tracking.py:13-38) into surface.vertices,
-// as the forward's transport phase computed them: one warp per boundary vertex,
-// anchor + sum_b w_b (pred_b - anchor) with pred_b = x_p + F_p o_b and the first binding's
-// prediction as the anchor, summed lane-strided and reduced in the same order.
-__global__ void k_tadj_vertex_positions(TParams P, const float* __restrict__ x, const float* __restrict__ F,
-                                        BkSurface sf) {
-    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= sf.vertex_count) return;
-    const int vid = sf.vertex_ids[w];
-    const int b0 = sf.binding_offsets[vid], b1 = sf.binding_offsets[vid + 1];
-    const int64_t vp = sf.vertex_pitch, bp = sf.binding_pitch, pitch = P.pitch;
-    if (b0 == b1) {
-        if (lane < 3) sf.vertices[lane * vp + vid] = sf.reference_vertices[lane * vp + vid];
-        return;
-    }
-    auto predict = [&](int b, float* r) {
-        const int p = sf.binding_particles[b];
-        const M3 f = load_m3(F, p, pitch);
-        const V3 xp = load_v3(x, p, pitch);
-        const float o[3] = {sf.reference_offsets[b], sf.reference_offsets[bp + b], sf.reference_offsets[2 * bp + b]};
-#pragma unroll
-        for (int a = 0; a < 3; ++a) r[a] = xp.v[a] + (f.m[3 * a] * o[0] + f.m[3 * a + 1] * o[1] + f.m[3 * a + 2] * o[2]);
-    };
-    float anchor[3];
-    predict(b0, anchor);
-    float disp[3] = {0.f, 0.f, 0.f};
-    for (int b = b0 + lane; b < b1; b += 32) {
-        float pr[3];
-        predict(b, pr);
-        const float wgt = sf.binding_weights[b];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) disp[a] += wgt * (pr[a] - anchor[a]);
-    }
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) disp[a] += __shfl_xor_sync(0xffffffffu, disp[a], o);
-    if (lane < 3) sf.vertices[lane * vp + vid] = anchor[lane] + disp[lane];
+// as the forward's transport phase computes them (vertex_block: one block per boundary vertex).
+__global__ void __launch_bounds__(kThreads) k_tadj_vertex_positions(TParams P, const float* __restrict__ x,
+                                                                  const float* __restrict__ F, BkSurface sf) {
+    const int vid = sf.vertex_ids[blockIdx.x];
+    const float v = vertex_block<kThreads>(sf.binding_offsets, sf.binding_particles, sf.binding_weights,
+                                           sf.reference_offsets, sf.binding_pitch, sf.reference_vertices,
+                                           sf.vertex_pitch, x, F, P.pitch, vid);
+    if (threadIdx.x < 3) sf.vertices[threadIdx.x * sf.vertex_pitch + vid] = v;
 }
 
 __device__ __forceinline__ void face_vertices(const BkSurface& sf, int f, double q[3][3], int vid[3]) {
@@ -624,24 +594,28 @@ __global__ void k_tadj_owners(TParams P, BkState in, BkConstants cst, BkSurface 
     }
 }
 
-// One warp per surface vertex: its adjoint to the bound particles' x and F, then zeroed.
-__global__ void k_tadj_vertices(TParams P, BkSurface sf, BkAdjointTransport a, const BkAdjointState adj) {
-    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= sf.vertex_count) return;
-    const int vid = sf.vertex_ids[w];
+// One block per surface vertex: its adjoint to the bound particles' x and F, then zeroed.
+__global__ void __launch_bounds__(kThreads) k_tadj_vertices(TParams P, BkSurface sf, BkAdjointTransport a,
+                                                          const BkAdjointState adj) {
+    __shared__ float s_w[kThreads / 32];
+    const int vid = sf.vertex_ids[blockIdx.x];
+    const int t = threadIdx.x;
     const int64_t vp = sf.vertex_pitch, bp = sf.binding_pitch, pitch = P.pitch;
     const double vb[3] = {a.vertices[vid], a.vertices[vp + vid], a.vertices[2 * vp + vid]};
-    __syncwarp();
-    if (lane < 3) a.vertices[lane * vp + vid] = 0.0;
+    __syncthreads();
+    if (t < 3) a.vertices[t * vp + vid] = 0.0;
     const int b0 = sf.binding_offsets[vid], b1 = sf.binding_offsets[vid + 1];
-    if (b0 == b1 || (vb[0] == 0.0 && vb[1] == 0.0 && vb[2] == 0.0)) return;
+    if (b0 == b1 || (vb[0] == 0.0 && vb[1] == 0.0 && vb[2] == 0.0)) return;  // the same for the whole block
     // v = (1 - sum_b w_b) pred_b0 + sum_b w_b pred_b
     float wsum = 0.f;
-    for (int b = b0 + lane; b < b1; b += 32) wsum += sf.binding_weights[b];
+    for (int b = b0 + t; b < b1; b += kThreads) wsum += sf.binding_weights[b];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
-    for (int b = b0 + lane; b < b1; b += 32) {
+    if ((t & 31) == 0) s_w[t >> 5] = wsum;
+    __syncthreads();
+    wsum = 0.f;
+    for (int w = 0; w < kThreads / 32; ++w) wsum += s_w[w];
+    for (int b = b0 + t; b < b1; b += kThreads) {
         const float c = sf.binding_weights[b] + (b == b0 ? 1.f - wsum : 0.f);
         const int p = sf.binding_particles[b];
         const float o[3] = {sf.reference_offsets[b], sf.reference_offsets[bp + b], sf.reference_offsets[2 * bp + b]};
@@ -768,7 +742,7 @@ int bk_transport_adjoint(const BkSubstepParams* params, const BkState* in, const
     k_tadj_scatter<<<blocks(p.n, kThreads), kThreads, 0, s>>>(P, *in, *constants, g, a, *mechanics);
     if (int rc = check_launch("bk_transport_adjoint/scatter")) return rc;
     if (surface->vertex_count > 0) {
-        k_tadj_vertex_positions<<<blocks(surface->vertex_count * 32, 128), 128, 0, s>>>(P, in->x, in->F, *surface);
+        k_tadj_vertex_positions<<<(unsigned)surface->vertex_count, kThreads, 0, s>>>(P, in->x, in->F, *surface);
         if (int rc = check_launch("bk_transport_adjoint/vertex_positions")) return rc;
     }
     if (surface->owner_count > 0) {
@@ -776,7 +750,7 @@ int bk_transport_adjoint(const BkSubstepParams* params, const BkState* in, const
         if (int rc = check_launch("bk_transport_adjoint/owners")) return rc;
     }
     if (surface->vertex_count > 0) {
-        k_tadj_vertices<<<blocks(surface->vertex_count * 32, 128), 128, 0, s>>>(P, *surface, a, *mechanics);
+        k_tadj_vertices<<<(unsigned)surface->vertex_count, kThreads, 0, s>>>(P, *surface, a, *mechanics);
         if (int rc = check_launch("bk_transport_adjoint/vertices")) return rc;
     }
     k_tadj_clear<<<box_blocks, 256, 0, s>>>(P, g, box);

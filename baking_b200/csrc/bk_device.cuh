@@ -797,4 +797,56 @@ BK_DEV double gas_pressure(double moles, float T, float J, float n) {
     return moles * kGasConstant * (double)T / ((double)J * (double)n);
 }
 
+// ------------------------------------------- geometry/mesh_tracking.py:13-38
+// One mesh vertex reconstructed by a whole block of kBlock threads: anchor + sum_b w_b (pred_b -
+// anchor) over its bindings b0..b1, pred_b = x_p + F_p o_b (o_b: the binding's reference offset,
+// 3 planes of `bp`), the anchor being the first binding's prediction; a vertex without bindings
+// keeps its reference position. Every thread of the block must call it (it synchronises the block);
+// threads 0, 1, 2 get components x, y, z.
+template <int kBlock>
+BK_DEV float vertex_block(const int* __restrict__ offsets, const int* __restrict__ particles,
+                          const float* __restrict__ weights, const float* __restrict__ ref_offsets, int64_t bp,
+                          const float* __restrict__ ref_vertices, int64_t vp, const float* __restrict__ x,
+                          const float* __restrict__ F, int64_t pitch, int vid) {
+    __shared__ float s_part[3][kBlock / 32];
+    const int b0 = offsets[vid], b1 = offsets[vid + 1];
+    const int t = threadIdx.x;
+    if (b0 == b1) return t < 3 ? ref_vertices[t * vp + vid] : 0.0f;  // the same branch for the whole block
+    auto predict = [&](int b, float* r) {
+        const int p = particles[b];
+        const M3 f = load_m3(F, p, pitch);
+        const V3 xp = load_v3(x, p, pitch);
+        const float o[3] = {ref_offsets[b], ref_offsets[bp + b], ref_offsets[2 * bp + b]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) r[a] = xp.v[a] + (f.m[3 * a] * o[0] + f.m[3 * a + 1] * o[1] + f.m[3 * a + 2] * o[2]);
+    };
+    float anchor[3];
+    predict(b0, anchor);
+    float disp[3] = {0.f, 0.f, 0.f};
+#pragma unroll 4
+    for (int b = b0 + t; b < b1; b += kBlock) {  // unrolled: several bindings' gathers in flight
+        float pr[3];
+        predict(b, pr);
+        const float w = weights[b];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) disp[a] += w * (pr[a] - anchor[a]);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) disp[a] += __shfl_xor_sync(0xffffffffu, disp[a], o);
+    if ((t & 31) == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) s_part[a][t >> 5] = disp[a];
+    }
+    __syncthreads();
+    float out = 0.0f;
+    if (t < 3) {
+        float sum = 0.0f;
+        for (int w = 0; w < kBlock / 32; ++w) sum += s_part[t][w];
+        out = anchor[t] + sum;
+    }
+    return out;
+}
+
 }  // namespace bk

@@ -174,42 +174,15 @@ __device__ __forceinline__ int64_t tile_node(const BlockBox& bb, int t, int R) {
 }
 
 // ------------------------------------------------------------------ surface
-// geometry/mesh_tracking.py:13-38 restricted to the vertices of boundary faces; one warp per vertex.
-__global__ void k_surface_vertices(Params P, const float* __restrict__ x, const float* __restrict__ F,
-                                   BkSurface sf) {
-    int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    if (w >= sf.vertex_count) return;
-    int vid = sf.vertex_ids[w];
-    int b0 = sf.binding_offsets[vid], b1 = sf.binding_offsets[vid + 1];
-    const int64_t vp = sf.vertex_pitch, bp = sf.binding_pitch, pitch = P.pitch;
-    if (b0 == b1) {
-        if (lane < 3) sf.vertices[lane * vp + vid] = sf.reference_vertices[lane * vp + vid];
-        return;
-    }
-    auto predict = [&](int b, float* r) {
-        int p = sf.binding_particles[b];
-        M3 f = load_m3(F, p, pitch);
-        V3 xp = load_v3(x, p, pitch);
-        float o[3] = {sf.reference_offsets[b], sf.reference_offsets[bp + b], sf.reference_offsets[2 * bp + b]};
-#pragma unroll
-        for (int a = 0; a < 3; ++a) r[a] = xp.v[a] + (f.m[3 * a] * o[0] + f.m[3 * a + 1] * o[1] + f.m[3 * a + 2] * o[2]);
-    };
-    float anchor[3];
-    predict(b0, anchor);
-    float disp[3] = {0.f, 0.f, 0.f};
-    for (int b = b0 + lane; b < b1; b += 32) {
-        float pr[3];
-        predict(b, pr);
-        float wgt = sf.binding_weights[b];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) disp[a] += wgt * (pr[a] - anchor[a]);
-    }
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) disp[a] += __shfl_xor_sync(kFull, disp[a], o);
-    if (lane < 3) sf.vertices[lane * vp + vid] = anchor[lane] + disp[lane];
+// geometry/mesh_tracking.py:13-38 restricted to the vertices of boundary faces; one block per
+// vertex (a vertex binds thousands of particles: a block keeps enough gathers in flight).
+__global__ void __launch_bounds__(kThreads) k_surface_vertices(Params P, const float* __restrict__ x,
+                                                             const float* __restrict__ F, BkSurface sf) {
+    const int vid = sf.vertex_ids[blockIdx.x];
+    const float v = vertex_block<kThreads>(sf.binding_offsets, sf.binding_particles, sf.binding_weights,
+                                           sf.reference_offsets, sf.binding_pitch, sf.reference_vertices,
+                                           sf.vertex_pitch, x, F, P.pitch, vid);
+    if (threadIdx.x < 3) sf.vertices[threadIdx.x * sf.vertex_pitch + vid] = v;
 }
 
 // physics/thermal_water.py:77-92 (face areas, tray contact) and the surface terms of :108-122,
@@ -1093,7 +1066,7 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
         if (surface->vertex_count > 0) {
             {
                 int rec = profile_begin("surface_vertices", s);
-                k_surface_vertices<<<blocks_for(surface->vertex_count * 32, kThreads), kThreads, 0, s>>>(P, in->x, in->F,
+                k_surface_vertices<<<(unsigned)surface->vertex_count, kThreads, 0, s>>>(P, in->x, in->F,
                                                                                                    *surface);
                 profile_end(rec, s);
             }
