@@ -41,8 +41,10 @@ def vec3s(n, dtype=torch.float32, device="cuda", pitch=None):
 
 
 def mat33s(n, dtype=torch.float32, device="cuda", pitch=None):
-    storage, _ = _planes(9, n, dtype, device, pitch)
-    return storage.t()[:n].view(n, 3, 3) if n > 0 else storage.t()[:0].reshape(0, 3, 3)
+    storage, pitch = _planes(9, n, dtype, device, pitch)
+    if n > 0:
+        return storage.t()[:n].view(n, 3, 3)
+    return storage.as_strided((0, 3, 3), (1, 3 * pitch, pitch))  # empty, with the plane strides
 
 
 def layout_pitch(t):
