@@ -124,7 +124,8 @@ def test_wall_clamp_in_boundary_cells():
     v[:32] = -5.0
     x[32:] = rng.uniform((R - 3.4) * DX, (R - 2.6) * DX, (32, 3)).astype(np.float32)  # near the high walls
     v[32:] = 5.0
-    dev, ref = device_transfer(x, v, C, tau, m, V0, F)
+    arrs = (x, v, C, tau, m, V0, F)
+    dev, ref = device_transfer(*arrs), oracle_transfer(*arrs)
     compare(dev, ref, np.ones(n, dtype=bool))
     nv = dev["node_v"][:, :3].reshape(R, R, R, 3)
     assert (nv[:3, :, :, 0] >= 0).all() and (nv[R - 3:, :, :, 0] <= 0).all()
