@@ -484,10 +484,11 @@ __global__ void __launch_bounds__(kThreads) k_tadj_scatter(TParams P, BkState in
 // ---------------------------------------------------------------- surface
 // Mesh vertex positions of this substep (geometry/mesh_tracking.py:13-38) into surface.vertices,
 // as the forward's transport phase computes them (vertex_block: one block per boundary vertex).
-__global__ void __launch_bounds__(kThreads) k_tadj_vertex_positions(TParams P, const float* __restrict__ x,
-                                                                  const float* __restrict__ F, BkSurface sf) {
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock) k_tadj_vertex_positions(TParams P, const float* __restrict__ x,
+                                                               const float* __restrict__ F, BkSurface sf) {
     const int vid = sf.vertex_ids[blockIdx.x];
-    const float v = vertex_block<kThreads>(sf.binding_offsets, sf.binding_particles, sf.binding_weights,
+    const float v = vertex_block<kBlock>(sf.binding_offsets, sf.binding_particles, sf.binding_weights,
                                            sf.reference_offsets, sf.binding_pitch, sf.reference_vertices,
                                            sf.vertex_pitch, x, F, P.pitch, vid);
     if (threadIdx.x < 3) sf.vertices[threadIdx.x * sf.vertex_pitch + vid] = v;
@@ -595,9 +596,10 @@ __global__ void k_tadj_owners(TParams P, BkState in, BkConstants cst, BkSurface 
 }
 
 // One block per surface vertex: its adjoint to the bound particles' x and F, then zeroed.
-__global__ void __launch_bounds__(kThreads) k_tadj_vertices(TParams P, BkSurface sf, BkAdjointTransport a,
-                                                          const BkAdjointState adj) {
-    __shared__ float s_w[kThreads / 32];
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock) k_tadj_vertices(TParams P, BkSurface sf, BkAdjointTransport a,
+                                                       const BkAdjointState adj) {
+    __shared__ float s_w[kBlock / 32];
     const int vid = sf.vertex_ids[blockIdx.x];
     const int t = threadIdx.x;
     const int64_t vp = sf.vertex_pitch, bp = sf.binding_pitch, pitch = P.pitch;
@@ -608,14 +610,14 @@ __global__ void __launch_bounds__(kThreads) k_tadj_vertices(TParams P, BkSurface
     if (b0 == b1 || (vb[0] == 0.0 && vb[1] == 0.0 && vb[2] == 0.0)) return;  // the same for the whole block
     // v = (1 - sum_b w_b) pred_b0 + sum_b w_b pred_b
     float wsum = 0.f;
-    for (int b = b0 + t; b < b1; b += kThreads) wsum += sf.binding_weights[b];
+    for (int b = b0 + t; b < b1; b += kBlock) wsum += sf.binding_weights[b];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
     if ((t & 31) == 0) s_w[t >> 5] = wsum;
     __syncthreads();
     wsum = 0.f;
-    for (int w = 0; w < kThreads / 32; ++w) wsum += s_w[w];
-    for (int b = b0 + t; b < b1; b += kThreads) {
+    for (int w = 0; w < kBlock / 32; ++w) wsum += s_w[w];
+    for (int b = b0 + t; b < b1; b += kBlock) {
         const float c = sf.binding_weights[b] + (b == b0 ? 1.f - wsum : 0.f);
         const int p = sf.binding_particles[b];
         const float o[3] = {sf.reference_offsets[b], sf.reference_offsets[bp + b], sf.reference_offsets[2 * bp + b]};
@@ -742,7 +744,12 @@ int bk_transport_adjoint(const BkSubstepParams* params, const BkState* in, const
     k_tadj_scatter<<<blocks(p.n, kThreads), kThreads, 0, s>>>(P, *in, *constants, g, a, *mechanics);
     if (int rc = check_launch("bk_transport_adjoint/scatter")) return rc;
     if (surface->vertex_count > 0) {
-        k_tadj_vertex_positions<<<(unsigned)surface->vertex_count, kThreads, 0, s>>>(P, in->x, in->F, *surface);
+        const unsigned nv = (unsigned)surface->vertex_count;
+        switch (vertex_block_threads(surface->vertex_count, surface->binding_count)) {
+            case 256: k_tadj_vertex_positions<256><<<nv, 256, 0, s>>>(P, in->x, in->F, *surface); break;
+            case 128: k_tadj_vertex_positions<128><<<nv, 128, 0, s>>>(P, in->x, in->F, *surface); break;
+            default: k_tadj_vertex_positions<32><<<nv, 32, 0, s>>>(P, in->x, in->F, *surface); break;
+        }
         if (int rc = check_launch("bk_transport_adjoint/vertex_positions")) return rc;
     }
     if (surface->owner_count > 0) {
@@ -750,7 +757,12 @@ int bk_transport_adjoint(const BkSubstepParams* params, const BkState* in, const
         if (int rc = check_launch("bk_transport_adjoint/owners")) return rc;
     }
     if (surface->vertex_count > 0) {
-        k_tadj_vertices<<<(unsigned)surface->vertex_count, kThreads, 0, s>>>(P, *surface, a, *mechanics);
+        const unsigned nv = (unsigned)surface->vertex_count;
+        switch (vertex_block_threads(surface->vertex_count, surface->binding_count)) {
+            case 256: k_tadj_vertices<256><<<nv, 256, 0, s>>>(P, *surface, a, *mechanics); break;
+            case 128: k_tadj_vertices<128><<<nv, 128, 0, s>>>(P, *surface, a, *mechanics); break;
+            default: k_tadj_vertices<32><<<nv, 32, 0, s>>>(P, *surface, a, *mechanics); break;
+        }
         if (int rc = check_launch("bk_transport_adjoint/vertices")) return rc;
     }
     k_tadj_clear<<<box_blocks, 256, 0, s>>>(P, g, box);

@@ -797,6 +797,14 @@ BK_DEV double gas_pressure(double moles, float T, float J, float n) {
     return moles * kGasConstant * (double)T / ((double)J * (double)n);
 }
 
+// Threads per vertex block for surface vertices with `bindings` particle bindings in total: a
+// block's worth of gathers in flight for vertices binding thousands of particles (large bodies),
+// one warp for vertices binding tens (small bodies, or an unknown count).
+inline int vertex_block_threads(int64_t vertices, int64_t bindings) {
+    const int64_t mean = vertices > 0 ? bindings / vertices : 0;
+    return mean >= 1024 ? 256 : (mean >= 128 ? 128 : 32);
+}
+
 // ------------------------------------------- geometry/mesh_tracking.py:13-38
 // One mesh vertex reconstructed by a whole block of kBlock threads: anchor + sum_b w_b (pred_b -
 // anchor) over its bindings b0..b1, pred_b = x_p + F_p o_b (o_b: the binding's reference offset,

@@ -176,10 +176,11 @@ __device__ __forceinline__ int64_t tile_node(const BlockBox& bb, int t, int R) {
 // ------------------------------------------------------------------ surface
 // geometry/mesh_tracking.py:13-38 restricted to the vertices of boundary faces; one block per
 // vertex (a vertex binds thousands of particles: a block keeps enough gathers in flight).
-__global__ void __launch_bounds__(kThreads) k_surface_vertices(Params P, const float* __restrict__ x,
-                                                             const float* __restrict__ F, BkSurface sf) {
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock) k_surface_vertices(Params P, const float* __restrict__ x,
+                                                          const float* __restrict__ F, BkSurface sf) {
     const int vid = sf.vertex_ids[blockIdx.x];
-    const float v = vertex_block<kThreads>(sf.binding_offsets, sf.binding_particles, sf.binding_weights,
+    const float v = vertex_block<kBlock>(sf.binding_offsets, sf.binding_particles, sf.binding_weights,
                                            sf.reference_offsets, sf.binding_pitch, sf.reference_vertices,
                                            sf.vertex_pitch, x, F, P.pitch, vid);
     if (threadIdx.x < 3) sf.vertices[threadIdx.x * sf.vertex_pitch + vid] = v;
@@ -1066,8 +1067,12 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
         if (surface->vertex_count > 0) {
             {
                 int rec = profile_begin("surface_vertices", s);
-                k_surface_vertices<<<(unsigned)surface->vertex_count, kThreads, 0, s>>>(P, in->x, in->F,
-                                                                                                   *surface);
+                const unsigned nv = (unsigned)surface->vertex_count;
+                switch (vertex_block_threads(surface->vertex_count, surface->binding_count)) {
+                    case 256: k_surface_vertices<256><<<nv, 256, 0, s>>>(P, in->x, in->F, *surface); break;
+                    case 128: k_surface_vertices<128><<<nv, 128, 0, s>>>(P, in->x, in->F, *surface); break;
+                    default: k_surface_vertices<32><<<nv, 32, 0, s>>>(P, in->x, in->F, *surface); break;
+                }
                 profile_end(rec, s);
             }
             if (int rc = check_launch("bk_substep/surface_vertices")) return rc;

@@ -39,7 +39,7 @@ class BkSurface(C.Structure):
                 ("binding_weights", P), ("binding_pitch", C.c_int64), ("reference_offsets", P),
                 ("vertex_pitch", C.c_int64), ("vertices", P), ("reference_vertices", P), ("owner_count", C.c_int64),
                 ("owners", P), ("owner_face_offsets", P), ("faces", P), ("owner_heat", P), ("owner_loss", P),
-                ("floor_height", C.c_float), ("contact_distance", C.c_float)]
+                ("floor_height", C.c_float), ("contact_distance", C.c_float), ("binding_count", C.c_int64)]
 
 
 class BkDiagnostics(C.Structure):
@@ -187,6 +187,7 @@ class SubstepEngine:
         ids = t["vertex_ids"].cpu().numpy()
         offs = mb.tables.binding_offsets
         self.surface_bindings = int((offs[ids + 1] - offs[ids]).sum())
+        sf.binding_count = self.surface_bindings
         self.owned_faces = int(len(faces))
         s = sim.simulation_config
         sf.floor_height = s.grid_origin[1] + (s.boundary_cells - 1) * s.grid_spacing

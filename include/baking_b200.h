@@ -232,6 +232,8 @@ typedef struct BkSurface {
     const int32_t *faces;          /* 3 vertex ids per face, grouped by owner */
     double *owner_heat, *owner_loss;   /* per owner, this substep */
     float floor_height, contact_distance;
+    int64_t binding_count;         /* total bindings of the vertex_ids vertices, a launch-size hint
+                                      (0: unknown, one warp per vertex) */
 } BkSurface;
 
 /* Optional full per-particle outputs of the reference kernels (NULL pointers are skipped). */
