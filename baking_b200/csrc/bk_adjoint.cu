@@ -4,8 +4,10 @@
 // t (node mass, momentum and velocity, recomputed by the caller from the checkpointed state t):
 //
 //   adj_g2p_return   per particle: recompute G2P and the return map, then pull the adjoints of
-//                    x', v', C', F', Fe', tau', porosity' back to x, F, Fe, porosity, temperature and
-//                    the material parameters; scatter the grid-velocity adjoint.
+//                    v', C', F', Fe', tau', porosity' back to F, Fe, porosity, temperature and the
+//                    material parameters, and form the v-bar, C-bar the G2P gather receives.
+//   adj_g2p_scatter  per particle: the weight-gradient terms of x; v-bar, C-bar scattered to the
+//                    grid-velocity adjoint through shared-memory tiles (the forward P2G's scheme).
 //   adj_grid         per node: velocity adjoint -> momentum and mass adjoints (walls clamp to zero).
 //   adj_p2g          per particle: gather the momentum/mass adjoints -> v, C, tau (and, for the
 //                    neo-Hookean model, F and mu, lambda) and the weight-gradient terms of x.
@@ -358,8 +360,7 @@ __device__ __forceinline__ float qweight_grad(float l, int o) {
 template <bool kCoupled>
 __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkState in, const float4* __restrict__ grid_v,
                                                           const float* __restrict__ eta_param, AdjState out_adj,
-                                                          AdjState in_adj, float4* __restrict__ grid_v_adj,
-                                                          double* __restrict__ params_adj) {
+                                                          AdjState in_adj, double* __restrict__ params_adj) {
     const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
     float acc_mu = 0.f, acc_lam = 0.f, acc_eta = 0.f;
     if (i < P.n) {
@@ -367,8 +368,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
         V3 xi = load_v3(in.x, i, pitch);
         Stencil st = make_stencil(xi, P.origin, P.dx, P.R);
         if (st.valid) {
-            // ---- forward recompute: G2P
-            float nv[3] = {0.f, 0.f, 0.f}, nc[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            // ---- forward recompute: G2P (C' only; v' does not enter the reverse sweep)
+            float nc[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             const float k4 = 4.0f / (P.dx * P.dx);
 #pragma unroll
             for (int ox = 0; ox < 3; ++ox)
@@ -381,11 +382,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                         float4 u = __ldg(grid_v + node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R));
                         float uu[3] = {u.x, u.y, u.z};
 #pragma unroll
-                        for (int r = 0; r < 3; ++r) {
-                            nv[r] += w * uu[r];
+                        for (int r = 0; r < 3; ++r)
 #pragma unroll
                             for (int c = 0; c < 3; ++c) nc[3 * r + c] += k4 * w * (uu[r] * d[c]);
-                        }
                     }
             M3 F = load_m3(in.F, i, pitch);
             M3 G;
@@ -583,8 +582,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                     porb_in = dpar[kA] * da;
                 }
             }
-            // ---- G2P backward
-            // x' = x + dt v'; F' = (I + dt C') F
+            // ---- G2P backward, per particle: x' = x + dt v'; F' = (I + dt C') F. The node scatter
+            // of v-bar and C-bar and the weight gradients of x follow in k_adj_g2p_scatter, which
+            // takes v-bar and C-bar from in_adj.v and in_adj.C (k_adj_p2g overwrites both later).
 #pragma unroll
             for (int r = 0; r < 3; ++r) vb[r] += P.dt * xb[r];
             float Fb_in[9];
@@ -601,46 +601,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                     Fb_in[3 * r + c] = fc;
                     Cb[3 * r + c] += P.dt * cc;
                 }
-            // v' = sum w v_i; C' = k sum w v_i d^T with d = x_i - x_p
-            float xg[3] = {xb[0], xb[1], xb[2]};
-            const float inv_dx = 1.f / P.dx;
 #pragma unroll
-            for (int ox = 0; ox < 3; ++ox)
+            for (int c = 0; c < 3; ++c) in_adj.v[c * pitch + i] = vb[c];
 #pragma unroll
-                for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-                    for (int oz = 0; oz < 3; ++oz) {
-                        const int o[3] = {ox, oy, oz};
-                        float wa[3] = {st.w[0][ox], st.w[1][oy], st.w[2][oz]};
-                        float w = wa[0] * wa[1] * wa[2];
-                        float d[3] = {((float)ox - st.l[0]) * P.dx, ((float)oy - st.l[1]) * P.dx, ((float)oz - st.l[2]) * P.dx};
-                        int64_t node = node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R);
-                        float4 u = __ldg(grid_v + node);
-                        float uu[3] = {u.x, u.y, u.z};
-                        // node velocity adjoint: w (vb + k Cb d)
-                        float nb[3];
-#pragma unroll
-                        for (int r = 0; r < 3; ++r)
-                            nb[r] = w * (vb[r] + k4 * (Cb[3 * r] * d[0] + Cb[3 * r + 1] * d[1] + Cb[3 * r + 2] * d[2]));
-                        atomicAdd(grid_v_adj + node, make_float4(nb[0], nb[1], nb[2], 0.f));
-                        // scalar s = vb . u + k u^T Cb d  (the weight's cofactor)
-                        float sdot = vb[0] * uu[0] + vb[1] * uu[1] + vb[2] * uu[2];
-                        float cu[3];
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) cu[c] = Cb[c] * uu[0] + Cb[3 + c] * uu[1] + Cb[6 + c] * uu[2];
-                        sdot += k4 * (cu[0] * d[0] + cu[1] * d[1] + cu[2] * d[2]);
-#pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            float dw = qweight_grad(st.l[a], o[a]) * inv_dx;
-                            float rest = 1.f;
-#pragma unroll
-                            for (int b2 = 0; b2 < 3; ++b2)
-                                if (b2 != a) rest *= wa[b2];
-                            xg[a] += dw * rest * sdot - k4 * w * cu[a];  // d = x_i - x_p: dd/dx_p = -I
-                        }
-                    }
-            store_v3(in_adj.x, i, pitch, V3{{xg[0], xg[1], xg[2]}});
-            // F, C (of state t) adjoints: F from G2P; C gets no direct dependence from G2P (C' does)
+            for (int e = 0; e < 9; ++e) in_adj.C[e * pitch + i] = Cb[e];
+            // F (of state t): from G2P; C gets no direct dependence from G2P (C' does)
             M3 fbm;
 #pragma unroll
             for (int e = 0; e < 9; ++e) fbm.m[e] = Fb_in[e];
@@ -654,9 +619,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                 in_adj.temperature[i] = Tb;
             }
         } else {
-            // The forward raised the stencil flag for this particle; its adjoint is zero.
-#pragma unroll
-            for (int c = 0; c < 3; ++c) in_adj.x[c * pitch + i] = 0.f;
+            // The forward raised the stencil flag for this particle; its adjoint is zero (x: in
+            // k_adj_g2p_scatter).
 #pragma unroll
             for (int c = 0; c < 9; ++c) in_adj.F[c * pitch + i] = 0.f;
             if (P.material == 1) {
@@ -671,6 +635,176 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
         block_accumulate(params_adj + 0, acc_mu);
         block_accumulate(params_adj + 1, acc_lam);
         block_accumulate(params_adj + 2, acc_eta);
+    }
+}
+
+// ------------------------------------------------------------ G2P scatter
+// The node-velocity adjoint of G2P (transfer.py:90-104 reversed): node j receives
+// w_j (v-bar + 4/dx^2 C-bar d_j) with d_j = (o_j - l) dx, i.e. w_j (q + A o_j) with
+// q = v-bar - (4/dx) C-bar l and A = (4/dx) C-bar -- the forward P2G's form, scattered the same
+// way: runs of particles with one stencil base within a warp, lane j < 27 summing node j over the
+// run, a shared-memory tile over the block's node box (when it fits kTileNodes) and one global
+// atomic per tile node. Each particle also gathers the weight gradients of x (reads only).
+constexpr int kTileNodes = 512;
+
+struct ScatterSmem {
+    float4 rec[kThreads][6];  // {wx0 wx1 wx2 -} {wy0 wy1 wy2 q0} {wz0 wz1 wz2 q1} {A0 A1 A2 q2} {A3 A4 A5 -} {A6 A7 A8 -}
+    float4 tile[kTileNodes];
+    int box[6];
+};
+
+__device__ __forceinline__ float pick3(const float4& v, int o) { return o == 0 ? v.x : (o == 1 ? v.y : v.z); }
+
+__global__ void __launch_bounds__(kThreads) k_adj_g2p_scatter(AdjParams P, BkState in, const float4* __restrict__ grid_v,
+                                                            AdjState out_adj, AdjState in_adj,
+                                                            float4* __restrict__ grid_v_adj) {
+    __shared__ ScatterSmem sm;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int64_t i = blockIdx.x * (int64_t)kThreads + tid;
+    const int64_t pitch = P.pitch;
+    Stencil st;
+    st.valid = false;
+    st.b[0] = st.b[1] = st.b[2] = 0;
+    if (i < P.n) st = make_stencil(load_v3(in.x, i, pitch), P.origin, P.dx, P.R);
+    const bool valid = i < P.n && st.valid;
+    float q[3] = {0.f, 0.f, 0.f}, A[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (valid) {
+        const float k4 = 4.0f / (P.dx * P.dx), inv_dx = 1.f / P.dx;
+        float vb[3], Cb[9], xg[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            vb[c] = in_adj.v[c * pitch + i];
+            xg[c] = out_adj.x[c * pitch + i];
+        }
+#pragma unroll
+        for (int e = 0; e < 9; ++e) Cb[e] = in_adj.C[e * pitch + i];
+#pragma unroll
+        for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+            for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                for (int oz = 0; oz < 3; ++oz) {
+                    const int o[3] = {ox, oy, oz};
+                    const float wa[3] = {st.w[0][ox], st.w[1][oy], st.w[2][oz]};
+                    const float w = wa[0] * wa[1] * wa[2];
+                    const float d[3] = {((float)ox - st.l[0]) * P.dx, ((float)oy - st.l[1]) * P.dx,
+                                        ((float)oz - st.l[2]) * P.dx};
+                    const float4 u = __ldg(grid_v + node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R));
+                    const float uu[3] = {u.x, u.y, u.z};
+                    // the weight's cofactor s = vb . u + k u^T Cb d
+                    float sdot = vb[0] * uu[0] + vb[1] * uu[1] + vb[2] * uu[2];
+                    float cu[3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) cu[c] = Cb[c] * uu[0] + Cb[3 + c] * uu[1] + Cb[6 + c] * uu[2];
+                    sdot += k4 * (cu[0] * d[0] + cu[1] * d[1] + cu[2] * d[2]);
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const float dw = qweight_grad(st.l[a], o[a]) * inv_dx;
+                        float rest = 1.f;
+#pragma unroll
+                        for (int b2 = 0; b2 < 3; ++b2)
+                            if (b2 != a) rest *= wa[b2];
+                        xg[a] += dw * rest * sdot - k4 * w * cu[a];  // d = x_i - x_p: dd/dx_p = -I
+                    }
+                }
+        store_v3(in_adj.x, i, pitch, V3{{xg[0], xg[1], xg[2]}});
+        const float kd = k4 * P.dx;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+            q[r] = vb[r] - kd * (Cb[3 * r] * st.l[0] + Cb[3 * r + 1] * st.l[1] + Cb[3 * r + 2] * st.l[2]);
+#pragma unroll
+        for (int e = 0; e < 9; ++e) A[e] = kd * Cb[e];
+    } else if (i < P.n) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) in_adj.x[c * pitch + i] = 0.f;
+    }
+    {
+        float w[3][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int o = 0; o < 3; ++o) w[a][o] = valid ? st.w[a][o] : 0.f;
+        sm.rec[tid][0] = make_float4(w[0][0], w[0][1], w[0][2], 0.f);
+        sm.rec[tid][1] = make_float4(w[1][0], w[1][1], w[1][2], q[0]);
+        sm.rec[tid][2] = make_float4(w[2][0], w[2][1], w[2][2], q[1]);
+        sm.rec[tid][3] = make_float4(A[0], A[1], A[2], q[2]);
+        sm.rec[tid][4] = make_float4(A[3], A[4], A[5], 0.f);
+        sm.rec[tid][5] = make_float4(A[6], A[7], A[8], 0.f);
+    }
+    if (tid < 6) sm.box[tid] = tid < 3 ? INT_MAX : INT_MIN;
+    __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int lo = __reduce_min_sync(0xffffffffu, valid ? st.b[a] : INT_MAX);
+        const int hi = __reduce_max_sync(0xffffffffu, valid ? st.b[a] + 2 : INT_MIN);
+        if (lane == 0 && lo != INT_MAX) {
+            atomicMin(&sm.box[a], lo);
+            atomicMax(&sm.box[3 + a], hi);
+        }
+    }
+    __syncthreads();
+    int lo[3] = {0, 0, 0}, ext[3] = {1, 1, 1};
+    int count = 0;
+    bool tiled = false;
+    if (sm.box[0] != INT_MAX) {
+        long long c = 1;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = sm.box[a];
+            ext[a] = sm.box[3 + a] - sm.box[a] + 1;
+            c *= ext[a];
+        }
+        tiled = c <= kTileNodes;
+        count = tiled ? (int)c : 0;
+    }
+    for (int t = tid; t < count; t += kThreads) sm.tile[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
+    const long long key = valid ? (((long long)st.b[0] << 42) | ((long long)st.b[1] << 21) | (long long)st.b[2]) : -1;
+    const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
+    unsigned starts = __ballot_sync(0xffffffffu, valid && (lane == 0 || prev != key));
+    const int warp_base = tid & ~31;
+    const int ox = (lane < 27 ? lane : 0) / 9, oy = ((lane < 27 ? lane : 0) / 3) % 3, oz = (lane < 27 ? lane : 0) % 3;
+    const float fo[3] = {(float)ox, (float)oy, (float)oz};
+    while (starts) {
+        const int s0 = __ffs(starts) - 1;
+        starts &= starts - 1;
+        const int e = starts ? __ffs(starts) - 1 : 32;
+        const int b0 = __shfl_sync(0xffffffffu, st.b[0], s0), b1 = __shfl_sync(0xffffffffu, st.b[1], s0),
+                  b2 = __shfl_sync(0xffffffffu, st.b[2], s0);
+        if (lane < 27) {
+            float aq[3] = {0.f, 0.f, 0.f}, aA[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll 2
+            for (int k = warp_base + s0; k < warp_base + e; ++k) {
+                const float4 r0 = sm.rec[k][0], r1 = sm.rec[k][1], r2 = sm.rec[k][2];
+                const float4 r3 = sm.rec[k][3], r4 = sm.rec[k][4], r5 = sm.rec[k][5];
+                const float w = pick3(r0, ox) * pick3(r1, oy) * pick3(r2, oz);
+                aq[0] += w * r1.w;
+                aq[1] += w * r2.w;
+                aq[2] += w * r3.w;
+                aA[0] += w * r3.x; aA[1] += w * r3.y; aA[2] += w * r3.z;
+                aA[3] += w * r4.x; aA[4] += w * r4.y; aA[5] += w * r4.z;
+                aA[6] += w * r5.x; aA[7] += w * r5.y; aA[8] += w * r5.z;
+            }
+            float ap[3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) ap[r] = aq[r] + (aA[3 * r] * fo[0] + aA[3 * r + 1] * fo[1] + aA[3 * r + 2] * fo[2]);
+            if (tiled) {
+                float* cell = reinterpret_cast<float*>(
+                    &sm.tile[((b0 + ox - lo[0]) * ext[1] + (b1 + oy - lo[1])) * ext[2] + (b2 + oz - lo[2])]);
+                atomicAdd(cell + 0, ap[0]);
+                atomicAdd(cell + 1, ap[1]);
+                atomicAdd(cell + 2, ap[2]);
+            } else {
+                atomicAdd(grid_v_adj + node_index(b0 + ox, b1 + oy, b2 + oz, P.R), make_float4(ap[0], ap[1], ap[2], 0.f));
+            }
+        }
+    }
+    __syncthreads();
+    for (int t = tid; t < count; t += kThreads) {
+        const float4 v = sm.tile[t];
+        if (v.x == 0.f && v.y == 0.f && v.z == 0.f) continue;
+        const int z = t % ext[2], y = (t / ext[2]) % ext[1], x = t / (ext[2] * ext[1]);
+        atomicAdd(grid_v_adj + node_index(lo[0] + x, lo[1] + y, lo[2] + z, P.R), v);
     }
 }
 
@@ -927,14 +1061,16 @@ int bk_substep_adjoint(const BkSubstepParams* params, const BkState* in, const B
     if (p.material == 1 && p.ding.coupled_porosity)
         k_adj_g2p_return<true><<<blocks, kThreads, 0, s>>>(a, *in, reinterpret_cast<const float4*>(node_v),
                                                          constants->viscosity_parameter, adj_state(*out_adjoint),
-                                                         adj_state(*in_adjoint), reinterpret_cast<float4*>(node_v_adjoint),
-                                                         parameter_adjoint);
+                                                         adj_state(*in_adjoint), parameter_adjoint);
     else
         k_adj_g2p_return<false><<<blocks, kThreads, 0, s>>>(a, *in, reinterpret_cast<const float4*>(node_v),
                                                           constants->viscosity_parameter, adj_state(*out_adjoint),
-                                                          adj_state(*in_adjoint), reinterpret_cast<float4*>(node_v_adjoint),
-                                                          parameter_adjoint);
+                                                          adj_state(*in_adjoint), parameter_adjoint);
     if (int rc = bk::check_launch("bk_substep_adjoint/g2p_return")) return rc;
+    k_adj_g2p_scatter<<<blocks, kThreads, 0, s>>>(a, *in, reinterpret_cast<const float4*>(node_v),
+                                                  adj_state(*out_adjoint), adj_state(*in_adjoint),
+                                                  reinterpret_cast<float4*>(node_v_adjoint));
+    if (int rc = bk::check_launch("bk_substep_adjoint/g2p_scatter")) return rc;
     if (node_box) {
         int device = 0, sms = 148;
         cudaGetDevice(&device);
