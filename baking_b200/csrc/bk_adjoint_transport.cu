@@ -178,15 +178,26 @@ __global__ void __launch_bounds__(kThreads) k_tadj_scalar(TParams P, BkState in,
         a.water_in[i] = 0.0;
         if (P.gas) a.gas_moles_in[i] = 0.0;
     } else if (valid) {
+        // one pass over the stencil: T' and W' need sum w (dT, r); the weight gradients of x need
+        // sum grad w (dT, r), which do not depend on the adjoints
         double dTp = 0.0, ratio = 0.0;
+        float gT[3] = {0.f, 0.f, 0.f}, gr[3] = {0.f, 0.f, 0.f};
+        const float inv_dx = 1.f / P.dx;
 #pragma unroll
         for (int j = 0; j < 27; ++j) {
             int ox, oy, oz;
             node_offset(j, ox, oy, oz);
-            const double w = (double)(st.w[0][ox] * st.w[1][oy] * st.w[2][oz]);
+            float dw[3];
+            const double w = (double)weight_and_grad(st, ox, oy, oz, inv_dx, dw);
             const double2 d = dTr[node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R)];
             dTp += w * d.x;
             ratio += w * d.y;
+            const float fx = (float)d.x, fy = (float)d.y;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                gT[c] += dw[c] * fx;
+                gr[c] += dw[c] * fy;
+            }
         }
         const double T = in.temperature[i], Tn = T + dTp;
         const double W = in.water[i];
@@ -237,21 +248,9 @@ __global__ void __launch_bounds__(kThreads) k_tadj_scalar(TParams P, BkState in,
         a.water_in[i] = Wnb * (1.0 + ratio);
         a.temperature_in[i] = Tnb + Tb_direct;
         // weight gradients: x_bar += sum_j grad w_j (dT_j T'_bar + r_j ratio_bar)
-        const float inv_dx = 1.f / P.dx;
-        float xg[3] = {0.f, 0.f, 0.f};
-#pragma unroll 1
-        for (int j = 0; j < 27; ++j) {
-            int ox, oy, oz;
-            node_offset(j, ox, oy, oz);
-            float dw[3];
-            weight_and_grad(st, ox, oy, oz, inv_dx, dw);
-            const double2 d = dTr[node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R)];
-            const float s = (float)(d.x * Tnb + d.y * ratiob);
+        const float tb = (float)Tnb, rb = (float)ratiob;
 #pragma unroll
-            for (int c = 0; c < 3; ++c) xg[c] += dw[c] * s;
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c) adj.x[c * pitch + i] += xg[c];
+        for (int c = 0; c < 3; ++c) adj.x[c * pitch + i] += gT[c] * tb + gr[c] * rb;
         add_det_grad(adj.F, i, pitch, F, (float)Jb);
     }
     // ---- scatter w (T'_bar, ratio_bar) into the node adjoints

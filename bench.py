@@ -408,11 +408,21 @@ def rollout_variant(sim, dist, stream, world, scene, fb_steps=64, every=8):
     fwd_bwd()  # warm-up: first-call set-up of the reverse-mode buffers and kernels
     for t in (T0, rates, E0):
         t.grad = None
-    t_fb, _ = _timed(fwd_bwd, dist, stream)
+    repeats = 3  # forward + backward rollouts timed back to back (one alone varies by ~20% between runs)
+
+    def rollouts():
+        for _ in range(repeats):
+            for t in (T0, rates, E0):
+                t.grad = None
+            fwd_bwd()
+
+    t_fb, _ = _timed(rollouts, dist, stream)
+    t_fb /= repeats
     t_f, _ = _timed(lambda: sim.AdvanceUnchecked(fb_steps), dist, stream)
     finite = all(bool(torch.isfinite(t.grad).all()) for t in (T0, rates, E0))
     out = {"value": world * n * fb_steps / t_fb, "unit": UNIT, "forward_only": world * n * fb_steps / t_f,
            "ms_per_substep": 1e3 * t_fb / fb_steps, "steps": fb_steps, "checkpoint_every": every,
+           "rollouts_timed": repeats,
            "gradients": ["transport_temperatures", "gas_source_rates", "young_modulus"],
            "finite_gradients": finite, "scene": scene}
     del sim
