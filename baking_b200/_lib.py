@@ -58,6 +58,7 @@ SIGNATURES = {
     "bk_porosity_coefficient": [I64, P, P, P],
     "bk_profile_start": [],
     "bk_profile_stop": [],
+    "bk_profile_select": [C.c_char_p],
     "bk_profile_report": [I32, P, I32, P, P, P],
 }
 
@@ -111,20 +112,31 @@ def require_cuda(device=None):
 
 class KernelTimer:
     """Per-kernel CUDA-event timing while active: the library's own events around every launch
-    inside the fused entry points, plus host-side events around each other C-ABI call."""
+    inside the fused entry points, plus host-side events around each other C-ABI call. ``only``
+    restricts the events to one kernel name (every event pair costs the stream a few microseconds)."""
 
     active = None
+
+    def __init__(self, only=None):
+        self.only = only
+        self.events = {}
 
     def __enter__(self):
         self.events = {}
         lib = load()
         lib.bk_profile_start()
+        lib.bk_profile_select(self.only.encode() if self.only else None)
         KernelTimer.active = self
         return self
 
     def __exit__(self, *exc):
         KernelTimer.active = None
-        load().bk_profile_stop()
+        lib = load()
+        lib.bk_profile_stop()
+        lib.bk_profile_select(None)
+
+    def wants(self, name):
+        return self.only is None or name == self.only
 
     def add(self, name, start, end):
         if name.startswith("bk_substep"):
@@ -156,7 +168,7 @@ def call(name, *args):
     """Call one C-ABI entry point; raise RuntimeError on a nonzero status."""
     lib = load()
     timer = KernelTimer.active
-    if timer is not None:
+    if timer is not None and timer.wants(name):
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
         rc = getattr(lib, name)(*args)
@@ -172,7 +184,7 @@ def call(name, *args):
 def call_raw(fn, name, *args):
     """Call an already-declared C-ABI function object (timed like ``call``); raise on failure."""
     timer = KernelTimer.active
-    if timer is not None:
+    if timer is not None and timer.wants(name):
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
         rc = fn(*args)

@@ -17,6 +17,7 @@ struct Record {
 
 std::mutex g_mutex;
 bool g_enabled = false;
+std::string g_only;  // when not empty, only the kernel of this name is recorded
 std::vector<std::string> g_names;
 std::vector<Record> g_records;
 std::vector<cudaEvent_t> g_free;
@@ -37,6 +38,7 @@ cudaEvent_t take_event() {
 int bk::profile_begin(const char* name, cudaStream_t stream) {
     if (!g_enabled) return -1;
     std::lock_guard<std::mutex> lock(g_mutex);
+    if (!g_only.empty() && g_only != name) return -1;
     int id = -1;
     for (size_t k = 0; k < g_names.size(); ++k)
         if (g_names[k] == name) id = (int)k;
@@ -68,6 +70,12 @@ int bk_profile_start(void) {
     g_records.clear();
     g_names.clear();
     g_enabled = true;
+    return BK_OK;
+}
+
+int bk_profile_select(const char* name) {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    g_only = name ? name : "";
     return BK_OK;
 }
 

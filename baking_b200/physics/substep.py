@@ -278,17 +278,11 @@ class SubstepEngine:
             diag.plastic_gradients = _p(m.plastic_gradients)
             diag.return_residuals = _p(m.return_residuals)
             diag.porosity_residuals = _p(m.porosity_residuals)
-        timer = _lib.KernelTimer.active
+        # (under a KernelTimer the library times bk_substep's kernels one by one)
         stream = _lib.stream_handle()
-        if timer is not None:
-            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            start.record()
         rc = self.lib.bk_substep(C.byref(p), C.byref(sin), C.byref(sout), C.byref(cst),
                                  C.byref(self.grid if grid is None else grid),
                                  C.byref(self.surface), C.byref(diag), C.byref(self.flags), int(phases), stream)
-        if timer is not None:
-            end.record()
-            timer.add(f"bk_substep[{phases}]", start, end)
         if rc != 0:
             raise RuntimeError(f"bk_substep failed ({rc}): {self.lib.bk_last_error().decode(errors='replace')}")
 

@@ -320,6 +320,9 @@ BK_API int bk_substep_static_grid(const BkSubstepParams *params, const BkState *
    the total milliseconds and launch count. */
 BK_API int bk_profile_start(void);
 BK_API int bk_profile_stop(void);
+/* Record only the kernel named `name` (NULL or "": every kernel). Each recorded launch adds two
+   event records to its stream, a few microseconds between kernels. */
+BK_API int bk_profile_select(const char *name);
 BK_API int bk_profile_report(int32_t max_kernels, char *names, int32_t name_capacity, double *total_ms,
                              int32_t *counts, int32_t *kernel_count);
 
