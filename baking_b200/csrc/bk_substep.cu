@@ -2,9 +2,10 @@
 //
 // The reference runs ~16 Warp launches per substep (physics/mpm.py:163-225,
 // physics/thermal_water.py:296-367) with three host synchronisations and fresh
-// dense-grid allocations. Here one substep is seven launches:
+// dense-grid allocations. Here one substep is eight launches (nine with clear_previous):
 //
-//   surface_vertices   rebuild only the boundary-face vertices (warp per vertex)
+//   surface_vertices   rebuild only the boundary-face vertices (a block of 32-256 threads per
+//                      vertex, sized by its mean particle bindings)
 //   surface_owners     face areas -> boundary heat/loss/exchange of face-owning particles, scattered
 //   transport_scatter  scalar P2G (volume, capacity, energy, water), warp-cooperative per stencil base
 //   diffuse            7-point finite-volume heat/water flux over the active node box only
