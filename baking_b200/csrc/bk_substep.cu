@@ -2,7 +2,8 @@
 //
 // The reference runs ~16 Warp launches per substep (physics/mpm.py:163-225,
 // physics/thermal_water.py:296-367) with three host synchronisations and fresh
-// dense-grid allocations. Here one substep is eight launches (nine with clear_previous):
+// dense-grid allocations. Here one substep is eight launches, clear_previous (which zeroes the last
+// substep's momentum box) and these seven:
 //
 //   surface_vertices   rebuild only the boundary-face vertices (a block of 32-256 threads per
 //                      vertex, sized by its mean particle bindings)
