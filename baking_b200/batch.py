@@ -85,6 +85,45 @@ class BatchedSimulators:
         return [sim.CheckState() for sim in self.sims]
 
 
+class _MappedDoubles:
+    """float64 slots in pinned host memory mapped into the device address space (cudaHostAlloc
+    with cudaHostAllocMapped): kernels store through ``device_ptr``, the host reads ``view``."""
+
+    def __init__(self, count):
+        import ctypes
+        import numpy as np
+        from cuda.bindings import runtime as cudart
+        self._cudart = cudart
+        err, self._host_ptr = cudart.cudaHostAlloc(8 * count, cudart.cudaHostAllocMapped)
+        if err != cudart.cudaError_t.cudaSuccess:
+            raise RuntimeError(f"cudaHostAlloc failed: {err}")
+        err, self.device_ptr = cudart.cudaHostGetDevicePointer(self._host_ptr, 0)
+        if err != cudart.cudaError_t.cudaSuccess:
+            cudart.cudaFreeHost(self._host_ptr)
+            raise RuntimeError(f"cudaHostGetDevicePointer failed: {err}")
+        self.view = np.ctypeslib.as_array((ctypes.c_double * count).from_address(self._host_ptr))
+        self.view[:] = 0.0
+
+    def __del__(self):
+        if getattr(self, "_host_ptr", None):
+            self._cudart.cudaFreeHost(self._host_ptr)
+            self._host_ptr = None
+
+
+class StepResult:
+    """One substep's (grid mass, kinetic energy), written by its graph into mapped host memory."""
+
+    def __init__(self, event, view):
+        self.event = event
+        self.view = view
+
+    def get(self):
+        """Wait for the substep, then read its two values on the host (no copy is issued). The
+        slot is rewritten by the substep two later: read it before launching that one."""
+        self.event.synchronize()
+        return [float(self.view[0]), float(self.view[1])]
+
+
 class SubstepGraphs:
     """One simulator's substep as two captured CUDA graphs, state A -> B and B -> A, each followed
     by the step-result reduction (``MpmSimulator.StepSummary``): ``Advance(1)`` is one graph launch.
@@ -94,17 +133,23 @@ class SubstepGraphs:
     ``inputs``: device tensors the caller refills before every substep (per-particle gas source
     rates, say). Each graph starts by copying them from a staging buffer of its own, so ``load``
     can upload the inputs of the substep after the next one from pinned host memory, on a copy
-    stream, while the next one runs. The graphs hold the simulator's arrays and parameters at
-    capture time: refill parameter tensors in place between steps, and capture again after
-    replacing one."""
+    stream, while the next one runs. ``host_results``: the two graphs write their step results
+    into two slots of mapped pinned host memory (the reduction's last kernel stores them there, no
+    copy is queued), and ``Advance`` returns a ``StepResult`` for the slot, so a caller can read
+    one substep's result while the next one runs. The graphs hold the simulator's arrays and
+    parameters at capture time: refill parameter tensors in place between steps, and capture again
+    after replacing one."""
 
-    def __init__(self, sim, inputs=()):
+    def __init__(self, sim, inputs=(), host_results=False):
         if sim.IsSettling:
             raise ValueError("captured substeps start after settling (settling_duration_s = 0)")
         if sim.retain_history:
             raise ValueError("captured substeps keep no history")
         self.sim = sim
         self.summary = torch.zeros(2, dtype=torch.float64, device=sim.device)
+        self._host = None
+        if host_results:
+            self._host = _MappedDoubles(4)
         self.inputs = list(inputs)
         self.staging = [[torch.empty_like(t) for t in self.inputs] for _ in range(2)]
         self.loaded = [None, None]     # events: staging set k filled
@@ -116,7 +161,10 @@ class SubstepGraphs:
         for t, staged in zip(self.inputs, self.staging[parity]):
             t.copy_(staged)
         BatchedSimulators._substep(self.sim, state_in, state_out)
-        self.sim._engine.step_summary(state_out, self.summary)
+        if self._host is not None:
+            self.sim._engine.step_summary(state_out, out_ptr=self._host.device_ptr + 16 * parity)
+        else:
+            self.sim._engine.step_summary(state_out, self.summary)
 
     def _parity(self, ahead=0):
         """Staging set read by the substep ``ahead`` substeps after the next one."""
@@ -161,8 +209,8 @@ class SubstepGraphs:
         self.loaded[parity] = event
 
     def Advance(self, steps=1):
-        """Advance by ``steps`` substeps; returns the device tensor (grid mass, kinetic energy) of
-        the last one."""
+        """Advance by ``steps`` substeps. Returns the last one's (grid mass, kinetic energy): a
+        device tensor, or with ``host_results`` a ``StepResult``."""
         if self.graphs is None:
             self.capture()
         sim = self.sim
@@ -179,7 +227,9 @@ class SubstepGraphs:
             sim.next_state, sim._current = sim._current, nxt
             sim.step_count += 1
             sim._stale = True
-        return self.summary
+            if self._host is not None:
+                result = StepResult(done, self._host.view[2 * parity:2 * parity + 2])
+        return result if self._host is not None and steps > 0 else self.summary
 
 
 def _state_tensors(sim):

@@ -286,10 +286,11 @@ class SubstepEngine:
         if rc != 0:
             raise RuntimeError(f"bk_substep failed ({rc}): {self.lib.bk_last_error().decode(errors='replace')}")
 
-    def step_summary(self, state, out=None):
-        """(grid mass of the last substep, kinetic energy of ``state``) as a float64 device tensor."""
+    def step_summary(self, state, out=None, out_ptr=None):
+        """(grid mass of the last substep, kinetic energy of ``state``) as a float64 device tensor,
+        or into the 2 doubles at device address ``out_ptr``."""
         dev = self.sim.device
-        if out is None:
+        if out is None and out_ptr is None:
             out = torch.empty(2, dtype=torch.float64, device=dev)
         if getattr(self, "_summary_scratch", None) is None:
             self._summary_scratch = torch.empty(2 * 296, dtype=torch.float64, device=dev)
@@ -297,7 +298,8 @@ class SubstepEngine:
         cst = self.constants(False)
         s = state_struct(state, self.is_ding, self.transport, self.gas)
         _lib.call_raw(self.lib.bk_step_summary, "bk_step_summary", C.byref(p), C.byref(s), C.byref(cst),
-                      C.byref(self.grid), out.data_ptr(), self._summary_scratch.data_ptr(), _lib.stream_handle())
+                      C.byref(self.grid), out.data_ptr() if out_ptr is None else out_ptr,
+                      self._summary_scratch.data_ptr(), _lib.stream_handle())
         return out
 
     def accumulate_surface(self, transport_state):

@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -266,11 +267,12 @@ def main():
     # End to end through the public API: pinned host inputs (the per-particle gas source rates) uploaded
     # for every substep, the substep (SubstepGraphs: one graph launch per substep, with the step-result
     # reduction), and the step's result (grid mass, kinetic energy) read back to the host. Each
-    # substep's upload runs on a copy stream while the substep before it computes.
+    # substep's upload runs on a copy stream while the substep before it computes; each result lands
+    # in mapped host memory and is read while the next substep computes.
     from baking_b200.batch import SubstepGraphs
     host_rates = torch.from_numpy(scene.gas_source_rates).pin_memory()
     e2e_steps = max(1, min(args.steps, 100))
-    stepper = SubstepGraphs(sim, inputs=[sim.material.production_parameter]).capture()
+    stepper = SubstepGraphs(sim, inputs=[sim.material.production_parameter], host_results=True).capture()
     copy_stream = torch.cuda.Stream()
     torch.cuda.synchronize()
     if dist:
@@ -279,12 +281,20 @@ def main():
     e1 = torch.cuda.Event(enable_timing=True)
     wall0 = time.perf_counter()
     e0.record(stream)
+    results = []
+    pending = None
     stepper.load([host_rates], 0, copy_stream)
     for k in range(e2e_steps):
-        out = stepper.Advance(1)
+        step = stepper.Advance(1)
         if k + 1 < e2e_steps:
             stepper.load([host_rates], 0, copy_stream)  # the next substep's inputs, during this one
-        result = out.cpu()
+        if pending is not None:
+            results.append(pending.get())  # the previous substep's result, during this one
+        pending = step
+    results.append(pending.get())
+    result = results[-1]
+    if len(results) != e2e_steps or not all(math.isfinite(v) for r in results for v in r):
+        raise RuntimeError("end-to-end loop lost or corrupted a step result")
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_elapsed = max(e0.elapsed_time(e1) / 1e3, time.perf_counter() - wall0)

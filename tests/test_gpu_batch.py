@@ -100,3 +100,26 @@ def test_substep_graphs_staged_inputs():
     torch.testing.assert_close(rates, some.to(rates.device))
     del stepper
     torch.cuda.synchronize()
+
+
+def test_substep_graphs_host_results():
+    """Results written by the graphs into mapped host memory match StepSummary, substep by substep,
+    read one substep behind while the next one runs."""
+    import torch
+    from baking_b200 import scenes
+    from baking_b200.batch import SubstepGraphs
+    sc = scenes.dough_ball(32, 8_000, seed=4)
+    sim = scenes.make_simulator(sc, diagnostics="lean")
+    stepper = SubstepGraphs(sim, host_results=True).capture()
+    pending, got, expected = None, [], []
+    for _ in range(4):
+        step = stepper.Advance(1)
+        torch.cuda.current_stream().synchronize()
+        expected.append(sim.StepSummary().cpu().numpy().tolist())
+        if pending is not None:
+            got.append(pending.get())
+        pending = step
+    got.append(pending.get())
+    np.testing.assert_allclose(np.array(got), np.array(expected), rtol=1e-12)
+    del stepper
+    torch.cuda.synchronize()
