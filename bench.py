@@ -250,10 +250,7 @@ def main():
             end.record(stream)
         torch.cuda.synchronize()
     elapsed = start.elapsed_time(end) / 1e3
-    if dist:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = reduce_max(elapsed, dist)
     sim.CheckState()
     timed_kernels = kernel_events.summary()
     breakdown_steps = max(1, min(args.steps, 50))
@@ -298,10 +295,7 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_elapsed = max(e0.elapsed_time(e1) / 1e3, time.perf_counter() - wall0)
-    if dist:
-        t = torch.tensor([e2e_elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_elapsed = float(t.item())
+    e2e_elapsed = reduce_max(e2e_elapsed, dist)
     del result, stepper
 
     peak, peak_kind = load_peaks()
@@ -352,6 +346,18 @@ def result_bytes():
     return 2 * 8
 
 
+def reduce_max(value, dist):
+    """The maximum of ``value`` over the ranks of the process group (``dist``, or None for one
+    process): on the GPU under NCCL, on the host under gloo."""
+    if not dist:
+        return value
+    import torch
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _timed(fn, dist, stream):
     """Device time of fn() between CUDA events on the launching stream, max over ranks."""
     import torch
@@ -363,12 +369,7 @@ def _timed(fn, dist, stream):
     out = fn()
     b.record(stream)
     torch.cuda.synchronize()
-    t = a.elapsed_time(b) / 1e3
-    if dist:
-        tt = torch.tensor([t], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
-    return t, out
+    return reduce_max(a.elapsed_time(b) / 1e3, dist), out
 
 
 def batched(args, rank, dist, net, count=64, steps=200):
