@@ -34,9 +34,12 @@ sys.path.insert(0, str(ROOT))
 METRIC = "particle-substeps/s at 1M particles (plain vs surrogate vs fwd+bwd) on 1 B200"
 UNIT = "particle-substeps/s"
 
-# Algorithmic HBM bytes: every required per-particle state array read once and
-# written once per substep at its stored precision (gas mode), plus the grid
-# traffic of each active node. Derivation in DESIGN.md.
+# Algorithmic HBM bytes of one substep (gas mode), every required state array read once and
+# written once at the reference's dtypes; derivable constants (masses, capacities) count 0.
+# Per particle: reads x, v 12 each, C, F, Fe, tau 36 each, porosity, gelled 4 each, temperature,
+# water, gas moles 8 each, V0 4 = 204 B; writes the same less V0 = 200 B. Per active node:
+# mechanics 56 (momentum/mass write+read 32, velocity write+read 24) plus transport 176 (seven
+# float64 scattered fields write+read 112, node temperature/saturation 32, dT/dW 32).
 BYTES_PER_PARTICLE = 404
 BYTES_PER_ACTIVE_NODE = 232
 
