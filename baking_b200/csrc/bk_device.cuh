@@ -562,12 +562,29 @@ BK_DEV float solve_porosity_bisection(float q, float p, float d, float h, float 
 // is resolved to ~1e-14 relative, far below the float32 rounding of the returned porosity.
 // Each evaluation's overstress root starts from the previous one (`warm`, which also returns the
 // last root to the caller); the roots are the reference's to its |residual| < 1e-12 test.
+//
+// The elastic early exit (q + a(trial) p <= 1) is first decided in float32 where that is certain:
+// a float32 a(n) is within 1e-6 (2/ln(1/n) + 1) relative of the float64 one, so when
+// q + a p <= 1 - 4e-6 (2/ln(1/n) + 1) a p the float64 test passes as well, both at the float64
+// trial and at its float32 rounding (which moves ln n by at most 2^-24). `elastic_exit` (may be
+// NULL) reports that certain case; there prediction(float(trial)) has no overstress and equals
+// trial, so the caller can skip that evaluation. Every other case takes the float64 test.
 BK_DEV float solve_porosity(float q, float p, float d, float h, float e, double Vp, float n0,
-                            double* warm = nullptr) {
+                            double* warm = nullptr, bool* elastic_exit = nullptr) {
     double r_local = 0.0;
     if (!warm) warm = &r_local;
+    if (elastic_exit) *elastic_exit = false;
     double trial = Vp - 1.0 + (double)n0;
     if (trial > 0.0 && trial < 1.0) {
+        const float nf = (float)trial;
+        const float lgf = logf(1.0f / nf);
+        const float af = 9.0f / (4.0f * (lgf * lgf) * (3.5f * nf + 1.0f));
+        const double ap = (double)af * (double)p;
+        const double bound = 4.0e-6 * (2.0 / (double)lgf + 1.0) * ap;
+        if (nf >= 1.0e-30f && lgf > 0.0f && (double)q + ap <= 1.0 - bound) {
+            if (elastic_exit) *elastic_exit = true;
+            return nf;
+        }
         double a = pressure_coefficient64(trial);
         if ((double)q + a * (double)p <= 1.0) return (float)trial;
     }
@@ -759,8 +776,11 @@ BK_DEV void ding_exact(const DingParamsDev& P, const DingPrelude& d, float por, 
         float ms = 2.0f / 3.0f * (2.0f * mu + 3.0f * lam) * dt * ty * ty / eta;
         float ex = 3.0f * mean / (2.0f * mu + 3.0f * lam);
         double Vp = 1.0 - (double)n0 + (double)por;
-        ret_por = solve_porosity(qv, pv, df, ms, ex, Vp, n0, &r_warm);
-        double pred = porosity_prediction((double)ret_por, qv, pv, df, ms, ex, Vp, n0, &r_warm);
+        bool elastic_exit;
+        ret_por = solve_porosity(qv, pv, df, ms, ex, Vp, n0, &r_warm, &elastic_exit);
+        // Certain elastic exit: prediction(ret_por) has r = 0 and returns Vp - 1 + n0 exactly.
+        double pred = elastic_exit ? Vp - 1.0 + (double)n0
+                                   : porosity_prediction((double)ret_por, qv, pv, df, ms, ex, Vp, n0, &r_warm);
         consistency = (float)fabs((double)ret_por - pred);
         if (consistency > 1.0e-6f || ret_por <= 0.0f || ret_por >= 1.0f) set_flag(flags, 1);
     }

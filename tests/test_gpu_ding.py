@@ -110,3 +110,42 @@ def test_porosity_solve_matches_reference_bisection():
     got, pred = SolvePorosity([4.115], [29.464], [0.001052], [0.003390], [-0.0230067], [1 - 0.2 + fr], 0.2)
     assert 0 < float(got[0]) < fr
     np.testing.assert_allclose(float(got[0]), float(pred[0]), atol=1e-12)
+
+
+def test_porosity_solve_elastic_exit_at_the_yield_margin():
+    """The elastic early exit (q + a(trial) p <= 1), decided in float32 where that is certain and
+    in float64 otherwise, against the oracle's float64 test on cases placed within 2e-5 relative
+    of the margin, porosities from 1e-12 to 1 - 1e-7: where the reference exits elastically the
+    same float32 porosity bit for bit, elsewhere within its rounding, and the prediction at it equal
+    to the oracle's."""
+    from baking_b200.physics.materials.porous_return import SolvePorosity
+    rng = np.random.default_rng(7)
+    m = 1000
+    n0 = 0.2
+    por = np.concatenate([rng.uniform(1e-6, 1 - 1e-7, m), 10 ** rng.uniform(-12, -1, m),
+                          1 - 10 ** rng.uniform(-7, -1, m)])
+    n0f = float(np.float32(n0))  # the solver takes n0 as float32
+    Vp = 1.0 - n0f + por
+    trial = Vp - 1.0 + n0f  # the elastic prediction as the solver forms it
+    assert np.all((trial > 0) & (trial < 1))
+    lg = np.log(1.0 / trial)
+    a = 9.0 / (4.0 * lg * lg * (3.5 * trial + 1.0))
+    p = rng.uniform(0.0, 1.0, trial.size).astype(np.float32)
+    k = np.concatenate([rng.uniform(-2e-5, 2e-5, trial.size - 200), rng.uniform(-1e-12, 1e-12, 200)])
+    q = np.clip(1.0 - a * p.astype(np.float64) * (1.0 + k), 0.0, None).astype(np.float32)
+    d = np.full(trial.size, 1e-3, np.float32)
+    h = np.full(trial.size, 3e-3, np.float32)
+    e = rng.uniform(-0.05, 0.0, trial.size).astype(np.float32)
+    got, pred = SolvePorosity(q, p, d, h, e, Vp, n0)
+    got, pred = got.cpu().numpy(), pred.cpu().numpy()
+    args = [tuple(float(v[i]) for v in (q, p, d, h, e)) for i in range(trial.size)]
+    ref = np.array([ora.solve_porosity(*args[i], float(Vp[i]), n0) for i in range(trial.size)], np.float32)
+    np.testing.assert_allclose(got, ref, rtol=2e-7, atol=0)
+    # Where the reference's float64 test takes the elastic exit the device returns float32(trial).
+    elastic = q.astype(np.float64) + a * p.astype(np.float64) <= 1.0
+    np.testing.assert_array_equal(got[elastic], trial[elastic].astype(np.float32))
+    np.testing.assert_array_equal(got[elastic], ref[elastic])
+    ref_pred = np.array([ora.porosity_prediction(float(got[i]), *args[i], float(Vp[i]), n0)
+                         for i in range(trial.size)])
+    np.testing.assert_allclose(pred, ref_pred, rtol=1e-12, atol=1e-15)
+    assert elastic.sum() > trial.size // 4 and (~elastic).sum() > trial.size // 4
