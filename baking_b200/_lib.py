@@ -33,7 +33,7 @@ class BkScalarParams(C.Structure):
                 ("resolution", C.c_int32)]
 
 
-# name -> argtypes (all functions return int status except the two queries)
+# name -> argtypes (an int status unless RESTYPES says otherwise; bk_version and bk_last_error are bound apart)
 SIGNATURES = {
     "bk_particle_to_grid": [I64, I64, P, P, P, P, P, P, P, P, F32, I32, F32, P, P],
     "bk_update_grid": [I32, P, P, I32, P, F32, P],
@@ -60,7 +60,11 @@ SIGNATURES = {
     "bk_profile_stop": [],
     "bk_profile_select": [C.c_char_p],
     "bk_profile_report": [I32, P, I32, P, P, P],
+    "bk_sort_by_cell": [I64, I64, P, P, F32, I32, P, P, I64, P],
+    "bk_sort_by_cell_scratch_bytes": [I64, I32],
 }
+# entry points whose return value is a count, not a status
+RESTYPES = {"bk_sort_by_cell_scratch_bytes": C.c_int64}
 
 _lib = None
 
@@ -98,7 +102,7 @@ def _bind(lib):
     lib.bk_last_error.argtypes = []
     for name, argtypes in SIGNATURES.items():
         fn = getattr(lib, name)
-        fn.restype = C.c_int
+        fn.restype = RESTYPES.get(name, C.c_int)
         fn.argtypes = argtypes
     _lib = lib
     return lib

@@ -75,9 +75,30 @@ class MpmSimulator:
             self.material.initial_temperature_k = transport_config.initial_temperature_k
             self.transport = ThermalWaterTransport(self, transport_config)
         self._buffers = {}
+        # particle_order[k]: index in the constructor's samples of the particle at position k
+        self.particle_order = torch.arange(len(particle_samples.particle_positions), device=self.device)
+        self.sort_count = 0
         self.Reset()
 
     # --------------------------------------------------------------- state
+    @property
+    def particle_samples(self):
+        """The particle samples in the current particle order (permuted on first read after
+        SortParticles)."""
+        if self._samples_order is not None:
+            order = self._samples_order.cpu().numpy()
+            s, n = self._particle_samples, len(order)
+            self._particle_samples = replace(s, **{
+                f.name: np.asarray(getattr(s, f.name))[order] for f in fields(s)
+                if np.ndim(getattr(s, f.name)) >= 1 and len(getattr(s, f.name)) == n})
+            self._samples_order = None
+        return self._particle_samples
+
+    @particle_samples.setter
+    def particle_samples(self, samples):
+        self._particle_samples = samples
+        self._samples_order = None
+
     @property
     def current_state(self):
         """The accepted state; its derivable reference fields are filled before it is returned."""
@@ -146,6 +167,106 @@ class MpmSimulator:
                                "baking was not started. Increase the maximum duration or review tolerances/material.")
 
     # -------------------------------------------------------------- set-up
+    # ------------------------------------------------------------ particle order
+    def CellOrder(self):
+        """The permutation that groups the current particles by quadratic stencil base in Morton
+        order (``bk_sort_by_cell``, stable): int64 device tensor, position k takes the particle now
+        at ``order[k]``."""
+        n = self.particle_data.particle_count
+        x = self._current.particle_positions
+        s = self.simulation_config
+        lib = _lib.load()
+        need = lib.bk_sort_by_cell_scratch_bytes(n, s.grid_resolution)
+        if need < 0:
+            raise RuntimeError(f"bk_sort_by_cell_scratch_bytes: {lib.bk_last_error().decode(errors='replace')}")
+        scratch = torch.empty(max(int(need), 1), dtype=torch.uint8, device=self.device)
+        order = torch.empty(n, dtype=torch.int32, device=self.device)
+        origin = (_lib.C.c_float * 3)(*s.grid_origin)
+        _lib.call("bk_sort_by_cell", n, arrays.layout_pitch(x) if n else 0, arrays.ptr(x), _lib.C.addressof(origin),
+                  s.grid_spacing, s.grid_resolution, order.data_ptr(), scratch.data_ptr(), int(need),
+                  _lib.stream_handle())
+        return order.long()
+
+    def _particle_arrays(self):
+        """Every device array holding one row per particle, each storage view once."""
+        n = self.particle_data.particle_count
+        out, seen = [], set()
+
+        def visit(t):
+            if isinstance(t, torch.Tensor) and t.dim() >= 1 and t.shape[0] == n:
+                key = (t.data_ptr(), tuple(t.shape), tuple(t.stride()), t.dtype)
+                if key not in seen:
+                    seen.add(key)
+                    out.append(t)
+
+        def visit_fields(holder):
+            if holder is not None:
+                for f in fields(holder):
+                    visit(getattr(holder, f.name))
+
+        for st in (self._current, self.next_state):
+            visit_fields(st)
+            visit_fields(st.material_state)
+            visit_fields(st.transport_state)
+        visit_fields(self.particle_data)
+        for t in (self.kirchhoff_stresses, self._stress_water, self.settling_reference_plastic,
+                  *self._prepared.values(), *self._buffers.get("transport", {}).values()):
+            visit(t)
+        if isinstance(self.material, DingMaterial) and n > 1:
+            visit(self.material.production_parameter)
+        if self.transport is not None:
+            for t in (self.transport.reference_volumes, self.transport.dry_masses, self.transport.capacities):
+                visit(t)
+        return out
+
+    def SortParticles(self, order=None):
+        """Reorder the particles in place by grid cell (``CellOrder``, or a given permutation), so
+        that the scatter kernels see long runs of particles sharing a stencil base and compact
+        per-block node boxes. No counterpart in the reference, whose kernels read particles in
+        sample order; results differ from the unsorted run only by float summation order.
+
+        Every per-particle array (both ping-pong states, constants, gas source rates, settling
+        reference) is permuted in place, so captured CUDA graphs stay valid; the particle indices of
+        the mesh binding and of the surface face owners are renumbered, and ``particle_samples``
+        is replaced by a permuted copy (``Reset`` then starts from the sorted order).
+        ``particle_order[k]`` is the index, in the samples given at construction, of the particle
+        now at position k. Per-particle inputs given afterwards (gas source rates, rollout inputs)
+        are in the new order. Not available while the simulator keeps a state history."""
+        if self.retain_history:
+            raise ValueError("SortParticles would reorder the kept state history")
+        n = self.particle_data.particle_count
+        if order is None:
+            order = self.CellOrder()
+        else:
+            order = torch.as_tensor(order, device=self.device).long()
+            if order.shape != (n,) or (n and not torch.equal(torch.sort(order).values,
+                                                            torch.arange(n, device=self.device))):
+                raise ValueError("order must be a permutation of the particle indices")
+        if n == 0:
+            return order
+        self.current_state  # fill the derivable arrays so they move with the particles
+        inverse = torch.empty_like(order)
+        inverse[order] = torch.arange(n, device=self.device)
+        for t in self._particle_arrays():
+            t.copy_(t.index_select(0, order))
+        index_arrays = [self.mesh_binding.binding_particles]
+        if self.transport is not None:
+            index_arrays.append(self.transport.owners)
+            surface = getattr(self._engine, "_surface_tensors", None)
+            if surface is not None:
+                index_arrays.append(surface["owners"])
+        for t in index_arrays:
+            t.copy_(torch.where(t >= 0, inverse[t.clamp(min=0).long()].to(t.dtype), t))
+        self.mesh_binding.tables = replace(self.mesh_binding.tables,
+                                           binding_particles=self.mesh_binding.binding_particles.cpu().numpy())
+        # the host samples follow when next read (particle_samples)
+        self._samples_order = order if self._samples_order is None else self._samples_order[order]
+        self.particle_order = self.particle_order[order]
+        self.sort_count += 1
+        self._buffers.pop("rollout", None)  # reverse-mode buffers hold per-particle copies
+        self._stale = True
+        return order
+
     def SetGasSourceRates(self, rates):
         """Per-particle gas source rate alpha_i (mol/(kg s)) in place of the scalar production parameter."""
         rates = torch.as_tensor(np.asarray(rates, dtype=np.float32), device=self.device).reshape(-1)
@@ -414,6 +535,8 @@ class MpmSimulator:
             source_tets=np.asarray(self.particle_samples.source_tets).copy(),
             simulation_time=self.step_count * self.simulation_config.time_step,
             baking_time_s=self.baking_time, settling_steps=self.settling_steps)
+        if self.sort_count:
+            snap["particle_order"] = self.particle_order.cpu().numpy()  # after SortParticles
         if isinstance(self.material, DingMaterial):
             for name in ("elastic_gradients", "plastic_gradients", "kirchhoff_stresses", "return_residuals",
                          "porosities", "temperatures", "gelled", "yield_stresses", "viscosities", "gas_moles",

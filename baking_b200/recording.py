@@ -84,25 +84,32 @@ class SimulationRecorder:
         self._tets = torch.as_tensor(np.ascontiguousarray(sim.tet_mesh.tet_indices, dtype=np.int32), device=dev)
         self._regions = None
         if sim.transport is not None:
-            # bit 0: owns a boundary face; bit 1: the initial core, radius < 0.4 of the largest
-            # distance of a sampled position from the mesh centroid (recording.py:80-86)
-            n = sim.particle_data.particle_count
-            regions = np.zeros(n, dtype=np.uint8)
-            regions[sim.transport.owners.cpu().numpy()] |= 1
-            positions = np.asarray(sim.particle_samples.particle_positions)
-            center = np.mean(sim.tet_mesh.vertex_positions, axis=0)
-            radius = np.linalg.norm(positions - center, axis=1)
-            core = radius < 0.4 * radius.max()
-            if not core.any():
-                core = radius == radius.min()
-            regions[core] |= 2
-            self._regions = torch.as_tensor(regions, device=dev)
+            self._regions = self._particle_regions()
             config = sim.transport.config
             volumes = np.asarray(sim.particle_samples.reference_volumes, dtype=np.float64)
             self._initial_water = config.water_density * config.initial_saturation * volumes.sum()
 
+    def _particle_regions(self):
+        """Per-particle region bits in the simulator's current particle order: bit 0, owns a
+        boundary face; bit 1, the initial core, radius < 0.4 of the largest distance of a sampled
+        position from the mesh centroid (recording.py:80-86)."""
+        sim = self.simulator
+        self._sort_count = sim.sort_count
+        regions = np.zeros(sim.particle_data.particle_count, dtype=np.uint8)
+        regions[sim.transport.owners.cpu().numpy()] |= 1
+        positions = np.asarray(sim.particle_samples.particle_positions)
+        center = np.mean(sim.tet_mesh.vertex_positions, axis=0)
+        radius = np.linalg.norm(positions - center, axis=1)
+        core = radius < 0.4 * radius.max()
+        if not core.any():
+            core = radius == radius.min()
+        regions[core] |= 2
+        return torch.as_tensor(regions, device=sim.device)
+
     def _inputs(self, state):
         sim = self.simulator
+        if self._regions is not None and sim.sort_count != self._sort_count:
+            self._regions = self._particle_regions()  # the particles were reordered
         m = BkMeasureInputs()
         m.n = sim.particle_data.particle_count
         m.pitch = arrays.layout_pitch(state.deformation_gradients)

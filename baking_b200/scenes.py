@@ -12,7 +12,7 @@ grid cell inside the ball, meshed with the voxels that the ball covers.
 
 from __future__ import annotations
 
-from dataclasses import dataclass, replace
+from dataclasses import dataclass, fields, replace
 
 import numpy as np
 
@@ -168,6 +168,22 @@ def jittered_sphere(resolution=64, per_axis=2, radius=0.1, center=(0.5, 0.5, 0.3
     return Scene("jittered_sphere", mesh, samples, sim, MaterialConfig(model="ding2019"), DingConfig(),
                  TransportConfig(enabled=True, initial_temperature_k=298.15, oven_temperature_k=453.15,
                                  tray_temperature_k=453.15, initial_saturation=0.4))
+
+
+def permuted(scene, order):
+    """The same scene with its particles listed in another order (``order[k]`` is the sample that
+    goes to position k): every per-particle sample array and per-particle gas source rate."""
+    order = np.asarray(order)
+    n = len(scene.samples.particle_positions)
+    if sorted(order.tolist()) != list(range(n)):
+        raise ValueError("order must be a permutation of the particle indices")
+    s = scene.samples
+    samples = replace(s, **{f.name: np.asarray(getattr(s, f.name))[order] for f in fields(s)
+                            if np.ndim(getattr(s, f.name)) >= 1 and len(getattr(s, f.name)) == n})
+    rates = scene.gas_source_rates
+    if rates is not None and np.ndim(rates) >= 1 and len(rates) == n:
+        rates = np.asarray(rates)[order]
+    return replace(scene, samples=samples, gas_source_rates=rates)
 
 
 def make_simulator(scene, engine="cuda", **kwargs):

@@ -510,7 +510,35 @@ def variants(args, rank, dist):
         make_simulator(sphere, diagnostics="lean"), dist, stream, world,
         f"dough sphere {sphere.particle_count} particles, 64^3, Ding + gas + thermal-water")
     out["batched"] = batched(args, rank, dist, net)
+    out["cell_order"] = cell_order_variant(args, rank, dist, stream, world)
     return out
+
+
+def cell_order_variant(args, rank, dist, stream, world, steps=20):
+    """The headline loaf with its particles listed in a random order, timed before and after
+    MpmSimulator.SortParticles (device radix sort by stencil base, every per-particle array
+    permuted in place), and the cost of the sort itself."""
+    import torch
+    from baking_b200.scenes import box_loaf, make_simulator, permuted
+    scene = box_loaf(args.resolution, args.particles, seed=rank)
+    n = scene.particle_count
+    shuffled = permuted(scene, np.random.default_rng(rank).permutation(n))
+    sim = make_simulator(shuffled, diagnostics="lean")
+    sim.AdvanceUnchecked(3)
+    t_shuffled, _ = _timed(lambda: sim.AdvanceUnchecked(steps), dist, stream)
+    sim.CellOrder()  # loads the sort kernels
+    t_keys, _ = _timed(sim.CellOrder, dist, stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter()
+    t_sort, _ = _timed(sim.SortParticles, dist, stream)
+    wall = reduce_max(time.perf_counter() - wall, dist)
+    sim.AdvanceUnchecked(3)
+    t_sorted, _ = _timed(lambda: sim.AdvanceUnchecked(steps), dist, stream)
+    sim.CheckState()
+    return {"unit": UNIT, "shuffled": world * n * steps / t_shuffled, "sorted": world * n * steps / t_sorted,
+            "speedup": t_shuffled / t_sorted, "cell_order_ms": 1e3 * t_keys, "sort_particles_ms": 1e3 * t_sort,
+            "sort_particles_wall_ms": 1e3 * wall, "steps": steps,
+            "scene": f"box loaf {n} particles, {args.resolution}^3, particles in random order"}
 
 
 if __name__ == "__main__":

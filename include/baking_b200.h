@@ -494,6 +494,21 @@ BK_API int bk_measure_state(const BkMeasureInputs *in, double *out, double *scra
 BK_API int bk_step_summary(const BkSubstepParams *params, const BkState *state, const BkConstants *constants,
                            const BkGrid *grid, double *out, double *scratch, void *stream);
 
+/* ---- particle order (no counterpart in the reference, whose Warp kernels read particles in
+   sample order) ---- */
+
+/* Device bytes of `scratch` that bk_sort_by_cell needs for n particles on an R^3 grid; -1 with
+   an error message on bad arguments. Host call, no launch. */
+BK_API int64_t bk_sort_by_cell_scratch_bytes(int64_t n, int32_t resolution);
+
+/* order[k] = index of the particle that goes to position k: particles grouped by quadratic stencil
+   base floor((x - origin)/dx - 0.5), the bases in Morton order, particles of one base in their
+   current relative order (stable); particles whose stencil leaves the grid go last. x: 3 planes
+   of `pitch`; origin: 3 floats in HOST memory; order: n int32 (device); scratch: device, 256-byte
+   aligned, at least bk_sort_by_cell_scratch_bytes(n, resolution) bytes. */
+BK_API int bk_sort_by_cell(int64_t n, int64_t pitch, const float *x, const float *origin, float dx,
+                           int32_t resolution, int32_t *order, void *scratch, int64_t scratch_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
