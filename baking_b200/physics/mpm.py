@@ -33,6 +33,11 @@ from .thermal_water import AllocateTransportState, ThermalWaterTransport
 
 
 
+_DING_SNAPSHOT = ("elastic_gradients", "plastic_gradients", "kirchhoff_stresses", "return_residuals", "porosities",
+                  "temperatures", "gelled", "yield_stresses", "viscosities", "gas_moles", "gas_pressures",
+                  "porosity_residuals", "reference_densities")
+
+
 class MpmSimulator:
     def __init__(self, tet_mesh, particle_samples, simulation_config, material_config,
                  initial_velocity=(0.0, 0.0, 0.0), retain_history=False, ding_config=None, transport_config=None,
@@ -538,14 +543,88 @@ class MpmSimulator:
         if self.sort_count:
             snap["particle_order"] = self.particle_order.cpu().numpy()  # after SortParticles
         if isinstance(self.material, DingMaterial):
-            for name in ("elastic_gradients", "plastic_gradients", "kirchhoff_stresses", "return_residuals",
-                         "porosities", "temperatures", "gelled", "yield_stresses", "viscosities", "gas_moles",
-                         "gas_pressures", "porosity_residuals", "reference_densities"):
+            for name in _DING_SNAPSHOT:
                 snap["ding_" + name] = arrays.to_numpy(getattr(st.material_state, name)).copy()
         if st.transport_state is not None:
             for field in fields(st.transport_state):
                 snap["transport_" + field.name] = arrays.to_numpy(getattr(st.transport_state, field.name)).copy()
+        # Resume fields (LoadSnapshot; the reference writes no resume data): the step counter, the
+        # settling state machine and the per-particle gas source rates.
+        snap.update(resume_step_count=self.step_count, resume_mesh_step_count=self.mesh_step_count,
+                    resume_baking_start_step=-1 if self._baking_start_step is None else self._baking_start_step,
+                    resume_settling_quiet_steps=self.settling_quiet_steps,
+                    resume_settling_reference_step=self.settling_reference_step,
+                    resume_settling_plastic_rate=self.settling_plastic_rate,
+                    resume_settling_reason=self.settling_reason)
+        if self.settling_reference_plastic is not None:
+            snap["resume_settling_reference_plastic"] = arrays.to_numpy(self.settling_reference_plastic).copy()
+        if isinstance(self.material, DingMaterial):
+            snap["resume_gas_source_rates"] = self.material.production_parameter.cpu().numpy().copy()
         return snap
+
+    def LoadSnapshot(self, snapshot):
+        """Resume from a snapshot (a path written by ``SaveSnapshot`` or a ``CaptureSnapshot``
+        dict) of a simulator built from the same scene and configuration. Restores the particle
+        state, the mesh vertices, the step counter, the settling state machine, the gas source
+        rates and, for a sorted simulator, its particle order; the next substep continues the
+        saved run (up to float summation order). The reference saves snapshots but cannot load
+        them."""
+        if isinstance(snapshot, (str, Path)):
+            with np.load(snapshot) as data:
+                snap = {k: data[k] for k in data.files}
+        else:
+            snap = dict(snapshot)
+        if self.retain_history:
+            raise ValueError("LoadSnapshot would bypass the kept state history")
+        if "resume_step_count" not in snap:
+            raise ValueError("the snapshot has no resume fields")
+        n = self.particle_data.particle_count
+        if (len(snap["particle_positions"]) != n or not np.array_equal(snap["tetrahedra"], self.tet_mesh.tet_indices)
+                or abs(float(snap["simulation_time"]) - int(snap["resume_step_count"]) *
+                       self.simulation_config.time_step) > 1e-9 * max(1.0, float(snap["simulation_time"]))):
+            raise ValueError("the snapshot belongs to another scene or time step")
+        order = snap.get("particle_order")
+        current = self.particle_order.cpu().numpy()
+        target = np.arange(n) if order is None else np.asarray(order)
+        if not np.array_equal(target, current):
+            inverse = np.empty(n, dtype=np.int64)
+            inverse[current] = np.arange(n)
+            self.SortParticles(order=inverse[target])
+        if not np.array_equal(snap["reference_volumes"], arrays.to_numpy(self.particle_data.reference_volumes)):
+            raise ValueError("the snapshot's reference volumes differ from this simulator's")
+        st = self._current
+        for name in ("particle_positions", "particle_velocities", "deformation_gradients", "affine_velocities"):
+            arrays.assign(getattr(st, name), snap[name])
+        if isinstance(self.material, DingMaterial):
+            for name in _DING_SNAPSHOT:
+                arrays.assign(getattr(st.material_state, name), snap["ding_" + name])
+            rates = snap.get("resume_gas_source_rates")
+            if rates is not None:
+                if rates.shape == tuple(self.material.production_parameter.shape):
+                    arrays.assign(self.material.production_parameter, rates)
+                else:
+                    self.SetGasSourceRates(rates)
+        if st.transport_state is not None:
+            for field in fields(st.transport_state):
+                arrays.assign(getattr(st.transport_state, field.name), snap["transport_" + field.name])
+        arrays.assign(self.vertex_positions, snap["vertices"])
+        if self.settling_reference_plastic is not None and "resume_settling_reference_plastic" in snap:
+            arrays.assign(self.settling_reference_plastic, snap["resume_settling_reference_plastic"])
+        self.step_count = int(snap["resume_step_count"])
+        self.mesh_step_count = int(snap["resume_mesh_step_count"])
+        start = int(snap["resume_baking_start_step"])
+        self._baking_start_step = None if start < 0 else start
+        self.settling_quiet_steps = int(snap["resume_settling_quiet_steps"])
+        self.settling_reference_step = int(snap["resume_settling_reference_step"])
+        self.settling_plastic_rate = float(snap["resume_settling_plastic_rate"])
+        self.settling_reason = str(snap["resume_settling_reason"])
+        self.error_flags.zero_()
+        if self.transport is not None:
+            self.transport.error_flags.zero_()
+        if isinstance(self.material, DingMaterial):
+            self.material.error_flags.zero_()
+        self._buffers.pop("rollout", None)
+        self._stale = True
 
     def SaveSnapshot(self, output_path):
         self.UpdateMesh()
