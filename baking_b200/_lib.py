@@ -62,7 +62,12 @@ SIGNATURES = {
     "bk_profile_report": [I32, P, I32, P, P, P],
     "bk_sort_by_cell": [I64, I64, P, P, F32, I32, P, P, I64, P],
     "bk_sort_by_cell_scratch_bytes": [I64, I32],
+    "bk_permute_particles": [I64, P, I32, P, P, I64, P],
 }
+
+
+class BkParticleArray(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("pitch", C.c_int64), ("planes", C.c_int32), ("element_bytes", C.c_int32)]
 # entry points whose return value is a count, not a status
 RESTYPES = {"bk_sort_by_cell_scratch_bytes": C.c_int64}
 

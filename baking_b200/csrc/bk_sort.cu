@@ -73,6 +73,17 @@ size_t cub_bytes(int64_t n, int end_bit) {
     return bytes;
 }
 
+// scratch[p * n + k] = data[p * pitch + order[k]] over planes x n elements.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_gather_planes(int64_t n, const int32_t* __restrict__ order,
+                                                            int64_t total, const T* __restrict__ data, int64_t pitch,
+                                                            T* __restrict__ scratch) {
+    const int64_t e = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+    if (e >= total) return;
+    const int64_t p = e / n, k = e - p * n;
+    scratch[e] = data[p * pitch + order[k]];
+}
+
 }  // namespace
 
 extern "C" {
@@ -119,6 +130,38 @@ int bk_sort_by_cell(int64_t n, int64_t pitch, const float* x, const float* origi
                                                     end_bit, s);
     if (e != cudaSuccess) return fail(BK_ERR_LAUNCH, cudaGetErrorString(e));
     return check_launch("bk_sort_by_cell/radix_sort");
+}
+
+int bk_permute_particles(int64_t n, const int32_t* order, int32_t array_count, const BkParticleArray* arrays,
+                         void* scratch, int64_t scratch_bytes, void* stream) {
+    if (n < 0 || array_count < 0) return fail(BK_ERR_ARGUMENT, "bk_permute_particles: negative count");
+    if (n == 0 || array_count == 0) return BK_OK;
+    if (!order || !arrays || !scratch) return fail(BK_ERR_ARGUMENT, "bk_permute_particles: null argument");
+    for (int32_t a = 0; a < array_count; ++a) {
+        const BkParticleArray& arr = arrays[a];
+        if (!arr.data || arr.planes < 1 || arr.pitch < n || (arr.element_bytes != 4 && arr.element_bytes != 8))
+            return fail(BK_ERR_ARGUMENT, "bk_permute_particles: bad array (data, planes, pitch or element size)");
+        if ((int64_t)arr.planes * n * arr.element_bytes > scratch_bytes)
+            return fail(BK_ERR_ARGUMENT, "bk_permute_particles: scratch smaller than the largest array");
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    for (int32_t a = 0; a < array_count; ++a) {
+        const BkParticleArray& arr = arrays[a];
+        const int64_t total = (int64_t)arr.planes * n;
+        const unsigned blocks = (unsigned)((total + kThreads - 1) / kThreads);
+        if (arr.element_bytes == 4)
+            k_gather_planes<uint32_t><<<blocks, kThreads, 0, s>>>(n, order, total, static_cast<const uint32_t*>(arr.data),
+                                                                  arr.pitch, static_cast<uint32_t*>(scratch));
+        else
+            k_gather_planes<uint64_t><<<blocks, kThreads, 0, s>>>(n, order, total, static_cast<const uint64_t*>(arr.data),
+                                                                  arr.pitch, static_cast<uint64_t*>(scratch));
+        if (int rc = check_launch("bk_permute_particles/gather")) return rc;
+        const size_t row = (size_t)n * arr.element_bytes;
+        cudaError_t e = cudaMemcpy2DAsync(arr.data, (size_t)arr.pitch * arr.element_bytes, scratch, row, row,
+                                          (size_t)arr.planes, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) return fail(BK_ERR_LAUNCH, cudaGetErrorString(e));
+    }
+    return BK_OK;
 }
 
 }  // extern "C"

@@ -7,6 +7,8 @@ reference-volume weights (as deviations from the first binding, the anchor).
 
 from __future__ import annotations
 
+from dataclasses import replace
+
 import numpy as np
 import torch
 
@@ -17,7 +19,8 @@ from .sampling import MeshBindingTables_build
 class ParticleMeshBinding:
     def __init__(self, tet_mesh, particle_samples, device_name="cuda"):
         tables = MeshBindingTables_build(tet_mesh, particle_samples)
-        self.tables = tables
+        self._tables = tables
+        self._host_particles_stale = False
         self.unmapped_vertex_count = tables.unmapped_vertex_count
         self.vertex_count = len(tet_mesh.vertex_positions)
         self.reference_vertices = arrays.from_numpy(tet_mesh.vertex_positions.astype(np.float32), "f4", device_name)
@@ -25,6 +28,21 @@ class ParticleMeshBinding:
         self.binding_particles = torch.as_tensor(tables.binding_particles, device=device_name)
         self.binding_weights = torch.as_tensor(tables.binding_weights.astype(np.float32), device=device_name)
         self.reference_offsets = arrays.from_numpy(tables.reference_offsets.astype(np.float32), "f4", device_name)
+
+    @property
+    def tables(self):
+        """The host binding tables; their particle indices follow a renumbering of the device
+        ones (``RenumberParticles``) when next read."""
+        if self._host_particles_stale:
+            self._tables = replace(self._tables, binding_particles=self.binding_particles.cpu().numpy())
+            self._host_particles_stale = False
+        return self._tables
+
+    def RenumberParticles(self, new_index):
+        """After a particle reordering: binding particle p becomes ``new_index[p]`` (device)."""
+        t = self.binding_particles
+        t.copy_(torch.where(t >= 0, new_index[t.clamp(min=0).long()].to(t.dtype), t))
+        self._host_particles_stale = True
 
     def Reconstruct(self, particle_state, output_vertices):
         x = particle_state.particle_positions

@@ -33,6 +33,17 @@ from .thermal_water import AllocateTransportState, ThermalWaterTransport
 
 
 
+def _plane_layout(t):
+    """True for a (n, 3) or (n, 3, 3) view whose components are planes of one pitch."""
+    try:
+        pitch = arrays.layout_pitch(t)
+    except ValueError:
+        return False
+    if t.dim() == 2:
+        return t.stride(0) == 1 and t.stride(1) == pitch
+    return t.dim() == 3 and t.stride(0) == 1 and t.stride(2) == pitch and t.stride(1) == 3 * pitch
+
+
 _DING_SNAPSHOT = ("elastic_gradients", "plastic_gradients", "kirchhoff_stresses", "return_residuals", "porosities",
                   "temperatures", "gelled", "yield_stresses", "viscosities", "gas_moles", "gas_pressures",
                   "porosity_residuals", "reference_densities")
@@ -224,6 +235,27 @@ class MpmSimulator:
                 visit(t)
         return out
 
+    def _permute_arrays(self, order):
+        """Every per-particle array in place through bk_permute_particles (one gather kernel and
+        one 2-D copy per array); arrays not in plane layout go through torch."""
+        n = self.particle_data.particle_count
+        table, largest = [], 0
+        for t in self._particle_arrays():
+            planes = t.numel() // n if n else 0
+            pitch = n if t.dim() == 1 else arrays.layout_pitch(t) if _plane_layout(t) else None
+            if pitch is None or t.element_size() not in (4, 8) or (t.dim() == 1 and t.stride(0) != 1):
+                t.copy_(t.index_select(0, order))
+                continue
+            table.append(_lib.BkParticleArray(t.data_ptr(), pitch, planes, t.element_size()))
+            largest = max(largest, planes * n * t.element_size())
+        if not table:
+            return
+        scratch = torch.empty(largest, dtype=torch.uint8, device=self.device)
+        order32 = order.to(torch.int32)
+        entries = (_lib.BkParticleArray * len(table))(*table)
+        _lib.call("bk_permute_particles", n, order32.data_ptr(), len(table), _lib.C.addressof(entries),
+                  scratch.data_ptr(), largest, _lib.stream_handle())
+
     def SortParticles(self, order=None):
         """Reorder the particles in place by grid cell (``CellOrder``, or a given permutation), so
         that the scatter kernels see long runs of particles sharing a stencil base and compact
@@ -252,9 +284,9 @@ class MpmSimulator:
         self.current_state  # fill the derivable arrays so they move with the particles
         inverse = torch.empty_like(order)
         inverse[order] = torch.arange(n, device=self.device)
-        for t in self._particle_arrays():
-            t.copy_(t.index_select(0, order))
-        index_arrays = [self.mesh_binding.binding_particles]
+        self._permute_arrays(order)
+        self.mesh_binding.RenumberParticles(inverse)
+        index_arrays = []
         if self.transport is not None:
             index_arrays.append(self.transport.owners)
             surface = getattr(self._engine, "_surface_tensors", None)
@@ -262,8 +294,6 @@ class MpmSimulator:
                 index_arrays.append(surface["owners"])
         for t in index_arrays:
             t.copy_(torch.where(t >= 0, inverse[t.clamp(min=0).long()].to(t.dtype), t))
-        self.mesh_binding.tables = replace(self.mesh_binding.tables,
-                                           binding_particles=self.mesh_binding.binding_particles.cpu().numpy())
         # the host samples follow when next read (particle_samples)
         self._samples_order = order if self._samples_order is None else self._samples_order[order]
         self.particle_order = self.particle_order[order]

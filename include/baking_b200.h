@@ -509,6 +509,22 @@ BK_API int64_t bk_sort_by_cell_scratch_bytes(int64_t n, int32_t resolution);
 BK_API int bk_sort_by_cell(int64_t n, int64_t pitch, const float *x, const float *origin, float dx,
                            int32_t resolution, int32_t *order, void *scratch, int64_t scratch_bytes, void *stream);
 
+/* One per-particle array for bk_permute_particles: `planes` planes of n elements of
+   `element_bytes` (4 or 8) bytes, `pitch` elements apart, starting at `data` (device). */
+typedef struct {
+    void *data;
+    int64_t pitch;
+    int32_t planes;
+    int32_t element_bytes;
+} BkParticleArray;
+
+/* In place, for every array: element k of each plane becomes the element order[k] had. `arrays`
+   is a HOST table of `array_count` entries; order: n int32 (device), a permutation; scratch:
+   device, at least planes * n * element_bytes bytes of the largest array. Arrays must not overlap
+   one another. One gather kernel and one 2-D copy per array, in order on `stream`. */
+BK_API int bk_permute_particles(int64_t n, const int32_t *order, int32_t array_count, const BkParticleArray *arrays,
+                                void *scratch, int64_t scratch_bytes, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -177,3 +177,37 @@ def test_rollout_gradients_follow_the_order():
     (gT, gr, _), (sT, sr, order) = results
     np.testing.assert_allclose(sT, gT[order], rtol=1e-4, atol=1e-5 * np.abs(gT).max())
     np.testing.assert_allclose(sr, gr[order], rtol=1e-4, atol=1e-5 * np.abs(gr).max())
+
+
+def test_permute_particles_planes_and_element_sizes():
+    """bk_permute_particles on float32 planes (1, 3 and 9 planes, pitch above n), float64 and int32
+    arrays against numpy indexing; a scratch smaller than the largest array is refused."""
+    import ctypes
+    import torch
+    from baking_b200 import _lib, arrays
+    dev = torch.device("cuda:0")
+    n = 1000
+    rng = np.random.default_rng(4)
+    order = rng.permutation(n)
+    host = [rng.standard_normal((n, 3)).astype(np.float32), rng.standard_normal((n, 3, 3)).astype(np.float32),
+            rng.standard_normal(n), rng.integers(0, 9, n).astype(np.int32)]
+    dev_arrays = [arrays.from_numpy(host[0], "f4", dev), arrays.from_numpy(host[1], "f4", dev),
+                  torch.as_tensor(host[2], device=dev), torch.as_tensor(host[3], device=dev)]
+    assert arrays.layout_pitch(dev_arrays[0]) > n
+    table = (_lib.BkParticleArray * 4)(
+        _lib.BkParticleArray(dev_arrays[0].data_ptr(), arrays.layout_pitch(dev_arrays[0]), 3, 4),
+        _lib.BkParticleArray(dev_arrays[1].data_ptr(), arrays.layout_pitch(dev_arrays[1]), 9, 4),
+        _lib.BkParticleArray(dev_arrays[2].data_ptr(), n, 1, 8),
+        _lib.BkParticleArray(dev_arrays[3].data_ptr(), n, 1, 4))
+    order_d = torch.as_tensor(order, dtype=torch.int32, device=dev)
+    scratch = torch.empty(9 * n * 4, dtype=torch.uint8, device=dev)
+    lib = _lib.load()
+    assert lib.bk_permute_particles(n, order_d.data_ptr(), 4, ctypes.addressof(table), scratch.data_ptr(),
+                                    9 * n * 4 - 1, _lib.stream_handle()) != 0
+    _lib.call("bk_permute_particles", n, order_d.data_ptr(), 4, ctypes.addressof(table), scratch.data_ptr(),
+              9 * n * 4, _lib.stream_handle())
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(arrays.to_numpy(dev_arrays[0]), host[0][order])
+    np.testing.assert_array_equal(arrays.to_numpy(dev_arrays[1]), host[1][order])
+    np.testing.assert_array_equal(dev_arrays[2].cpu().numpy(), host[2][order])
+    np.testing.assert_array_equal(dev_arrays[3].cpu().numpy(), host[3][order])
