@@ -52,14 +52,21 @@ _DING_SNAPSHOT = ("elastic_gradients", "plastic_gradients", "kirchhoff_stresses"
 class MpmSimulator:
     def __init__(self, tet_mesh, particle_samples, simulation_config, material_config,
                  initial_velocity=(0.0, 0.0, 0.0), retain_history=False, ding_config=None, transport_config=None,
-                 diagnostics="full"):
+                 diagnostics="full", sort_interval=0):
         """``diagnostics="full"`` keeps every reference output array current after each substep;
         ``"lean"`` writes only the primary state per substep and fills the derivable arrays
         (plastic gradients, material temperature, density, yield stress, viscosity, gas pressure,
         saturation, particle mass) when ``current_state`` is read. Per-particle return residuals
-        are kept only in "full" mode; both modes keep their per-substep maximum."""
+        are kept only in "full" mode; both modes keep their per-substep maximum.
+
+        ``sort_interval`` k > 0 calls ``SortParticles`` after every k-th substep of ``Step``,
+        ``Advance`` and ``AdvanceUnchecked`` (the particle order then changes; 0, the default,
+        keeps the sample order)."""
         if diagnostics not in ("full", "lean"):
             raise ValueError("diagnostics must be 'full' or 'lean'")
+        if int(sort_interval) != sort_interval or sort_interval < 0 or (sort_interval and retain_history):
+            raise ValueError("sort_interval must be a nonnegative integer, and 0 with retain_history")
+        self.sort_interval = int(sort_interval)
         self.diagnostics = diagnostics
         simulation_config.Validate(material_config)
         self.device = _lib.require_cuda(simulation_config.device_name)
@@ -439,6 +446,8 @@ class MpmSimulator:
             if was_settling and not self.IsSettling:
                 self.result_recorder.settled_measurement = dict(self.result_recorder.last_measurement)
                 self.result_recorder.QueueSnapshot()
+        if self.sort_interval and self.step_count % self.sort_interval == 0:
+            self.SortParticles()
 
     def MaxReturnResiduals(self):
         """(max return residual, max porosity residual) of the last substep, on the host."""

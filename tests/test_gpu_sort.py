@@ -211,3 +211,21 @@ def test_permute_particles_planes_and_element_sizes():
     np.testing.assert_array_equal(arrays.to_numpy(dev_arrays[1]), host[1][order])
     np.testing.assert_array_equal(dev_arrays[2].cpu().numpy(), host[2][order])
     np.testing.assert_array_equal(dev_arrays[3].cpu().numpy(), host[3][order])
+
+
+def test_sort_interval_sorts_during_advance():
+    """sort_interval=5: Advance(10) sorts twice and follows the unsorted run."""
+    from baking_b200.scenes import make_simulator
+    scene = _shuffled_sphere(seed=13)
+    plain = make_simulator(scene)
+    auto = make_simulator(scene, sort_interval=5)
+    plain.Advance(10)
+    auto.Advance(10)
+    assert auto.sort_count == 2
+    src = auto.particle_order.cpu().numpy()
+    np.testing.assert_allclose(_host(auto.current_state.particle_positions),
+                               _host(plain.current_state.particle_positions)[src], rtol=0, atol=2e-6)
+    np.testing.assert_allclose(_host(auto.current_state.transport_state.temperatures),
+                               _host(plain.current_state.transport_state.temperatures)[src], rtol=1e-7)
+    with pytest.raises(ValueError):
+        make_simulator(scene, sort_interval=5, retain_history=True)
