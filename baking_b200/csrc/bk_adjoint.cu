@@ -240,7 +240,17 @@ __device__ __noinline__ float coupled_solve_grad(const float* s, float mu, float
                                                  float n0, float por, float* G) {
     const CoupledFwd c = coupled_forward(s, mu, lam, ty, eta, dt, n0, por);
     double r = 0.0;
-    const float nf = solve_porosity(c.q, c.p, c.df, c.ms, c.ex, c.Vp, n0, &r);
+    bool elastic_exit;
+    const float nf = solve_porosity(c.q, c.p, c.df, c.ms, c.ex, c.Vp, n0, &r, &elastic_exit);
+    if (elastic_exit) {
+        // Certain elastic exit: q + a(nf) p <= 1, so r = 0, v = 1, E = 1 and every derivative below
+        // is an exact zero except dn/dVp = 1 (the same values the general path computes for finite
+        // parameters).
+#pragma unroll
+        for (int k = 0; k < 7; ++k) G[k] = 0.f;
+        G[7] = 1.f;
+        return nf;
+    }
     const double n = (double)nf;
     const double q = c.q, p = c.p, d = c.df, h = c.ms, e = c.ex, Vp = c.Vp;
     const double a = pressure_coefficient64(n);
