@@ -44,3 +44,15 @@ def test_permuted_rejects_non_permutations():
         permuted(scene, np.zeros(n, dtype=np.int64))
     with pytest.raises(ValueError):
         permuted(scene, np.arange(n - 1))
+
+
+def test_permutation_table_takes_plane_layout_arrays_only():
+    """SortParticles hands plane-layout arrays ((n, 3) with strides (1, pitch), (n, 3, 3) with
+    strides (1, 3 pitch, pitch)) to bk_permute_particles and row-major ones to torch."""
+    import ctypes
+    import torch
+    from baking_b200 import _lib, arrays
+    from baking_b200.physics.mpm import _plane_layout
+    assert _plane_layout(arrays.vec3s(100, device="cpu")) and _plane_layout(arrays.mat33s(100, device="cpu"))
+    assert not _plane_layout(torch.zeros(100, 3)) and not _plane_layout(torch.zeros(100, 3, 3))
+    assert ctypes.sizeof(_lib.BkParticleArray) == 24  # void*, int64_t, int32_t, int32_t
