@@ -199,11 +199,15 @@ def make_simulator(scene, engine="cuda", **kwargs):
     if scene.gas_source_rates is not None:
         sim.SetGasSourceRates(scene.gas_source_rates)
     if any(scene.initial_log_strain):
-        import torch
         stretch = np.diag(np.exp(np.asarray(scene.initial_log_strain, np.float64))).astype(np.float32)
         st = sim.current_state
         for target in (st.deformation_gradients, getattr(st.material_state, "elastic_gradients", None)):
-            if target is not None:
+            if target is None:
+                continue
+            if isinstance(target, np.ndarray):
+                target[...] = stretch
+            else:
+                import torch
                 target.copy_(torch.as_tensor(stretch, device=target.device).expand(target.shape))
     return sim
 

@@ -1,0 +1,119 @@
+"""Parity at the stated bar on the benchmark scenes themselves, device substep against the oracle.
+
+The bar: grid mass and momentum within 1e-5 relative at every substep; particle x within 1e-4*dx
+and F, Fe, temperature, water, gas content and porosity within 1e-4 relative at the end.
+
+* The 64^3 jittered dough sphere (r 0.1 at (0.5, 0.5, 0.3), 2 particles per axis per cell, Ding
+  defaults, 25 C start, saturation 0.4, 180 C oven, gas off, dt 1e-4) for 200 substeps.
+* The 1,000,000-particle box loaf on the 128^3 grid (Ding + gas + thermal-water, per-particle gas
+  source rates in [0, 1e-3], dt 5e-5), the benchmark workload at full size, for 20 substeps.
+* The same loaf part-baked (318.15 K) and pre-stressed (isochoric log strain 0.08), so every
+  particle takes the plastic branch of the return map and the coupled porosity solve.
+
+Each test prints the largest deviation it saw (in units of its tolerance) so a run with ``-s``
+records the margin. The reference steps these scenes through ``MpmSimulator.Step``
+(physics/mpm.py:163-225) with the defaults of config.py:110-171.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from tests.scenes import to_np
+
+pytestmark = pytest.mark.gpu
+
+
+class Margins:
+    """Largest deviation over the run per checked quantity, as a fraction of its tolerance."""
+
+    def __init__(self, name):
+        self.name = name
+        self.worst = {}
+
+    def note(self, key, value):
+        self.worst[key] = max(self.worst.get(key, 0.0), float(value))
+
+    def report(self):
+        parts = ", ".join(f"{k} {v:.3g}" for k, v in sorted(self.worst.items()))
+        print(f"\n[{self.name}] worst deviation / tolerance: {parts}")
+
+
+def _fraction(actual, desired, rtol, atol):
+    actual = np.asarray(actual, np.float64)
+    desired = np.asarray(desired, np.float64)
+    bound = atol + rtol * np.abs(desired)
+    return float(np.max(np.abs(actual - desired) / bound)) if actual.size else 0.0
+
+
+def _check(margins, key, actual, desired, rtol, atol):
+    frac = _fraction(actual, desired, rtol, atol)
+    margins.note(key, frac)
+    assert frac <= 1.0, f"{margins.name}: {key} off by {frac:.3g} x tolerance"
+
+
+def _check_grid(margins, ref, dev):
+    m_ref = ref.grid_masses.astype(np.float64)
+    m_dev = to_np(dev.grid_state.node_masses).astype(np.float64)
+    _check(margins, "grid mass total", m_dev.sum(), m_ref.sum(), 1e-5, 0.0)
+    _check(margins, "grid mass", m_dev, m_ref, 1e-5, 1e-5 * m_ref.max())
+    p_ref = ref.grid_momenta.astype(np.float64)
+    p_dev = to_np(dev.grid_state.node_momenta).astype(np.float64)
+    _check(margins, "grid momentum", p_dev, p_ref, 1e-5, 1e-5 * np.abs(p_ref).max())
+
+
+def _check_state(margins, ref, dev, dx):
+    a, b = ref.current_state, dev.current_state
+    _check(margins, "x", to_np(b.particle_positions), a.particle_positions, 0.0, 1e-4 * dx)
+    _check(margins, "F", to_np(b.deformation_gradients), a.deformation_gradients, 1e-4, 1e-4)
+    ts, td = a.transport_state, b.transport_state
+    _check(margins, "temperature", to_np(td.temperatures), ts.temperatures, 1e-4, 0.0)
+    _check(margins, "water", to_np(td.water_masses), ts.water_masses, 1e-4, 0.0)
+    ms, md = a.material_state, b.material_state
+    _check(margins, "Fe", to_np(md.elastic_gradients), ms.elastic_gradients, 1e-4, 1e-4)
+    _check(margins, "porosity", to_np(md.porosities), ms.porosities, 1e-4, 1e-7)
+    _check(margins, "gas", to_np(md.gas_moles), ms.gas_moles, 1e-4, 1e-12)
+
+
+def _run(scene, steps, name, threads=None):
+    from baking_b200.scenes import make_simulator
+    from oracle import ora
+    from oracle.sim import OracleSimulator
+    ora.set_threads(threads or os.cpu_count() or 1)
+    ref = make_simulator(scene, engine=OracleSimulator)
+    dev = make_simulator(scene)
+    margins = Margins(name)
+    for _ in range(steps):
+        ref.Step()
+        dev.Step()
+        _check_grid(margins, ref, dev)
+    _check_state(margins, ref, dev, scene.simulation.grid_spacing)
+    margins.report()
+    return ref, dev
+
+
+def test_jittered_sphere_200_substeps():
+    """64^3 sphere (about 8.8k particles) for 200 substeps at dt 1e-4."""
+    from baking_b200.scenes import jittered_sphere
+    scene = jittered_sphere(64, 2, 0.1, (0.5, 0.5, 0.3), seed=0, time_step=1e-4)
+    assert 8000 < scene.particle_count < 9500
+    ref, dev = _run(scene, 200, "sphere 64^3 x 200")
+    # The sphere fell under gravity for 200 substeps: 0.5 g t^2 with t = 0.02 s.
+    drop = float(np.mean(scene.samples.particle_positions[:, 1] - ref.current_state.particle_positions[:, 1]))
+    assert abs(drop - 0.5 * 9.8 * 0.02 ** 2) < 0.1 * 0.5 * 9.8 * 0.02 ** 2
+
+
+def test_box_loaf_full_size():
+    """The benchmark loaf itself: 1M particles, 128^3, gas + thermal-water, 20 substeps."""
+    from baking_b200.scenes import box_loaf
+    scene = box_loaf(128, 1_000_000, seed=0)
+    _run(scene, 20, "box loaf 1M x 20")
+
+
+def test_yielding_box_loaf_full_size():
+    """The loaf part-baked and pre-stressed so every particle yields: 1M particles, 20 substeps."""
+    from baking_b200.scenes import box_loaf
+    scene = box_loaf(128, 1_000_000, seed=0, initial_temperature=318.15, prestrain=0.08)
+    ref, dev = _run(scene, 20, "yielding loaf 1M x 20")
+    residuals = ref.current_state.material_state.return_residuals
+    assert np.mean(residuals > 0) > 0.9, "the pre-stressed loaf should yield almost everywhere"
