@@ -3,17 +3,16 @@
 The dataclasses carry the same sections, field names, defaults and validation
 messages as the reference's ``config.py`` (``MaterialConfig`` config.py:10-38,
 ``SimulationConfig`` :41-75, ``DingConfig`` :109-145, ``TransportConfig``
-:148-196, ``ExperimentConfig`` :199-233, INI loader :236-304), so a caller of the
-reference can hand its configuration objects to this package unchanged.
+:148-196, ``ExperimentConfig`` :199-233), so a caller of the reference can hand its
+configuration objects to this package unchanged. The reference's INI file loader is not part
+of the substep and is not provided.
 """
 
 from __future__ import annotations
 
-import configparser
 import math
 import re
-from dataclasses import dataclass, field, fields
-from pathlib import Path
+from dataclasses import dataclass, field
 
 
 def _finite(*values):
@@ -252,74 +251,3 @@ class ExperimentConfig:
             raise ValueError("snapshot_interval must be nonnegative")
         if self.run.steps < 1 or self.run.report_interval < 1:
             raise ValueError("steps and report_interval must be positive")
-
-
-_BOOLS = {"true": True, "false": False, "yes": True, "no": False, "1": True, "0": False}
-
-
-def ParseConfigValue(raw, default, variable_length=False):
-    """Convert one INI string to the type of ``default``."""
-    if isinstance(default, bool):
-        key = raw.lower()
-        if key not in _BOOLS:
-            raise ValueError("expected true or false")
-        return _BOOLS[key]
-    if isinstance(default, int):
-        return int(raw)
-    if isinstance(default, float):
-        return float(raw)
-    if isinstance(default, tuple):
-        values = tuple(float(part.strip()) for part in raw.split(","))
-        if (not variable_length and len(values) != len(default)) or not _finite(*values):
-            count = "three" if len(default) == 3 else str(len(default))
-            raise ValueError(f"expected {count} finite numbers separated by commas")
-        return values
-    if len(raw) >= 2 and raw[0] == raw[-1] and raw[0] in "\"'":
-        return raw[1:-1]
-    return raw
-
-
-def LoadExperimentConfig(config_path):
-    """Read a UTF-8 INI file into an ``ExperimentConfig``; unknown sections or keys are errors.
-
-    Relative ``mesh_path``/``output_path``/``log_path`` values resolve against the file's folder.
-    """
-    config_path = Path(config_path).expanduser().resolve()
-    parser = configparser.ConfigParser(interpolation=None, inline_comment_prefixes=("#", ";"))
-    parser.optionxform = str
-    try:
-        with config_path.open("r", encoding="utf-8-sig") as stream:
-            parser.read_file(stream)
-        if parser.defaults():
-            raise ValueError("[DEFAULT] is unsupported; place values in their named sections")
-        base = ExperimentConfig()
-        sections = {f.name: getattr(base, f.name) for f in fields(base)}
-        for name in parser.sections():
-            if name not in sections:
-                raise ValueError(f"unknown section [{name}]")
-        built = {}
-        for name, default_section in sections.items():
-            defaults = {f.name: getattr(default_section, f.name) for f in fields(default_section)}
-            values = {}
-            if parser.has_section(name):
-                for key, raw in parser.items(name):
-                    if key not in defaults:
-                        raise ValueError(f"unknown parameter [{name}] {key}")
-                    try:
-                        values[key] = ParseConfigValue(raw, defaults[key])
-                    except ValueError as error:
-                        raise ValueError(f"[{name}] {key}: {error}") from error
-            if name == "run":
-                values.setdefault("log_path", default_section.log_path)
-            for key in ("mesh_path", "output_path", "log_path"):
-                if values.get(key):
-                    path = Path(values[key]).expanduser()
-                    if not path.is_absolute():
-                        path = config_path.parent / path
-                    values[key] = str(path.resolve())
-            built[name] = type(default_section)(**values)
-        result = ExperimentConfig(**built)
-        result.Validate()
-        return result
-    except (OSError, UnicodeError, ValueError, configparser.Error) as error:
-        raise ValueError(f"Configuration file {config_path}: {error}") from error
