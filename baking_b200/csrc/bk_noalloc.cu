@@ -13,9 +13,15 @@
 // call on a device and keeps the last call's contents, so each call first resets the part it uses;
 // calls whose executions overlap on the GPU (different streams or threads) race on it and must
 // be serialised by the caller.
+//
+// Start-up. Under lazy module loading (CUDA_MODULE_LOADING=LAZY, the default since CUDA 12.2) the
+// module holding the array is loaded, and the array's device memory reserved, by the first call
+// in each CUDA context. That first call may therefore allocate; a caller that must not allocate
+// later makes one call per device (and per context it uses) at start-up, before any stream
+// capture. Every call works in whatever context is current: primary or not, before or after a
+// cudaDeviceReset.
 #include <climits>
 #include <cstdio>
-#include <mutex>
 
 #include "baking_b200.h"
 #include "bk_common.h"
@@ -31,29 +37,20 @@ constexpr long long kScratchBytes = kBoundsOffset + 256;
 // The grid scratch of bk_substep_static_grid: node_pm, then node_v, then 12 ints of bounds.
 static __device__ __align__(256) unsigned char g_grid_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-void* g_scratch_address[kMaxDevices] = {};
-
-// Device address of g_grid_scratch for the current device, looked up once per device. The host
-// symbol g_grid_scratch is only a handle: its host address must never reach a kernel.
+// Device address of g_grid_scratch in the current context. The host symbol g_grid_scratch is only
+// a handle: its host address must never reach a kernel. The address is looked up on every call
+// rather than cached per device: after cudaDeviceReset, or with a non-primary context made current
+// (cuCtxCreate/cuCtxSetCurrent), the array lives at another address, and once the module is
+// loaded in the context the lookup allocates nothing.
 int scratch_address(void** out) {
-    int device = 0;
-    cudaError_t e = cudaGetDevice(&device);
-    if (e != cudaSuccess) return bk::fail(BK_ERR_LAUNCH, "bk_substep_static_grid: no current CUDA device");
-    if (device < 0 || device >= kMaxDevices) return bk::fail(BK_ERR_UNSUPPORTED, "bk_substep_static_grid: device index too large");
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_address[device]) {
-        void* ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_grid_scratch);
-        if (e != cudaSuccess || !ptr) {
-            char msg[256];
-            snprintf(msg, sizeof msg, "bk_substep_static_grid: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-            return bk::fail(BK_ERR_LAUNCH, msg);
-        }
-        g_scratch_address[device] = ptr;
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_grid_scratch);
+    if (e != cudaSuccess || !ptr) {
+        char msg[256];
+        snprintf(msg, sizeof msg, "bk_substep_static_grid: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        return bk::fail(BK_ERR_LAUNCH, msg);
     }
-    *out = g_scratch_address[device];
+    *out = ptr;
     return BK_OK;
 }
 

@@ -2,7 +2,10 @@
 
 It must give the same particle state as bk_substep with a caller-allocated grid, for two
 substeps in a row (the second call finds the shared static grid holding the first call's nodes,
-so it also checks that each call resets what it uses). Both entry points are called directly
+so it also checks that each call resets what it uses), on the demo grid (40^3) and on the largest
+grid the array holds (48^3, where the velocity nodes and the box bounds sit at the array's end).
+The second call must leave the device's free memory unchanged: that is the property the entry
+point exists for. Both entry points are called directly
 through the C ABI on the same inputs. Float atomics accumulate in a different order in the two
 runs, so results agree to the parity tolerance used elsewhere (1e-5 relative), not bit for bit.
 """
@@ -15,13 +18,14 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-def _scene():
+def _scene(resolution=40):
     from dataclasses import replace
     from baking_b200.config import DingConfig, MaterialConfig, SimulationConfig
     from baking_b200.geometry import CreateDemoMesh, SampleParticles
     from baking_b200.physics.mpm import MpmSimulator
     mesh = CreateDemoMesh(3)
-    sim = MpmSimulator(mesh, SampleParticles(mesh, 1000.0, 4), replace(SimulationConfig(), device_name="cuda:0"),
+    cfg = replace(SimulationConfig(), device_name="cuda:0", grid_resolution=resolution, grid_spacing=1.0 / resolution)
+    sim = MpmSimulator(mesh, SampleParticles(mesh, 1000.0, 4), cfg,
                        MaterialConfig(model="ding2019"), initial_velocity=(0.3, -0.2, 0.1),
                        ding_config=DingConfig(yield_stress=300.0, viscosity=1e6))
     rng = np.random.default_rng(5)
@@ -38,10 +42,11 @@ def _grid(R, device):
             torch.tensor(empty + empty, dtype=torch.int32, device=device))
 
 
-def test_static_grid_substep_matches_allocated_grid_twice():
+@pytest.mark.parametrize("resolution", [40, 48])
+def test_static_grid_substep_matches_allocated_grid_twice(resolution):
     from baking_b200 import _lib
     from baking_b200.physics import substep as sub
-    sim = _scene()
+    sim = _scene(resolution)
     lib = _lib.load()
     fn = lib.bk_substep_static_grid
     fn.restype = C.c_int
@@ -72,8 +77,13 @@ def test_static_grid_substep_matches_allocated_grid_twice():
                 rc = lib.bk_substep(C.byref(params), C.byref(s_in), C.byref(s_out), C.byref(consts), C.byref(grid),
                                     None, C.byref(diag), C.byref(flags), sub.PHASE_MECHANICS, stream)
             else:
+                torch.cuda.synchronize()
+                free_before = torch.cuda.mem_get_info()[0]
                 rc = fn(C.byref(params), C.byref(s_in), C.byref(s_out), C.byref(consts), C.byref(diag), C.byref(flags),
                         stream)
+                torch.cuda.synchronize()
+                if call == 1:
+                    assert torch.cuda.mem_get_info()[0] == free_before, "the second call changed free device memory"
             assert rc == 0, lib.bk_last_error().decode()
             torch.cuda.synchronize()
             assert all(int(t.sum()) == 0 for t in flag_arrays)
@@ -112,3 +122,20 @@ def test_static_grid_rejects_oversized_grid():
             C.byref(sub.BkDiagnostics()), C.byref(sub.BkFlags()), None)
     assert rc != 0
     assert "resolution 49" in lib.bk_last_error().decode()
+
+
+@pytest.mark.parametrize("mode", ["transport", "gas"])
+def test_static_grid_rejects_transport_and_gas(mode):
+    from baking_b200 import _lib
+    from baking_b200.physics import substep as sub
+    sim = _scene()
+    lib = _lib.load()
+    fn = lib.bk_substep_static_grid
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p] * 7
+    params = sim._engine.params(False)
+    setattr(params, mode, 1)
+    rc = fn(C.byref(params), C.byref(sub.BkState()), C.byref(sub.BkState()), C.byref(sub.BkConstants()),
+            C.byref(sub.BkDiagnostics()), C.byref(sub.BkFlags()), None)
+    assert rc != 0
+    assert "mechanics nodes only" in lib.bk_last_error().decode()
