@@ -135,12 +135,16 @@ int bk_sort_by_cell(int64_t n, int64_t pitch, const float* x, const float* origi
 int bk_permute_particles(int64_t n, const int32_t* order, int32_t array_count, const BkParticleArray* arrays,
                          void* scratch, int64_t scratch_bytes, void* stream) {
     if (n < 0 || array_count < 0) return fail(BK_ERR_ARGUMENT, "bk_permute_particles: negative count");
+    if (n > INT32_MAX) return fail(BK_ERR_ARGUMENT, "bk_permute_particles: more particles than an int32 order can index");
     if (n == 0 || array_count == 0) return BK_OK;
     if (!order || !arrays || !scratch) return fail(BK_ERR_ARGUMENT, "bk_permute_particles: null argument");
+    if (((uintptr_t)scratch & 255) != 0) return fail(BK_ERR_ARGUMENT, "bk_permute_particles: scratch not 256-byte aligned");
     for (int32_t a = 0; a < array_count; ++a) {
         const BkParticleArray& arr = arrays[a];
         if (!arr.data || arr.planes < 1 || arr.pitch < n || (arr.element_bytes != 4 && arr.element_bytes != 8))
             return fail(BK_ERR_ARGUMENT, "bk_permute_particles: bad array (data, planes, pitch or element size)");
+        if (((uintptr_t)arr.data & (uintptr_t)(arr.element_bytes - 1)) != 0)
+            return fail(BK_ERR_ARGUMENT, "bk_permute_particles: array not aligned to its element size");
         if ((int64_t)arr.planes * n * arr.element_bytes > scratch_bytes)
             return fail(BK_ERR_ARGUMENT, "bk_permute_particles: scratch smaller than the largest array");
     }

@@ -52,3 +52,30 @@ def test_oracle_library_builds_and_exports():
     lib = ora.lib()
     for name in ("ora_particle_to_grid", "ora_update_ding", "ora_diffuse_grid", "ora_svd3"):
         assert hasattr(lib, name)
+
+
+def test_permute_particles_rejects_bad_arguments_before_any_device_work():
+    """Argument checks of bk_permute_particles run on the host before any CUDA call, so they are
+    exercised here without a GPU: n beyond the int32 order, scratch not 256-byte aligned and an
+    array not aligned to its element size each return BK_ERR_ARGUMENT with a message."""
+    from baking_b200 import _lib
+    lib = _lib.load()
+    fn = lib.bk_permute_particles  # bound by _lib.load() with the header's argument types
+
+    class Arr(ctypes.Structure):
+        _fields_ = [("data", ctypes.c_void_p), ("pitch", ctypes.c_int64), ("planes", ctypes.c_int32),
+                    ("element_bytes", ctypes.c_int32)]
+
+    table = (Arr * 1)()
+    table[0].data, table[0].pitch, table[0].planes, table[0].element_bytes = 4096, 1 << 20, 1, 8
+    aligned = 1 << 20
+    cases = [
+        ((2 ** 31, 256, 1, ctypes.addressof(table), aligned, 1 << 40, None), "int32"),
+        ((1000, 256, 1, ctypes.addressof(table), aligned + 8, 1 << 40, None), "256-byte"),
+    ]
+    for args, message in cases:
+        assert fn(*args) != 0
+        assert message in lib.bk_last_error().decode()
+    table[0].data = 4096 + 4
+    assert fn(1000, 256, 1, ctypes.addressof(table), aligned, 1 << 40, None) != 0
+    assert "element size" in lib.bk_last_error().decode()
