@@ -238,6 +238,185 @@ __global__ void k_step_summary_finish(const double* __restrict__ partial, double
     out[k] = v;
 }
 
+// ------------------------------------------------------------------ CheckState
+// physics/mpm.py:243-308 as one reduction; slots and their meaning are BK_CHECK_* of the header.
+constexpr int kCheckSlots = BK_CHECK_SLOTS;
+
+__host__ __device__ constexpr int check_op(int s) {
+    return s == BK_CHECK_J_MIN ? kMin
+           : (s == BK_CHECK_J_MAX || s == BK_CHECK_SPEED_MAX || s == BK_CHECK_GAS_WAVE_MAX ||
+              s == BK_CHECK_WATER_WAVE2_MAX || s == BK_CHECK_RESIDUAL_MAX || s <= BK_CHECK_TRANSPORT_FLAG1)
+                 ? kMax
+                 : kSum;
+}
+
+__device__ __forceinline__ void check_add(double* acc, int s, double v) { acc[s] = combine(check_op(s), acc[s], v); }
+
+__global__ void __launch_bounds__(kThreads) k_check_state(BkCheckInputs in, double* __restrict__ partial) {
+    double acc[kCheckSlots];
+#pragma unroll
+    for (int s = 0; s < kCheckSlots; ++s) {
+        const int op = check_op(s);
+        acc[s] = op == kMin ? INFINITY : (op == kMax ? -INFINITY : 0.0);
+    }
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t first = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t pitch = in.pitch;
+    const double inv_dx = 1.0 / (double)in.spacing;
+    const double hi = (double)in.resolution - 1.5;
+    for (int64_t i = first; i < in.n; i += stride) {
+        bool finite = true;
+        double x[3], v[3], F[9];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float xa = in.x[a * pitch + i], va = in.v[a * pitch + i];
+            finite = finite && isfinite(xa) && isfinite(va);
+            x[a] = xa;
+            v[a] = va;
+        }
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+            const float f = in.F[e * pitch + i], c = in.C[e * pitch + i];
+            finite = finite && isfinite(f) && isfinite(c);
+            F[e] = f;
+        }
+        if (!finite) check_add(acc, BK_CHECK_NONFINITE_STATE, 1.0);
+        const double J = F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) +
+                         F[2] * (F[3] * F[7] - F[4] * F[6]);
+        check_add(acc, BK_CHECK_J_MIN, J);
+        check_add(acc, BK_CHECK_J_MAX, J);
+        bool outside = false;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double g = (x[a] - (double)in.origin[a]) * inv_dx;
+            outside = outside || g < 0.5 || g >= hi;
+        }
+        if (outside) check_add(acc, BK_CHECK_OUTSIDE_STENCIL, 1.0);
+        const double speed2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        check_add(acc, BK_CHECK_SPEED_MAX, sqrt(speed2));
+        const double V0 = (double)in.reference_volume[i];
+        check_add(acc, BK_CHECK_PARTICLE_VOLUME, V0 * J);
+        const double m = in.water ? in.dry_mass[i] + in.water[i] : (double)in.mass[i];
+        check_add(acc, BK_CHECK_TOTAL_MASS, m);
+        check_add(acc, BK_CHECK_KINETIC_ENERGY, 0.5 * m * speed2);
+        const double rho = in.water ? m / V0 : (double)in.density;
+        if (in.gas_moles) {
+            const double n = (double)in.porosity[i];
+            const float T = in.temperature ? (float)in.temperature[i] : in.material_temperature[i];
+            const double p = gas_pressure(in.gas_moles[i], T, (float)J, (float)n);
+            const double bulk = p * (1.0 + (1.0 - (double)in.initial_porosity + n) / n);
+            check_add(acc, BK_CHECK_GAS_WAVE_MAX, sqrt(((double)in.gas_modulus + bulk) * J / rho));
+        }
+        if (in.water && in.water_enabled) {
+            const double sat = in.water[i] / ((double)in.water_density * V0 * J);
+            check_add(acc, BK_CHECK_WATER_WAVE2_MAX, (double)in.water_stress * sat * J / rho);
+        }
+        if (in.Fe) {
+            M3 Fe, Ff;
+            bool ok = true;
+#pragma unroll
+            for (int e = 0; e < 9; ++e) {
+                Fe.m[e] = in.Fe[e * pitch + i];
+                Ff.m[e] = (float)F[e];
+                ok = ok && isfinite(Fe.m[e]);
+            }
+            if (ok) {
+                const M3 Fp = matmul(inverse3(Fe), Ff);
+#pragma unroll
+                for (int e = 0; e < 9; ++e) ok = ok && isfinite(Fp.m[e]);
+            }
+            if (!ok) check_add(acc, BK_CHECK_NONFINITE_DING, 1.0);
+            if (in.return_residuals) check_add(acc, BK_CHECK_RESIDUAL_MAX, (double)in.return_residuals[i]);
+        }
+    }
+    if (in.node_pm && in.box) {
+        int lo[3], ext[3];
+        int64_t count = 1;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int l = max(in.box[k], 0), h = min(in.box[3 + k], in.resolution - 1);
+            lo[k] = l;
+            ext[k] = h >= l ? h - l + 1 : 0;
+            count *= ext[k];
+        }
+        const float4* pm = reinterpret_cast<const float4*>(in.node_pm);
+        for (int64_t t = first; t < count; t += stride) {
+            const int z = lo[2] + (int)(t % ext[2]);
+            const int y = lo[1] + (int)((t / ext[2]) % ext[1]);
+            const int xx = lo[0] + (int)(t / ((int64_t)ext[2] * ext[1]));
+            check_add(acc, BK_CHECK_GRID_MASS, (double)pm[node_index(xx, y, z, in.resolution)].w);
+        }
+    }
+    const int64_t vp = in.vertex_pitch;
+    for (int64_t q = first; q < in.vertex_count; q += stride) {
+        const float a = in.vertices[q], b = in.vertices[vp + q], c = in.vertices[2 * vp + q];
+        if (!(isfinite(a) && isfinite(b) && isfinite(c))) check_add(acc, BK_CHECK_NONFINITE_VERTICES, 1.0);
+    }
+    for (int64_t t = first; t < in.tet_count; t += stride) {
+        double c[4][3];
+        bool inside = true;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            int64_t q = in.tets[4 * t + k];
+            if (q < 0 || q >= in.vertex_count) {
+                inside = false;
+                q = 0;
+            }
+#pragma unroll
+            for (int a = 0; a < 3; ++a) c[k][a] = (double)in.vertices[a * vp + q];
+        }
+        double e[3][3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) e[k][a] = c[k + 1][a] - c[0][a];
+        const double vol = e[0][0] * (e[1][1] * e[2][2] - e[1][2] * e[2][1]) -
+                           e[0][1] * (e[1][0] * e[2][2] - e[1][2] * e[2][0]) +
+                           e[0][2] * (e[1][0] * e[2][1] - e[1][1] * e[2][0]);
+        if (!inside || vol <= 0.0) check_add(acc, BK_CHECK_INVERTED_TETS, 1.0);
+    }
+    __shared__ double s_warp[kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 0; s < kCheckSlots; ++s) {
+        const int op = check_op(s);
+        double v = acc[s];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = combine(op, v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) s_warp[warp] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double b = s_warp[0];
+            for (int w = 1; w < kThreads / 32; ++w) b = combine(op, b, s_warp[w]);
+            partial[(int64_t)blockIdx.x * kCheckSlots + s] = b;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_check_finish(const double* __restrict__ partial, double* __restrict__ out, int blocks,
+                               BkCheckInputs in) {
+    const int s = threadIdx.x;
+    if (s >= kCheckSlots) return;
+    const int op = check_op(s);
+    double v = partial[s];
+    for (int b = 1; b < blocks; ++b) v = combine(op, v, partial[(int64_t)b * kCheckSlots + s]);
+    if (s == BK_CHECK_SIM_FLAG0 || s == BK_CHECK_SIM_FLAG1) v = (double)in.sim_flags[s - BK_CHECK_SIM_FLAG0];
+    if (s >= BK_CHECK_DING_FLAG0 && s <= BK_CHECK_DING_FLAG2)
+        v = in.ding_flags ? (double)in.ding_flags[s - BK_CHECK_DING_FLAG0] : 0.0;
+    if (s == BK_CHECK_TRANSPORT_FLAG0 || s == BK_CHECK_TRANSPORT_FLAG1)
+        v = in.transport_flags ? (double)in.transport_flags[s - BK_CHECK_TRANSPORT_FLAG0] : 0.0;
+    if (s == BK_CHECK_RESIDUAL_MAX) {
+        if (in.max_residuals) v = fmax(v, (double)in.max_residuals[0]);
+        if (!in.Fe) v = 0.0;
+        v = fmax(v, 0.0);
+    }
+    if ((s == BK_CHECK_GAS_WAVE_MAX && !in.gas_moles) || (s == BK_CHECK_WATER_WAVE2_MAX && !(in.water && in.water_enabled)))
+        v = 0.0;
+    if (in.n == 0 && (s == BK_CHECK_J_MIN || s == BK_CHECK_J_MAX || s == BK_CHECK_SPEED_MAX)) v = 0.0;
+    out[s] = v;
+}
+
 }  // namespace
 
 extern "C" int bk_step_summary(const BkSubstepParams* params, const BkState* state, const BkConstants* constants,
@@ -278,4 +457,27 @@ extern "C" int bk_measure_state(const BkMeasureInputs* in, double* out, double* 
     k_measure_finish<<<1, 64, 0, s>>>(scratch, out, BK_MEASURE_BLOCKS, m.porosity != nullptr, m.gas_moles != nullptr,
                                       m.temperature != nullptr, m.vertex_count > 0);
     return check_launch("bk_measure_state/finish");
+}
+
+extern "C" int bk_check_state(const BkCheckInputs* in, double* out, double* scratch, void* stream) {
+    if (!in || !out || !scratch) return fail(BK_ERR_ARGUMENT, "bk_check_state: null argument");
+    const BkCheckInputs& c = *in;
+    if (c.n < 0 || c.vertex_count < 0 || c.tet_count < 0 || !c.sim_flags)
+        return fail(BK_ERR_ARGUMENT, "bk_check_state: bad counts or missing flags");
+    if (c.n > 0 && (c.pitch < c.n || !c.x || !c.v || !c.F || !c.C || !c.reference_volume ||
+                    (c.water ? !c.dry_mass : !c.mass)))
+        return fail(BK_ERR_ARGUMENT, "bk_check_state: bad particle arrays");
+    if (c.gas_moles && (!c.porosity || !(c.temperature || c.material_temperature)))
+        return fail(BK_ERR_ARGUMENT, "bk_check_state: gas arrays incomplete");
+    if (!(c.spacing > 0.0f) || c.resolution < 1) return fail(BK_ERR_ARGUMENT, "bk_check_state: bad grid");
+    if (c.node_pm && (!c.box || ((uintptr_t)c.node_pm & 15) != 0))
+        return fail(BK_ERR_ARGUMENT, "bk_check_state: grid needs its active box and 16-byte alignment");
+    if (c.vertex_count > 0 && (!c.vertices || c.vertex_pitch < c.vertex_count))
+        return fail(BK_ERR_ARGUMENT, "bk_check_state: bad vertex array");
+    if (c.tet_count > 0 && (!c.tets || c.vertex_count == 0)) return fail(BK_ERR_ARGUMENT, "bk_check_state: bad tets");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    k_check_state<<<BK_MEASURE_BLOCKS, kThreads, 0, s>>>(c, scratch);
+    if (int rc = check_launch("bk_check_state")) return rc;
+    k_check_finish<<<1, 32, 0, s>>>(scratch, out, BK_MEASURE_BLOCKS, c);
+    return check_launch("bk_check_state/finish");
 }

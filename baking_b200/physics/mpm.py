@@ -23,7 +23,6 @@ import numpy as np
 import torch
 
 from .. import _lib, arrays
-from ..geometry import ComputeSignedVolumes
 from ..geometry.mesh_tracking import ParticleMeshBinding
 from .grid import GridState
 from .materials.ding import DingMaterial
@@ -474,10 +473,19 @@ class MpmSimulator:
         start = self.step_count
         for _ in range(step_count):
             self._substep(check=self.IsSettling)
-        messages = self._device_flag_messages()
+        values = self._check_values()
+        messages = []
+        if isinstance(self.material, DingMaterial):
+            m = self.material.FlagMessage([values["ding_flag0"], values["ding_flag1"], values["ding_flag2"]])
+            if m:
+                messages.append(m)
+        if self.transport is not None:
+            m = self.transport.FlagMessage([values["transport_flag0"], values["transport_flag1"]])
+            if m:
+                messages.append(m)
         if messages:
             raise RuntimeError(messages[0] + f" (flag raised within substeps {start + 1}..{self.step_count})")
-        return self.CheckState()
+        return self.CheckState(values)
 
     def AdvanceUnchecked(self, step_count):
         """Run substeps with no host synchronisation; flags stay on the device until CheckState/Advance."""
@@ -500,67 +508,60 @@ class MpmSimulator:
             self.mesh_binding.Reconstruct(self.current_state, self.vertex_positions)
             self.mesh_step_count = self.step_count
 
-    def CheckState(self):
-        flags = self.error_flags.tolist()
-        if flags[0]:
+    def _check_values(self):
+        """Every input of CheckState from one device reduction over the current state, the mesh
+        vertices and the grid (bk_check_state), read back in one small copy."""
+        self.UpdateMesh()
+        return self._engine.check_state(self._current)
+
+    def CheckState(self, values=None):
+        """physics/mpm.py:243-308: the same checks, messages and returned summary. ``values`` are the
+        reduction's results when the caller already has them (Advance)."""
+        v = self._check_values() if values is None else values
+        if v["sim_flag0"]:
             raise RuntimeError("nonpositive/nonfinite J; reduce dt or inspect loading and sampling")
-        if flags[1]:
+        if v["sim_flag1"]:
             raise RuntimeError("particle stencil left the grid; enlarge the domain or reduce dt")
-        st = self.current_state
-        x = st.particle_positions.double()
-        v = st.particle_velocities.double()
-        F = st.deformation_gradients.double()
-        Cm = st.affine_velocities
-        if not all(bool(torch.isfinite(a).all()) for a in (x, v, F, Cm)):
+        if v["nonfinite_state"]:
             raise RuntimeError("nonfinite particle state; simulation stopped")
-        J = torch.linalg.det(F)
-        if float(J.min()) <= 0.0:
+        if v["j_min"] <= 0.0:
             raise RuntimeError("inverted particle deformation; reduce dt or loading")
-        sim = self.simulation_config
-        gpos = (x - torch.tensor(sim.grid_origin, device=x.device, dtype=x.dtype)) / sim.grid_spacing
-        if bool((gpos < 0.5).any()) or bool((gpos >= sim.grid_resolution - 1.5).any()):
+        if v["outside_stencil"]:
             raise RuntimeError("particle outside valid grid stencil")
-        masses = self.Masses().double()
-        vmax = float(torch.linalg.norm(st.particle_velocities.double(), dim=1).max())
+        sim = self.simulation_config
+        vmax = v["speed_max"]
         wave = self.material.material_config.wave_speed
         if isinstance(self.material, DingMaterial) and self.material.ding_config.gas_enabled:
-            wave = max(wave, self.material.GasWaveSpeed(st))
+            wave = max(wave, v["gas_wave_max"])
         if self.transport is not None and self.transport.config.water_enabled:
-            ww = (self.transport.config.water_stress * st.transport_state.saturations * J
-                  / st.material_state.reference_densities.double())
-            wave = float(math.sqrt(wave * wave + float(ww.max())))
+            wave = float(math.sqrt(wave * wave + v["water_wave2_max"]))
         cfl = (vmax + wave) * sim.time_step / sim.grid_spacing
         if cfl > sim.cfl_limit:
             raise RuntimeError(f"estimated CFL={cfl:.3f} > {sim.cfl_limit}; reduce dt")
         if isinstance(self.material, DingMaterial):
-            self.material.CheckState()
-            ms = st.material_state
-            if not bool(torch.isfinite(ms.elastic_gradients).all()) or not bool(torch.isfinite(ms.plastic_gradients).all()):
+            message = self.material.FlagMessage([v["ding_flag0"], v["ding_flag1"], v["ding_flag2"]])
+            if message:
+                raise RuntimeError(message)
+            if v["nonfinite_ding"]:
                 raise RuntimeError("nonfinite Ding internal state")
-            worst = (float(ms.return_residuals.max()) if self.diagnostics == "full"
-                     else self.MaxReturnResiduals()[0])
-            if worst > 1e-4:
+            if v["residual_max"] > 1e-4:
                 raise RuntimeError("Ding local return mapping did not converge")
-        self.UpdateMesh()
-        vertices = arrays.to_numpy(self.vertex_positions)
-        if not np.isfinite(vertices).all():
+        if v["nonfinite_vertices"]:
             raise RuntimeError("nonfinite reconstructed mesh vertices")
-        volumes = torch.as_tensor(self.particle_samples.reference_volumes, device=J.device, dtype=torch.float64)
         return {
             "step_count": self.step_count,
             "simulation_time": self.step_count * sim.time_step,
             "particle_count": self.particle_data.particle_count,
-            "particle_volume_m3": float(torch.dot(volumes, J)),
-            "total_mass": float(masses.sum()),
-            "grid_mass": float(self.grid_state.node_masses.double().sum()),
-            "minimum_j": float(J.min()),
-            "maximum_j": float(J.max()),
+            "particle_volume_m3": v["particle_volume"],
+            "total_mass": v["total_mass"],
+            "grid_mass": v["grid_mass"],
+            "minimum_j": v["j_min"],
+            "maximum_j": v["j_max"],
             "maximum_speed": vmax,
-            "kinetic_energy": float(0.5 * torch.sum(masses * torch.sum(v * v, dim=1))),
+            "kinetic_energy": v["kinetic_energy"],
             "estimated_cfl": cfl,
             "unmapped_mesh_vertices": self.mesh_binding.unmapped_vertex_count,
-            "inverted_mesh_tets": int(np.count_nonzero(ComputeSignedVolumes(vertices.astype(np.float64),
-                                                                            self.tet_mesh.tet_indices) <= 0.0)),
+            "inverted_mesh_tets": int(v["inverted_tets"]),
         }
 
     # ------------------------------------------------------------ snapshots

@@ -71,7 +71,27 @@ class BkSubstepParams(C.Structure):
 PHASE_TRANSPORT = 1
 PHASE_MECHANICS = 2
 
+class BkCheckInputs(C.Structure):
+    _fields_ = [("n", C.c_int64), ("pitch", C.c_int64), ("x", P), ("v", P), ("F", P), ("C", P),
+                ("reference_volume", P), ("mass", P), ("dry_mass", P), ("water", P), ("temperature", P),
+                ("material_temperature", P), ("Fe", P), ("porosity", P), ("gas_moles", P),
+                ("return_residuals", P), ("max_residuals", P), ("sim_flags", P), ("ding_flags", P),
+                ("transport_flags", P), ("origin", C.c_float * 3), ("spacing", C.c_float),
+                ("resolution", C.c_int32), ("water_enabled", C.c_int32), ("density", C.c_float),
+                ("water_density", C.c_float), ("water_stress", C.c_float), ("gas_modulus", C.c_float),
+                ("initial_porosity", C.c_float), ("node_pm", P), ("box", P), ("vertex_count", C.c_int64),
+                ("vertex_pitch", C.c_int64), ("vertices", P), ("tet_count", C.c_int64), ("tets", P)]
+
+
+# Slots of bk_check_state (include/baking_b200.h, BK_CHECK_*).
+CHECK_SLOTS = ("sim_flag0", "sim_flag1", "ding_flag0", "ding_flag1", "ding_flag2", "transport_flag0",
+               "transport_flag1", "nonfinite_state", "j_min", "j_max", "outside_stencil", "speed_max", "gas_wave_max",
+               "water_wave2_max", "nonfinite_ding", "residual_max", "particle_volume", "total_mass", "kinetic_energy",
+               "grid_mass", "nonfinite_vertices", "inverted_tets")
+CHECK_BLOCKS = 296
+
 _SIGS = {
+    "bk_check_state": [P, P, P, P],
     "bk_substep": [P] * 8 + [C.c_int32, P],
     "bk_materialize": [P] * 11 + [P],
     "bk_surface_accumulate": [P, C.c_float, P, P, P],
@@ -301,6 +321,57 @@ class SubstepEngine:
                       C.byref(self.grid), out.data_ptr() if out_ptr is None else out_ptr,
                       self._summary_scratch.data_ptr(), _lib.stream_handle())
         return out
+
+    def check_state(self, state):
+        """CheckState's inputs (the CHECK_SLOTS values) for ``state``, the simulator's vertex positions
+        and grid, from one device reduction (bk_check_state) and one copy to the host."""
+        sim = self.sim
+        dev = sim.device
+        if getattr(self, "_check_out", None) is None:
+            self._check_out = torch.zeros(len(CHECK_SLOTS), dtype=torch.float64, device=dev)
+            self._check_scratch = torch.empty(CHECK_BLOCKS * len(CHECK_SLOTS), dtype=torch.float64, device=dev)
+            self._check_tets = torch.as_tensor(np.ascontiguousarray(sim.tet_mesh.tet_indices, dtype=np.int32),
+                                               device=dev)
+        c = BkCheckInputs()
+        c.n = sim.particle_data.particle_count
+        c.pitch = arrays.layout_pitch(state.deformation_gradients)
+        c.x, c.v = _p(state.particle_positions), _p(state.particle_velocities)
+        c.F, c.C = _p(state.deformation_gradients), _p(state.affine_velocities)
+        c.reference_volume = _p(sim.particle_data.reference_volumes)
+        c.mass = _p(sim.particle_data.particle_masses)
+        c.sim_flags = _p(sim.error_flags)
+        mc = sim.material.material_config
+        c.density = mc.density
+        if self.transport:
+            ts = state.transport_state
+            c.water, c.dry_mass, c.temperature = _p(ts.water_masses), _p(sim.transport.dry_masses), _p(ts.temperatures)
+            c.transport_flags = _p(sim.transport.error_flags)
+            tc = sim.transport.config
+            c.water_enabled = int(tc.water_enabled)
+            c.water_density, c.water_stress = tc.water_density, tc.water_stress
+        if self.is_ding:
+            ms = state.material_state
+            c.Fe, c.ding_flags = _p(ms.elastic_gradients), _p(sim.material.error_flags)
+            if not self.transport:
+                c.material_temperature = _p(ms.temperatures)
+            if self.gas:
+                c.porosity, c.gas_moles = _p(ms.porosities), _p(ms.gas_moles)
+                c.gas_modulus = mc.lame_lambda + 2.0 * mc.shear_modulus
+                c.initial_porosity = sim.material.ding_config.porosity
+            if sim.diagnostics == "full":
+                c.return_residuals = _p(ms.return_residuals)
+            c.max_residuals = _p(self.max_residuals)
+        cfg = sim.simulation_config
+        for a in range(3):
+            c.origin[a] = cfg.grid_origin[a]
+        c.spacing, c.resolution = cfg.grid_spacing, cfg.grid_resolution
+        c.node_pm, c.box = _p(self.node_pm), self.bounds.data_ptr() + 6 * 4  # the last substep's box
+        verts = sim.vertex_positions
+        c.vertex_count, c.vertex_pitch, c.vertices = verts.shape[0], arrays.layout_pitch(verts), _p(verts)
+        c.tet_count, c.tets = self._check_tets.shape[0], _p(self._check_tets)
+        _lib.call_raw(self.lib.bk_check_state, "bk_check_state", C.byref(c), _p(self._check_out),
+                      _p(self._check_scratch), _lib.stream_handle())
+        return dict(zip(CHECK_SLOTS, self._check_out.tolist()))
 
     def accumulate_surface(self, transport_state):
         if not self.transport or self.surface.owner_count == 0:

@@ -307,9 +307,12 @@ BK_API int bk_substep(const BkSubstepParams *params, const BkState *in, BkState 
    allocates and frees nothing. It has no counterpart in the reference. Limits: neo-Hookean or
    Ding without transport or gas, grid resolution 4..48 (48^3 nodes, about 3.4 MB held on every
    GPU that loads the library until exit); larger grids return BK_ERR_ARGUMENT with a message.
-   The first call on each device looks up the array's device address (make it before any stream
-   capture). All calls on a device share the array and each call clears it first, so calls that
-   overlap on the GPU race and must be serialised by the caller. */
+   Every call looks up the array's device address in the current CUDA context, primary or not.
+   Under lazy module loading (the default since CUDA 12.2) the first call in each context loads
+   the module, which reserves the array's memory: make that first call at start-up, before any
+   stream capture, so that no later call allocates. All calls on a device share the array and
+   each call clears it first, so calls that overlap on the GPU race and must be serialised by the
+   caller. */
 BK_API int bk_substep_static_grid(const BkSubstepParams *params, const BkState *in, BkState *out,
                                   const BkConstants *constants, BkDiagnostics *diagnostics, BkFlags *flags,
                                   void *stream);
@@ -509,6 +512,63 @@ BK_API int64_t bk_sort_by_cell_scratch_bytes(int64_t n, int32_t resolution);
 BK_API int bk_sort_by_cell(int64_t n, int64_t pitch, const float *x, const float *origin, float dx,
                            int32_t resolution, int32_t *order, void *scratch, int64_t scratch_bytes, void *stream);
 
+/* CheckState (physics/mpm.py:243-308 with physics/materials/ding.py:294-301) as one device
+   reduction: the particle-state checks, the inputs of the CFL estimate and the values CheckState
+   returns, plus copies of the simulation, Ding and transport flag words, in BK_CHECK_SLOTS doubles. The host
+   raises the reference's messages from them after one small device-to-host copy. */
+enum {
+    BK_CHECK_SIM_FLAG0 = 0, BK_CHECK_SIM_FLAG1,      /* simulation flags [0] (J), [1] (stencil) */
+    BK_CHECK_DING_FLAG0, BK_CHECK_DING_FLAG1, BK_CHECK_DING_FLAG2,  /* Ding flags (porosity, return, gas CFL) */
+    BK_CHECK_TRANSPORT_FLAG0, BK_CHECK_TRANSPORT_FLAG1,             /* transport flags (heat, water stability) */
+    BK_CHECK_NONFINITE_STATE,        /* particles with a nonfinite x, v, F or C */
+    BK_CHECK_J_MIN, BK_CHECK_J_MAX,  /* det F in float64 */
+    BK_CHECK_OUTSIDE_STENCIL,        /* particles with a grid coordinate < 0.5 or >= R - 1.5 */
+    BK_CHECK_SPEED_MAX,              /* max |v| */
+    BK_CHECK_GAS_WAVE_MAX,           /* gas mode: max sqrt((K + p (1 + (1 - n0 + n) / n)) J / rho_ref) */
+    BK_CHECK_WATER_WAVE2_MAX,        /* transport with water: max water_stress s J / rho_ref */
+    BK_CHECK_NONFINITE_DING,         /* Ding: particles with a nonfinite Fe or Fp = Fe^-1 F */
+    BK_CHECK_RESIDUAL_MAX,           /* Ding: largest return residual */
+    BK_CHECK_PARTICLE_VOLUME,        /* sum V0 det F */
+    BK_CHECK_TOTAL_MASS,             /* sum of particle masses */
+    BK_CHECK_KINETIC_ENERGY,         /* sum 1/2 m |v|^2 */
+    BK_CHECK_GRID_MASS,              /* node masses of the last substep's active box */
+    BK_CHECK_NONFINITE_VERTICES,     /* mesh vertices with a nonfinite coordinate */
+    BK_CHECK_INVERTED_TETS,          /* tets with signed volume <= 0 (or a vertex index out of range) */
+    BK_CHECK_SLOTS
+};
+
+typedef struct {
+    int64_t n, pitch;
+    const float *x, *v, *F, *C;           /* state planes (device) */
+    const float *reference_volume;        /* V0 */
+    const float *mass;                    /* particle masses without transport, else NULL */
+    const double *dry_mass, *water;       /* transport: mass = dry + W, rho_ref = mass / V0 */
+    const double *temperature;            /* transport temperatures (gas pressure), else NULL */
+    const float *material_temperature;    /* Ding without transport (gas pressure), else NULL */
+    const float *Fe;                      /* Ding elastic gradients, else NULL */
+    const float *porosity;                /* gas mode, else NULL */
+    const double *gas_moles;              /* gas mode, else NULL */
+    const float *return_residuals;        /* per-particle residuals, or NULL */
+    const float *max_residuals;           /* the substep's max residual (1 float), or NULL */
+    const int32_t *sim_flags;             /* 2 ints */
+    const int32_t *ding_flags;            /* 3 ints, or NULL */
+    const int32_t *transport_flags;       /* 2 ints, or NULL */
+    float origin[3], spacing;
+    int32_t resolution;
+    int32_t water_enabled;
+    float density, water_density, water_stress, gas_modulus, initial_porosity;  /* gas_modulus = lambda + 2 mu */
+    const float *node_pm;                 /* grid (px, py, pz, m) float4 nodes, or NULL */
+    const int32_t *box;                   /* the last substep's active box (6 ints: lo, hi) */
+    int64_t vertex_count, vertex_pitch;
+    const float *vertices;                /* 3 planes of vertex_pitch floats */
+    int64_t tet_count;
+    const int32_t *tets;                  /* tet_count x 4 vertex ids */
+} BkCheckInputs;
+
+/* out: BK_CHECK_SLOTS doubles (device); scratch: BK_MEASURE_BLOCKS * BK_CHECK_SLOTS doubles (device).
+   Two launches (block partials, then a fixed-order finish), deterministic. */
+BK_API int bk_check_state(const BkCheckInputs *in, double *out, double *scratch, void *stream);
+
 /* One per-particle array for bk_permute_particles: `planes` planes of n elements of
    `element_bytes` (4 or 8) bytes, `pitch` elements apart, starting at `data` (device). */
 typedef struct {
@@ -519,9 +579,9 @@ typedef struct {
 } BkParticleArray;
 
 /* In place, for every array: element k of each plane becomes the element order[k] had. `arrays`
-   is a HOST table of `array_count` entries; order: n int32 (device), a permutation; scratch:
-   device, at least planes * n * element_bytes bytes of the largest array. Arrays must not overlap
-   one another. One gather kernel and one 2-D copy per array, in order on `stream`. */
+   is a HOST table of `array_count` entries, each array aligned to its element size; order: n
+   int32 (device), a permutation, so n <= INT32_MAX; scratch: device, 256-byte aligned, at least
+   planes * n * element_bytes bytes of the largest array. Arrays must not overlap one another. One gather kernel and one 2-D copy per array, in order on `stream`. */
 BK_API int bk_permute_particles(int64_t n, const int32_t *order, int32_t array_count, const BkParticleArray *arrays,
                                 void *scratch, int64_t scratch_bytes, void *stream);
 
