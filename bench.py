@@ -42,6 +42,21 @@ UNIT = "particle-substeps/s"
 # float64 scattered fields write+read 112, node temperature/saturation 32, dT/dW 32).
 BYTES_PER_PARTICLE = 404
 BYTES_PER_ACTIVE_NODE = 232
+# Forward + backward (Rollout with a checkpoint every k substeps), algorithmic bytes per
+# particle-substep: the forward substep (404), its recomputation from the checkpoint in the reverse
+# sweep (404), the reverse kernels' read of the substep's input state (204), the adjoint of every
+# state array read once and written once at the state's precision (204 + 200), and the checkpoint
+# written in the forward and read back for the recomputation (2 x 200 / k). Per active node: the
+# forward and recomputed grid passes (2 x 232) and the node adjoints of momentum, mass, velocity and
+# the transport fields written and read once (232).
+FWD_BWD_CHECKPOINT_EVERY = 8
+BYTES_PER_ACTIVE_NODE_FWD_BWD = 3 * 232
+
+
+def bytes_per_particle_fwd_bwd(every=FWD_BWD_CHECKPOINT_EVERY):
+    return 404 + 404 + 204 + 404 + 2 * 200 / every  # 1466 B at a checkpoint every 8 substeps
+
+CLOCK_WINDOW_S = 1.0
 
 
 def parse():
@@ -54,6 +69,9 @@ def parse():
     p.add_argument("--resolution", type=int, default=128)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-variants", action="store_true", help="skip the surrogate and fwd+bwd forms")
+    p.add_argument("--clock-window", type=float, default=CLOCK_WINDOW_S,
+                   help="seconds of untimed substeps (on a second copy of the loaf) sampled for clocks before "
+                        "the timed region; 0 skips them (profiling runs)")
     p.add_argument("--rollout-only", type=int, nargs=2, metavar=("STEPS", "EVERY"), default=None,
                    help="time only forward + adjoint of STEPS substeps, a checkpoint every EVERY, on the "
                         "headline loaf (for profiling the reverse sweep)")
@@ -61,18 +79,71 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+    """SM clock and clock-event (throttle) reasons of one GPU, sampled through NVML every
+    ``interval`` seconds on a host thread while the block runs (NVML is what nvidia-smi reads; a
+    direct query takes well under a millisecond, so even a timed region of a few milliseconds gets
+    samples). Falls back to ``nvidia-smi -lms 100`` when NVML cannot be loaded."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, interval=0.002):
         self.index = index
+        self.interval = interval
         self.proc = None
         self.lines = []
+        self.samples = []  # (seconds since start, sm MHz, max sm MHz, set of reason names)
+        self._stop = threading.Event()
+        self._nvml = None
+        self._handle = None
+
+    def _open_nvml(self):
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            props = torch.cuda.get_device_properties(self.index)
+            handle = None
+            uuid = str(getattr(props, "uuid", ""))
+            if uuid:
+                try:
+                    handle = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+                except pynvml.NVMLError:
+                    handle = None
+            if handle is None:
+                bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+                handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self._nvml, self._handle = pynvml, handle
+            return True
+        except Exception:  # noqa: BLE001 -- any NVML failure selects the nvidia-smi path
+            self._nvml = None
+            return False
+
+    def _poll_nvml(self):
+        nv, h = self._nvml, self._handle
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        t0 = time.perf_counter()
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except Exception:  # noqa: BLE001
+                break
+            self.samples.append((time.perf_counter() - t0, float(sm), float(smax),
+                                 {k for k, b in bits.items() if mask & b}))
+            self._stop.wait(self.interval)
 
     def __enter__(self):
+        if self._open_nvml():
+            self.thread = threading.Thread(target=self._poll_nvml, daemon=True)
+            self.thread.start()
+            return self
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "100", "-i", str(self.index)], stdout=subprocess.PIPE,
@@ -88,6 +159,10 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        self._stop.set()
+        if self._nvml is not None:
+            self.thread.join(timeout=5)
+            return
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -95,9 +170,16 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
+    def mark(self):
+        """Index of the next sample (to summarise a part of the sampled window)."""
+        return len(self.samples)
+
+    def summary(self, first=0, last=None):
         sm, smax, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for _, clock, top, active in self.samples[first:last]:
+            sm.append(clock)
+            smax = max(smax, top)
+            reasons |= active
         for line in self.lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 8:
@@ -107,11 +189,12 @@ class ClockSampler:
                 smax = max(smax, float(parts[1]))
             except ValueError:
                 continue
-            for name, flag in zip(names, parts[4:8]):
+            for name, flag in zip(self.NAMES, parts[4:8]):
                 if flag.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self._nvml is not None else "nvidia-smi"}
 
 
 def load_peaks():
@@ -154,8 +237,16 @@ def cpu_baseline_sample(scene, seconds=20.0, max_steps=50):
             break
     elapsed = time.perf_counter() - start
     n = scene.particle_count
+    # The same oracle on one host thread, one substep (about 5 s at 1M particles).
+    ora.set_threads(1)
+    t1 = time.perf_counter()
+    sim.Step()
+    one = time.perf_counter() - t1
+    ora.set_threads(threads)
     return {"value": n * steps / elapsed, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{steps} substeps of the {n}-particle loaf after 1 warm-up substep ({elapsed:.1f} s)"}
+            "sample": f"{steps} substeps of the {n}-particle loaf after 1 warm-up substep ({elapsed:.1f} s)",
+            "single_core": {"value": n / one, "unit": UNIT, "cores": 1,
+                            "sample": f"1 substep of the same loaf on one thread ({one:.1f} s)"}}
 
 
 def run_reference(args):
@@ -171,7 +262,7 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     ora.set_threads(threads)
     sim = make_simulator(scene, engine=OracleSimulator)
-    for _ in range(min(args.warmup, 1)):
+    for _ in range(args.warmup):
         sim.Step()
     budget = 90.0
     steps, start = 0, time.perf_counter()
@@ -183,7 +274,7 @@ def run_reference(args):
     elapsed = time.perf_counter() - start
     value = scene.particle_count * steps / elapsed
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * elapsed / steps,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": f"box loaf, {scene.particle_count} particles, {args.resolution}^3 grid, "
                                    "Ding+gas+thermal-water, dt=5e-5", "inputs": "larger than L2"},
@@ -244,14 +335,28 @@ def main():
     kernel_events = _lib.KernelTimer(only=dominant_name)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
+        # Clock window: a second copy of the loaf runs the same substeps for CLOCK_WINDOW_S seconds
+        # under the sampler just before the timed region, so the clock record covers sustained load
+        # even when the timed region lasts milliseconds; the timed loaf's state is untouched by it.
+        if args.clock_window > 0:
+            window_sim = make_simulator(scene, diagnostics="lean")
+            torch.cuda.synchronize()
+            t_window = time.perf_counter()
+            while time.perf_counter() - t_window < args.clock_window:
+                window_sim.AdvanceUnchecked(25)
+                torch.cuda.synchronize()
+            del window_sim
+        sim.AdvanceUnchecked(1)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
+        timed_first = clocks.mark()
         with kernel_events:
             start.record(stream)
             sim.AdvanceUnchecked(args.steps)
             end.record(stream)
         torch.cuda.synchronize()
+        timed_last = clocks.mark()
     elapsed = start.elapsed_time(end) / 1e3
     elapsed = reduce_max(elapsed, dist)
     sim.CheckState()
@@ -332,7 +437,9 @@ def main():
             "e2e": {"value": world * n * e2e_steps / e2e_elapsed, "unit": UNIT,
                     "h2d_bytes_per_step": int(host_rates.numel() * 4), "d2h_bytes_per_step": int(result_bytes()),
                     "steps": e2e_steps},
-            "clocks": clocks.summary()}
+            "clocks": dict(clocks.summary(), timed_region=clocks.summary(timed_first, timed_last),
+                           window=f"{args.clock_window:.1f} s of the same substeps on a second copy of the "
+                                  "loaf, one untimed substep, then the timed region")}
     if not args.no_variants:
         del sim
         line["variants"] = variants(args, rank, dist)
@@ -347,6 +454,18 @@ def main():
 
 def result_bytes():
     return 2 * 8
+
+
+def step_roofline(particles, active_nodes, steps, seconds, per_particle=BYTES_PER_PARTICLE,
+                  per_node=BYTES_PER_ACTIVE_NODE):
+    """Whole-substep roofline: algorithmic bytes (per particle and per active node) moved per second
+    against the HBM peak."""
+    peak, kind = load_peaks()
+    step_bytes = particles * per_particle + active_nodes * per_node
+    achieved = step_bytes * steps / seconds / 1e9
+    return {"bound": "hbm", "bytes_per_step": int(step_bytes), "bytes_per_particle": per_particle,
+            "bytes_per_active_node": per_node, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": kind}
 
 
 def reduce_max(value, dist):
@@ -393,6 +512,7 @@ def batched(args, rank, dist, net, count=64, steps=200):
     exact = BatchedSimulators(sims).capture()
     RestoreStates(sims, saved)
     t_exact, _ = _timed(lambda: exact.Advance(steps), dist, stream)
+    active = sum(active_node_count(s) for s in sims)
     t_launch, _ = _timed(lambda: exact.Advance(20, graph=False), dist, stream)
     exact.CheckState()
     del exact
@@ -408,10 +528,12 @@ def batched(args, rank, dist, net, count=64, steps=200):
     return {"value": world * n * steps / t_exact, "unit": UNIT, "surrogate": world * n * steps / t_sur,
             "without_graph": world * n * 20 / t_launch, "instances": count, "particles": n, "steps": steps,
             "surrogate_paths": dict(zip(("elastic", "surrogate", "exact_yielding"), paths)),
+            "roofline": step_roofline(n, active, steps, t_exact),
+            "surrogate_roofline": step_roofline(n, active, steps, t_sur),
             "scene": "dough balls (loaf dough: Ding + gas + thermal-water), dt 5e-5, one CUDA graph per 2 substeps"}
 
 
-def rollout_variant(sim, dist, stream, world, scene, fb_steps=64, every=8):
+def rollout_variant(sim, dist, stream, world, scene, fb_steps=64, every=FWD_BWD_CHECKPOINT_EVERY):
     """Forward + hand-written adjoint of ``fb_steps`` substeps with a checkpoint every ``every``
     (Rollout): loss = mean squared distance of the final positions to the initial cloud scaled by
     1.2 about its centre; gradients with respect to the per-particle initial temperatures and gas
@@ -449,8 +571,12 @@ def rollout_variant(sim, dist, stream, world, scene, fb_steps=64, every=8):
     t_fb, _ = _timed(rollouts, dist, stream)
     t_fb /= repeats
     t_f, _ = _timed(lambda: sim.AdvanceUnchecked(fb_steps), dist, stream)
+    active = active_node_count(sim)
     finite = all(bool(torch.isfinite(t.grad).all()) for t in (T0, rates, E0))
     out = {"value": world * n * fb_steps / t_fb, "unit": UNIT, "forward_only": world * n * fb_steps / t_f,
+           "forward_over_fwd_bwd": t_fb / t_f,
+           "roofline": step_roofline(n, active, fb_steps, t_fb, bytes_per_particle_fwd_bwd(every),
+                                     BYTES_PER_ACTIVE_NODE_FWD_BWD),
            "ms_per_substep": 1e3 * t_fb / fb_steps, "steps": fb_steps, "checkpoint_every": every,
            "rollouts_timed": repeats,
            "gradients": ["transport_temperatures", "gas_source_rates", "young_modulus"],
@@ -490,15 +616,18 @@ def variants(args, rank, dist):
             sur.reset_statistics()
         t, _ = _timed(lambda: sim.AdvanceUnchecked(steps), dist, stream)
         sim.CheckState()
-        results[mode] = (t, sim.current_state.particle_positions.double().clone(), sur.statistics() if sur else None)
+        results[mode] = (t, sim.current_state.particle_positions.double().clone(), sur.statistics() if sur else None,
+                         active_node_count(sim))
         del sim
-    (te, xe, _), (ts, xs, stats) = results["exact"], results["surrogate"]
+    (te, xe, _, ae), (ts, xs, stats, asur) = results["exact"], results["surrogate"]
     x0 = torch.as_tensor(loaf.samples.particle_positions, device=xe.device)
     moved = float((xe - x0).norm(dim=1).max())
     dev = float((xs - xe).norm(dim=1).max())
     out["surrogate"] = {"value": world * n * steps / ts, "unit": UNIT, "exact_same_scene": world * n * steps / te,
                         "speedup": te / ts, "steps": steps, "paths": stats,
                         "max_position_deviation_m": dev, "deviation_over_max_displacement": dev / moved,
+                        "roofline": step_roofline(n, asur, steps, ts),
+                        "exact_roofline": step_roofline(n, ae, steps, te),
                         "scene": f"box loaf {n} particles, {args.resolution}^3, 318 K, prestrain 0.08, gas + transport"}
     del results, xe, xs
     # forward + backward
@@ -510,8 +639,45 @@ def variants(args, rank, dist):
         make_simulator(sphere, diagnostics="lean"), dist, stream, world,
         f"dough sphere {sphere.particle_count} particles, 64^3, Ding + gas + thermal-water")
     out["batched"] = batched(args, rank, dist, net)
+    out["config4"] = config4_variant(args, rank, dist, stream, world, net)
     out["cell_order"] = cell_order_variant(args, rank, dist, stream, world)
     return out
+
+
+def config4_variant(args, rank, dist, stream, world, net, particles=4_000_000, resolution=256, steps=500):
+    """The learned return map deployed at scale: a 4M-particle box loaf on a 256^3 grid for 500
+    substeps, part-baked (318 K) and pre-stressed (prestrain 0.08) so that the return map yields
+    everywhere, with the surrogate attached (out-of-range particles take the exact map) and the exact
+    map on the same substeps from the same state; path counts, the judge's largest log-strain error
+    (one warp in 64 re-evaluated by the exact map) and the final position deviation."""
+    import torch
+    from baking_b200.scenes import box_loaf, make_simulator
+    from baking_b200.surrogate import ReturnMapSurrogate
+    loaf = box_loaf(resolution, particles, seed=rank, initial_temperature=318.15, prestrain=0.08)
+    n = loaf.particle_count
+    results = {}
+    for mode in ("exact", "surrogate"):
+        sim = make_simulator(loaf, diagnostics="lean")
+        sur = ReturnMapSurrogate(net, judge_stride=64).attach(sim) if mode == "surrogate" else None
+        sim.AdvanceUnchecked(3)
+        if sur:
+            sur.reset_statistics()
+        t, _ = _timed(lambda: sim.AdvanceUnchecked(steps), dist, stream)
+        sim.CheckState()
+        results[mode] = (t, sim.current_state.particle_positions.double().clone(),
+                         sur.statistics() if sur else None, active_node_count(sim))
+        del sim, sur
+        torch.cuda.empty_cache()
+    (te, xe, _, ae), (ts, xs, stats, asur) = results["exact"], results["surrogate"]
+    x0 = torch.as_tensor(loaf.samples.particle_positions, device=xe.device)
+    moved = float((xe - x0).norm(dim=1).max())
+    dev = float((xs - xe).norm(dim=1).max())
+    return {"value": world * n * steps / ts, "unit": UNIT, "exact": world * n * steps / te, "speedup": te / ts,
+            "steps": steps, "particles": n, "resolution": resolution, "paths": stats,
+            "max_position_deviation_m": dev, "deviation_over_max_displacement": dev / moved,
+            "roofline": step_roofline(n, asur, steps, ts), "exact_roofline": step_roofline(n, ae, steps, te),
+            "scene": f"box loaf {n} particles, {resolution}^3, 318 K, prestrain 0.08, gas + transport, "
+                     f"{steps} substeps after 3 warm-up substeps"}
 
 
 def cell_order_variant(args, rank, dist, stream, world, steps=20):
