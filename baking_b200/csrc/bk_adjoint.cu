@@ -64,11 +64,12 @@ struct PrincipalFwd {
     bool yielded, iso;
 };
 
-__device__ PrincipalFwd principal_forward(const float* s, float mu, float lam, float ty, float eta, float a, float dt) {
+__device__ PrincipalFwd principal_forward(const float* s, const float* e, float mu, float lam, float ty, float eta, float a,
+                                          float dt) {
     PrincipalFwd f;
     f.mu = mu; f.lam = lam; f.ty = ty; f.eta = eta; f.a = a; f.dt = dt;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) { f.s[k] = s[k]; f.eps[k] = logf(s[k]); }
+    for (int k = 0; k < 3; ++k) { f.s[k] = s[k]; f.eps[k] = e[k]; }
     f.tr = f.eps[0] + f.eps[1] + f.eps[2];
 #pragma unroll
     for (int k = 0; k < 3; ++k) f.ts[k] = 2.f * mu * f.eps[k] + lam * f.tr;
@@ -204,12 +205,12 @@ struct CoupledFwd {
     double Vp;
 };
 
-__device__ CoupledFwd coupled_forward(const float* s, float mu, float lam, float ty, float eta, float dt, float n0,
+__device__ CoupledFwd coupled_forward(const float* e, float mu, float lam, float ty, float eta, float dt, float n0,
                                       float por) {
     CoupledFwd c;
     c.mu = mu; c.lam = lam; c.ty = ty; c.eta = eta; c.dt = dt;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) c.eps[k] = logf(s[k]);
+    for (int k = 0; k < 3; ++k) c.eps[k] = e[k];
     c.tr = c.eps[0] + c.eps[1] + c.eps[2];
     float ts[3];
 #pragma unroll
@@ -236,9 +237,9 @@ __device__ CoupledFwd coupled_forward(const float* s, float mu, float lam, float
 // equation (the derivatives of the reference's SolvePorosityGradient, porous_return.py:64-100)
 // gives dn/dtheta = dpred/dtheta / (1 - dpred/dn); the elastic early exit is the case r = 0.
 // Out of line, called before the rest of the reverse sweep needs its registers.
-__device__ __noinline__ float coupled_solve_grad(const float* s, float mu, float lam, float ty, float eta, float dt,
+__device__ __noinline__ float coupled_solve_grad(const float* s, const float* log_s, float mu, float lam, float ty, float eta, float dt,
                                                  float n0, float por, float* G) {
-    const CoupledFwd c = coupled_forward(s, mu, lam, ty, eta, dt, n0, por);
+    const CoupledFwd c = coupled_forward(log_s, mu, lam, ty, eta, dt, n0, por);
     double r = 0.0;
     bool elastic_exit;
     const float nf = solve_porosity(c.q, c.p, c.df, c.ms, c.ex, c.Vp, n0, &r, &elastic_exit);
@@ -448,16 +449,16 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                 for (int e = 0; e < 9; ++e) Gd.m[e] = D.dt * nc[e] + ((e % 4) == 0 ? 1.f : 0.f);
                 M3 trial = matmul(Gd, Fe_old);
                 M3 U, V;
-                float s[3];
-                svd3f(trial, U, s, V);
+                float s[3], se[3];
+                svd3f(trial, U, s, V, se);
                 // Gas mode: the end-state porosity n_ret of the coupled solve sets a(n) of the
                 // return, and the returned Fe is rescaled to det F' / (1 - n0 + n_ret) (ding.py:183-205).
                 constexpr bool coupled = kCoupled;
                 float n_ret = por;
                 float nG[8];  // dn_ret/d(s0, s1, s2, mu, lambda, yield, viscosity, old porosity)
-                if (coupled) n_ret = coupled_solve_grad(s, D.mu, D.lam, ty, eta, D.dt, D.initial_porosity, por, nG);
+                if (coupled) n_ret = coupled_solve_grad(s, se, D.mu, D.lam, ty, eta, D.dt, D.initial_porosity, por, nG);
                 float a = porosity_coefficient(n_ret);
-                PrincipalFwd pr = principal_forward(s, D.mu, D.lam, ty, eta, a, D.dt);
+                PrincipalFwd pr = principal_forward(s, se, D.mu, D.lam, ty, eta, a, D.dt);
                 bool porosity_free = !(D.initial_porosity == 0.0f && por == 0.0f);
                 float detFn = det3(Fn);
                 float gv[3] = {pr.g[0], pr.g[1], pr.g[2]};  // principal values of the stored Fe'

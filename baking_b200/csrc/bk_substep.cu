@@ -789,7 +789,7 @@ SurrogateDev surrogate_dev(const BkReturnSurrogate* r) {
 // local memory).
 __device__ __forceinline__ float sel3(const float* a, int k) { return k == 0 ? a[0] : (k == 1 ? a[1] : a[2]); }
 
-// Singular-value order (descending) the network sees.
+// Singular-value order (descending) the network sees, from the values or their logs.
 __device__ __forceinline__ void order3(const float* s, int* perm) {
     int a = 0, b = 1, c = 2, t;
     if (s[a] < s[b]) { t = a; a = b; b = t; }
@@ -804,7 +804,7 @@ __device__ __forceinline__ void surrogate_features(const Params& P, const BkStat
                                                    int64_t i, const DingPrelude& d, float por, float J,
                                                    const int* perm, float* f) {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) f[k] = logf(sel3(d.s, perm[k]));
+    for (int k = 0; k < 3; ++k) f[k] = sel3(d.e, perm[k]);
     f[3] = d.T_eff;
     f[4] = P.transport ? (float)(out.water[i] / ((double)P.water_density * (double)cst.volume[i] * (double)J)) : 0.0f;
     f[5] = P.gas ? (float)out.gas_moles[i] : 0.0f;
@@ -814,7 +814,7 @@ __device__ __forceinline__ void surrogate_features(const Params& P, const BkStat
 // True when the exact return map leaves the particle elastic (no overstress solve): the cheap
 // path for which the exact map runs unchanged.
 __device__ __forceinline__ bool ding_elastic(const DingParamsDev& D, const DingPrelude& d, float por) {
-    float st[3] = {logf(d.s[0]), logf(d.s[1]), logf(d.s[2])};
+    const float* st = d.e;
     float tr = st[0] + st[1] + st[2];
     float ts[3];
 #pragma unroll
@@ -842,7 +842,7 @@ __device__ bool ding_surrogate(const DingParamsDev& D, const DingPrelude& d, flo
     const float mu = D.mu, bulk = 2.0f * D.mu + 3.0f * D.lam;
     float ret_por = por;
     if (D.coupled_porosity) {
-        double dv = (double)logf(d.s[0]) + (double)logf(d.s[1]) + (double)logf(d.s[2]) - ((double)e[0] + e[1] + e[2]);
+        double dv = (double)d.e[0] + (double)d.e[1] + (double)d.e[2] - ((double)e[0] + e[1] + e[2]);
         double rp = (1.0 - (double)D.initial_porosity + (double)por) * exp(dv) - 1.0 + (double)D.initial_porosity;
         if (!(rp > 0.0 && rp < 1.0)) return false;
         ret_por = (float)rp;
@@ -914,7 +914,7 @@ __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkS
         int slot = atomicAdd(sg.sample_count, 1);
         if (slot < sg.sample_capacity) {
             int perm[3];
-            order3(d.s, perm);
+            order3(d.e, perm);
             float f[7];
             surrogate_features(P, out, cst, i, d, por, det3(Fn), perm, f);
             float* row = sg.samples + (int64_t)slot * 12;
@@ -960,7 +960,7 @@ __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkSta
             ding = ding_prelude(P.ding, load_m3(in.Fe, i, pitch), por, in.gelled[i], Cn, T,
                                 __ldg(cst.viscosity_parameter), flags.ding, d);
             if (ding && !ding_elastic(P.ding, d, por)) {
-                order3(d.s, perm);
+                order3(d.e, perm);
                 float f[7];
                 surrogate_features(P, out, cst, i, d, por, det3(Fn), perm, f);
                 use_mlp = true;
@@ -971,8 +971,11 @@ __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkSta
                 }
             }
         }
-        float y[3];
-        const bool tile_ok = mlp::tile_eval(ts, x, use_mlp, y, phase);
+        float y[3] = {0.f, 0.f, 0.f};
+        // A tile whose particles all take the exact map (elastic, or outside the training range)
+        // skips the network; the barrier makes the decision uniform across the CTA.
+        const bool any_mlp = __syncthreads_or(use_mlp) != 0;
+        const bool tile_ok = any_mlp ? mlp::tile_eval(ts, x, use_mlp, y, phase) : true;
         int path = -1;
         if (ding) {
             DingParticleOut o;
@@ -983,7 +986,7 @@ __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkSta
 #pragma unroll
                 for (int j = 0; j < 3; ++j) {
                     const int r = perm[0] == j ? 0 : (perm[1] == j ? 1 : 2);
-                    e[j] = logf(d.s[j]) + sel3(y, r) * sel3(sg.out_scale, r);
+                    e[j] = d.e[j] + sel3(y, r) * sel3(sg.out_scale, r);
                 }
                 done = ding_surrogate(P.ding, d, por, Fn, e, flags.ding, o, diag.plastic_gradients != nullptr);
                 // Judged in whole warps, so that the exact map's cost falls on 1 warp in judge_stride.
