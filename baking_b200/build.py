@@ -53,7 +53,7 @@ def build(force=False, verbose=False, extra_flags=()):
     common = [nvcc(), *ARCH, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC}", *extra_flags]
     for src in sources():
         obj = build_dir / (src.stem + ".o")
-        cmd = common + ["-dc" if False else "-c", str(src), "-o", str(obj)]
+        cmd = common + ["-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), flush=True)
         result = subprocess.run(cmd, capture_output=True, text=True)

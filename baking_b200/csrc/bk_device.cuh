@@ -594,7 +594,7 @@ struct DingOut {
 
 // Ding return map (ding.py:103-137) given the SVD of the trial gradient (float32 factors) and its
 // principal log stretches log_s (svd3f).
-BK_DEV DingOut ding_return(const M3& trial, const M3& Um, const float* log_s, const M3& Vm, float mu, float lam,
+BK_DEV DingOut ding_return(float det_trial, const M3& Um, const float* log_s, const M3& Vm, float mu, float lam,
                            float ty, float eta, float a, float dt, float r0 = 0.0f) {
     const float* U = Um.m;
     const float* V = Vm.m;
@@ -633,7 +633,7 @@ BK_DEV DingOut ding_return(const M3& trial, const M3& Um, const float* log_s, co
         }
     if (a == 0.0f) {
         // pow(x, 1/3) of the reference; cube root of the same argument.
-        float scale = cbrtf(det3(trial) / det3(o.Fe));
+        float scale = cbrtf(det_trial / det3(o.Fe));
 #pragma unroll
         for (int e = 0; e < 9; ++e) o.Fe.m[e] *= scale;
     }
@@ -663,7 +663,8 @@ struct DingParticleOut {
 // The part of UpdateDing (ding.py:154-180) before the return: gelation latch, temperature tables,
 // trial gradient and its SVD.
 struct DingPrelude {
-    M3 trial, U, V;
+    M3 U, V;
+    float det_trial;   // det of the trial elastic gradient (the isochoric correction's numerator)
     float s[3], e[3];  // singular values and their logs (svd3f)
     float ty, eta, T_eff;
     int gel;
@@ -685,8 +686,9 @@ BK_DEV bool ding_prelude(const DingParamsDev& P, const M3& Fe_old, float por, in
     M3 G;
 #pragma unroll
     for (int e = 0; e < 9; ++e) G.m[e] = P.dt * C_new.m[e] + ((e % 4) == 0 ? 1.0f : 0.0f);
-    d.trial = matmul(G, Fe_old);
-    svd3f(d.trial, d.U, d.s, d.V, d.e);
+    const M3 trial = matmul(G, Fe_old);
+    d.det_trial = det3(trial);
+    svd3f(trial, d.U, d.s, d.V, d.e);
     d.ty = ty;
     d.eta = eta;
     d.T_eff = Teff;
@@ -694,11 +696,31 @@ BK_DEV bool ding_prelude(const DingParamsDev& P, const M3& Fe_old, float por, in
     return true;
 }
 
+// Where ding_close reads the total gradient F' from: a matrix the caller holds (FInRegs), or the F'
+// this thread stored earlier in the same kernel (FStored), read back with plain loads only where
+// the close needs it, so that it is not held in registers through the return map.
+struct FInRegs {
+    const M3& m;
+    BK_DEV M3 get() const { return m; }
+};
+struct FStored {
+    const float* p;  // not the read-only path: the data were written during this kernel
+    int64_t i, pitch;
+    BK_DEV M3 get() const {
+        M3 r;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) r.m[c] = p[c * pitch + i];
+        return r;
+    }
+};
+
 // Volume correction (gas mode), plastic gradient and porosity update shared by the exact and the
 // surrogate returns (ding.py:200-221).
-BK_DEV void ding_close(const DingParamsDev& P, float por, const M3& F_tot, float ret_por, M3 Fe, int32_t* flags,
+template <class FSrc>
+BK_DEV void ding_close(const DingParamsDev& P, float por, const FSrc& F_src, float ret_por, M3 Fe, int32_t* flags,
                        DingParticleOut& out, bool need_fp) {
     const float n0 = P.initial_porosity;
+    const M3 F_tot = F_src.get();
     if (P.coupled_porosity) {
         double target = 1.0 - (double)n0 + (double)ret_por;
         M3d Fd, Fed;
@@ -726,7 +748,8 @@ BK_DEV void ding_close(const DingParamsDev& P, float por, const M3& F_tot, float
 }
 
 // The exact return of UpdateDing after the prelude (ding.py:181-221).
-BK_DEV void ding_exact(const DingParamsDev& P, const DingPrelude& d, float por, const M3& F_tot, int32_t* flags,
+template <class FSrc>
+BK_DEV void ding_exact(const DingParamsDev& P, const DingPrelude& d, float por, const FSrc& F_tot, int32_t* flags,
                        DingParticleOut& out, bool need_fp) {
     const float dt = P.dt, mu = P.mu, lam = P.lam, n0 = P.initial_porosity;
     const float ty = d.ty, eta = d.eta;
@@ -755,7 +778,7 @@ BK_DEV void ding_exact(const DingParamsDev& P, const DingPrelude& d, float por, 
         consistency = (float)fabs((double)ret_por - pred);
         if (consistency > 1.0e-6f || ret_por <= 0.0f || ret_por >= 1.0f) set_flag(flags, 1);
     }
-    DingOut r = ding_return(d.trial, d.U, d.e, d.V, mu, lam, ty, eta, porosity_coefficient(ret_por), dt,
+    DingOut r = ding_return(d.det_trial, d.U, d.e, d.V, mu, lam, ty, eta, porosity_coefficient(ret_por), dt,
                             (float)r_warm);
     ding_close(P, por, F_tot, ret_por, r.Fe, flags, out, need_fp);
     out.tau = r.tau;
@@ -777,7 +800,7 @@ BK_DEV bool update_ding_particle(const DingParamsDev& P, const M3& Fe_old, float
                                  bool need_fp = true) {
     DingPrelude d;
     if (!ding_prelude(P, Fe_old, por, gel, C_new, T, eta_base, flags, d)) return false;
-    ding_exact(P, d, por, F_tot, flags, out, need_fp);
+    ding_exact(P, d, por, FInRegs{F_tot}, flags, out, need_fp);
     return true;
 }
 

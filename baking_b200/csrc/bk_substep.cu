@@ -677,8 +677,12 @@ __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkSta
 }
 
 // ------------------------------------------------------ fused G2P + return
+// The largest positive value over the warp's active lanes into *addr (nonnegative floats order as
+// their bit patterns): one atomic per warp instead of one per lane on the same address.
 __device__ __forceinline__ void atomic_max_nonneg(float* addr, float value) {
-    if (value > 0.0f) atomicMax(reinterpret_cast<int*>(addr), __float_as_int(value));
+    const unsigned mask = __activemask();
+    const int v = (int)__reduce_max_sync(mask, (unsigned)__float_as_int(value > 0.0f ? value : 0.0f));
+    if (v > 0 && (int)(threadIdx.x & 31) == __ffs(mask) - 1) atomicMax(reinterpret_cast<int*>(addr), v);
 }
 
 // G2P of one particle (transfer.py:73-109): writes x', v', C', F' and returns F', C'. False (and the
@@ -867,11 +871,11 @@ __device__ bool ding_surrogate(const DingParamsDev& D, const DingPrelude& d, flo
                                (U[3 * r + 2] * cs[2]) * U[3 * c + 2];
         }
     if (!D.coupled_porosity && porosity_coefficient(por) == 0.0f) {
-        float scale = cbrtf(det3(d.trial) / det3(Fe));
+        float scale = cbrtf(d.det_trial / det3(Fe));
 #pragma unroll
         for (int k = 0; k < 9; ++k) Fe.m[k] *= scale;
     }
-    ding_close(D, por, F_tot, ret_por, Fe, flags, out, need_fp);
+    ding_close(D, por, FInRegs{F_tot}, ret_por, Fe, flags, out, need_fp);
     out.tau = tau;
     out.residual = 0.0f;
     out.porosity_residual = 0.0f;
@@ -908,7 +912,7 @@ __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkS
                       flags.ding, d))
         return;
     DingParticleOut o;
-    ding_exact(P.ding, d, por, Fn, flags.ding, o, diag.plastic_gradients != nullptr);
+    ding_exact(P.ding, d, por, FStored{out.F, i, pitch}, flags.ding, o, diag.plastic_gradients != nullptr);
     ding_store(P, out, diag, i, T, o);
     if (sg.samples && o.yielded && i % sg.sample_stride == sg.sample_offset) {
         int slot = atomicAdd(sg.sample_count, 1);
@@ -916,7 +920,7 @@ __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkS
             int perm[3];
             order3(d.e, perm);
             float f[7];
-            surrogate_features(P, out, cst, i, d, por, det3(Fn), perm, f);
+            surrogate_features(P, out, cst, i, d, por, det3(FStored{out.F, i, pitch}.get()), perm, f);
             float* row = sg.samples + (int64_t)slot * 12;
 #pragma unroll
             for (int k = 0; k < 7; ++k) row[k] = f[k];
@@ -992,14 +996,14 @@ __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkSta
                 // Judged in whole warps, so that the exact map's cost falls on 1 warp in judge_stride.
                 if (done && sg.judge_error && sg.judge_stride > 0 && (i >> 5) % sg.judge_stride == 0) {
                     DingParticleOut ex;
-                    ding_exact(P.ding, d, por, Fn, nullptr, ex, false);  // judge only: no flags
+                    ding_exact(P.ding, d, por, FInRegs{Fn}, nullptr, ex, false);  // judge only: no flags
                     float err = 0.f;
 #pragma unroll
                     for (int k = 0; k < 3; ++k) err = fmaxf(err, fabsf(ex.e[k] - e[k]));
                     atomic_max_nonneg(sg.judge_error, err);
                 }
             }
-            if (!done) ding_exact(P.ding, d, por, Fn, flags.ding, o, diag.plastic_gradients != nullptr);
+            if (!done) ding_exact(P.ding, d, por, FInRegs{Fn}, flags.ding, o, diag.plastic_gradients != nullptr);
             path = done ? 1 : (o.yielded ? 2 : 0);
             ding_store(P, out, diag, i, T, o);
         }
