@@ -30,9 +30,11 @@ class BatchedSimulators:
         self.particle_count = sum(s.particle_data.particle_count for s in self.sims)
 
     @staticmethod
-    def _substep(sim, state_in, state_out):
+    def _substep(sim, state_in, state_out, prescattered=False, prescatter_next=False):
         eng = sim._engine
-        eng.run(state_in, state_out, False, PHASE_TRANSPORT | PHASE_MECHANICS, False)
+        ahead = eng.prescatter_allowed()
+        eng.run(state_in, state_out, False, PHASE_TRANSPORT | PHASE_MECHANICS, False,
+                prescattered=ahead and prescattered, prescatter_next=ahead and prescatter_next)
         if sim.transport is not None:
             eng.accumulate_surface(state_out.transport_state)
 
@@ -43,8 +45,9 @@ class BatchedSimulators:
             s.wait_stream(main)
             with torch.cuda.stream(s):
                 a, b = sim._current, sim.next_state
-                self._substep(sim, a, b)
-                self._substep(sim, b, a)
+                # the second substep of the pair finds its transport fields scattered by the first
+                self._substep(sim, a, b, prescatter_next=True)
+                self._substep(sim, b, a, prescattered=True)
         for s in self.streams:
             main.wait_stream(s)
 

@@ -56,6 +56,7 @@ struct Params {
     float conductivity, diffusivity, s0, water_stress;
     float ambient, density, elastic_modulus, cfl, peak, width;
     int keep_fields;
+    int prescattered, prescatter_next;
 };
 
 Params to_params(const BkSubstepParams& p) {
@@ -83,6 +84,8 @@ Params to_params(const BkSubstepParams& p) {
     k.ambient = p.gas_ambient_pressure; k.density = p.density; k.elastic_modulus = p.elastic_modulus;
     k.cfl = p.cfl_limit; k.peak = p.gas_peak; k.width = p.gas_width;
     k.keep_fields = p.keep_transport_fields;
+    k.prescattered = p.transport_prescattered;
+    k.prescatter_next = p.transport_prescatter_next;
     return k;
 }
 
@@ -127,9 +130,10 @@ struct BlockBox {
     bool tiled;                // the box fits a shared-memory tile of kTileNodes
 };
 
-// Block-level min/max of valid stencil nodes; also widens the active node box of the substep
-// (bounds[0..2] lo, [3..5] hi). Every thread of the block must call this (it synchronises the block).
-__device__ BlockBox block_box(int* bounds, bool valid, const int* b) {
+// Block-level min/max of valid stencil nodes; also widens the node box `bounds` ([0..2] lo, [3..5]
+// hi). The box is tiled when it holds at most `tile_nodes` nodes. Every thread of the block must
+// call this (it synchronises the block).
+__device__ BlockBox block_box(int* bounds, bool valid, const int* b, int tile_nodes = kTileNodes) {
     __shared__ int s_box[6];
     if (threadIdx.x < 6) s_box[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
     __syncthreads();
@@ -154,7 +158,7 @@ __device__ BlockBox block_box(int* bounds, bool valid, const int* b) {
             bb.ext[a] = s_box[3 + a] - s_box[a] + 1;
             count *= bb.ext[a];
         }
-        bb.tiled = count <= kTileNodes;
+        bb.tiled = count <= tile_nodes;
         bb.count = bb.tiled ? (int)count : 0;
         if (threadIdx.x < 3) {
             atomicMin(bounds + threadIdx.x, s_box[threadIdx.x]);
@@ -241,45 +245,27 @@ __global__ void k_surface_owners(Params P, BkState in, BkConstants cst, BkSurfac
 
 // ---------------------------------------------------------- transport P2G
 // physics/thermal_water.py:108-137 (volume, capacity, energy, water), warp-cooperative per stencil run.
-struct TransportSmem {
-    float w[kThreads][9];
-    double val[kThreads][4];
-    double tile[4][kTileNodes];
+// The block routine scatters its threads' particles; each thread passes its stencil, whether it is
+// valid, and its four values (V0 det F, capacity, capacity T, W). Every thread of the block calls it.
+template <int kT, int kTile>
+struct TransportTile {
+    float w[kT][9];
+    double val[kT][4];
+    double tile[4][kTile];
 };
 
-__global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkState in, BkConstants cst, GridPtrs g,
-                                                               int32_t* sim_flags) {
-    __shared__ TransportSmem sm;
+template <int kT, int kTile>
+__device__ void transport_scatter_block(TransportTile<kT, kTile>& sm, const Params& P, const GridPtrs& g, int* box,
+                                        bool valid, const Stencil& st, const double* val) {
     const int tid = threadIdx.x, lane = tid & 31;
-    const int64_t i = blockIdx.x * (int64_t)kThreads + tid;
-    const int64_t pitch = P.pitch;
-    bool valid = false;
-    Stencil st;
-    st.b[0] = st.b[1] = st.b[2] = 0;
-    if (i < P.n) {
-        st = make_stencil(load_v3(in.x, i, pitch), P.origin, P.dx, P.R);
-        valid = st.valid;
-        if (!valid) set_flag(sim_flags, 1);
-    }
-    if (valid) {
-        double vol = (double)cst.volume[i] * (double)det3(load_m3(in.F, i, pitch));
-        double cap = cst.capacity[i], T = in.temperature[i];
-        sm.val[tid][0] = vol;
-        sm.val[tid][1] = cap;
-        sm.val[tid][2] = cap * T;
-        sm.val[tid][3] = in.water[i];
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+    for (int k = 0; k < 4; ++k) sm.val[tid][k] = valid ? val[k] : 0.0;
 #pragma unroll
-            for (int o = 0; o < 3; ++o) sm.w[tid][3 * a + o] = st.w[a][o];
-    } else {
+    for (int a = 0; a < 3; ++a)
 #pragma unroll
-        for (int k = 0; k < 4; ++k) sm.val[tid][k] = 0.0;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) sm.w[tid][k] = 0.f;
-    }
-    const BlockBox bb = block_box(g.bounds, valid, st.b);  // synchronises the block
-    for (int t = tid; t < bb.count; t += kThreads)
+        for (int o = 0; o < 3; ++o) sm.w[tid][3 * a + o] = valid ? st.w[a][o] : 0.f;
+    const BlockBox bb = block_box(box, valid, st.b, kTile);  // synchronises the block
+    for (int t = tid; t < bb.count; t += kT)
 #pragma unroll
         for (int f = 0; f < 4; ++f) sm.tile[f][t] = 0.0;
     __syncthreads();
@@ -313,12 +299,36 @@ __global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkStat
         }
     }
     __syncthreads();
-    for (int t = tid; t < bb.count; t += kThreads) {
+    for (int t = tid; t < bb.count; t += kT) {
         if (sm.tile[1][t] == 0.0 && sm.tile[0][t] == 0.0 && sm.tile[3][t] == 0.0) continue;
         int64_t node = tile_node(bb, t, P.R);
 #pragma unroll
         for (int f = 0; f < 4; ++f) atomicAdd(g.f[f] + node, sm.tile[f][t]);
     }
+}
+
+__global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkState in, BkConstants cst, GridPtrs g,
+                                                               int32_t* sim_flags) {
+    __shared__ TransportTile<kThreads, kTileNodes> sm;
+    const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+    const int64_t pitch = P.pitch;
+    bool valid = false;
+    Stencil st;
+    st.b[0] = st.b[1] = st.b[2] = 0;
+    double val[4] = {0.0, 0.0, 0.0, 0.0};
+    if (i < P.n) {
+        st = make_stencil(load_v3(in.x, i, pitch), P.origin, P.dx, P.R);
+        valid = st.valid;
+        if (!valid) set_flag(sim_flags, 1);
+    }
+    if (valid) {
+        double cap = cst.capacity[i];
+        val[0] = (double)cst.volume[i] * (double)det3(load_m3(in.F, i, pitch));
+        val[1] = cap;
+        val[2] = cap * in.temperature[i];
+        val[3] = in.water[i];
+    }
+    transport_scatter_block<kThreads, kTileNodes>(sm, P, g, g.bounds, valid, st, val);
 }
 
 // ------------------------------------------------------------ grid passes
@@ -357,7 +367,9 @@ __global__ void __launch_bounds__(kDiffThreads) k_diffuse(Params P, GridPtrs g, 
     __shared__ unsigned char s_ok[kHaloNodes];
     int lo[3], ext[3];
     int64_t count;
-    if (!box_of(g.bounds, P.R, lo, ext, count)) return;
+    // The node box of the transport fields: built by this substep's scalar P2G, or by the previous
+    // substep's G2P when it scattered them ahead.
+    if (!box_of(P.prescattered ? g.bounds + 12 : g.bounds, P.R, lo, ext, count)) return;
     const int R = P.R;
     const double rho_w = (double)P.water_density;
     const double cell = (double)(P.dx * P.dx * P.dx);
@@ -456,6 +468,9 @@ __global__ void k_clear_previous(Params P, GridPtrs g) {
 __global__ void k_grid_update(Params P, GridPtrs g) {
     int lo[3], ext[3];
     int64_t count;
+    // The G2P that follows builds the next substep's transport box in bounds[12..17]: restart it
+    // empty (this substep's diffusion, its only reader, has finished; no block here reads it).
+    if (P.prescatter_next && blockIdx.x == 0 && threadIdx.x < 6) g.bounds[12 + threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
     if (!box_of(g.bounds, P.R, lo, ext, count)) return;
     const int R = P.R, bc = P.bc;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
@@ -892,15 +907,9 @@ __device__ bool ding_surrogate(const DingParamsDev& D, const DingPrelude& d, flo
 // latency bound, so resident warps outweigh the spilled registers (measured at 3 to 12 blocks per
 // SM: 8 is fastest for both elastic and yielding particles). With `sg.samples` set (harvest),
 // yielding particles on the sampling stride append (features, return) rows.
-__global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
-                                                   BkDiagnostics diag, BkFlags flags, SurrogateDev sg) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (blockIdx.x == 0 && threadIdx.x < 6) {
-        // This substep's box becomes the box the next substep clears; the active box restarts empty.
-        g.bounds[6 + threadIdx.x] = g.bounds[threadIdx.x];
-        g.bounds[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
-    }
-    if (i >= P.n) return;
+__device__ __forceinline__ void g2p_return_particle(const Params& P, const BkState& in, const BkState& out,
+                                                    const BkConstants& cst, const GridPtrs& g, const BkDiagnostics& diag,
+                                                    const BkFlags& flags, const SurrogateDev& sg, int64_t i) {
     M3 Fn, Cn;
     if (!g2p_gather(P, in, out, g, flags, i, Fn, Cn)) return;
     if (P.material != 1) return;
@@ -929,6 +938,48 @@ __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkS
             row[10] = 0.0f;
             row[11] = 0.0f;
         }
+    }
+}
+
+// Shared-memory node tile of the transport prescatter in k_g2p_return (128 particles per block).
+constexpr int kG2PTile = 256;
+using G2PTransportTile = TransportTile<128, kG2PTile>;
+
+__global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
+                                                   BkDiagnostics diag, BkFlags flags, SurrogateDev sg) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (blockIdx.x == 0 && threadIdx.x < 6) {
+        // This substep's box becomes the box the next substep clears; the active box restarts empty.
+        g.bounds[6 + threadIdx.x] = g.bounds[threadIdx.x];
+        g.bounds[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
+    }
+    if (i < P.n) g2p_return_particle(P, in, out, cst, g, diag, flags, sg, i);
+    if (P.prescatter_next) {
+        // The next substep's scalar P2G (thermal_water.py:108-137) from the state just written:
+        // x' and F' by this thread (read back with plain loads), T' and W' by this substep's P2G.
+        // The grid update has zeroed the transport fields over this substep's box and restarted
+        // the prescatter box bounds[12..17]. Uniform branch: every thread of the block scatters.
+        extern __shared__ __align__(16) unsigned char g2p_smem[];
+        G2PTransportTile& sm = *reinterpret_cast<G2PTransportTile*>(g2p_smem);
+        const int64_t pitch = P.pitch;
+        bool valid = false;
+        Stencil st;
+        st.b[0] = st.b[1] = st.b[2] = 0;
+        double val[4] = {0.0, 0.0, 0.0, 0.0};
+        if (i < P.n) {
+            const float* xs = out.x;
+            const V3 x{{xs[i], xs[pitch + i], xs[2 * pitch + i]}};
+            st = make_stencil(x, P.origin, P.dx, P.R);
+            valid = st.valid;
+            if (valid) {
+                const double cap = cst.capacity[i];
+                val[0] = (double)cst.volume[i] * (double)det3(FStored{out.F, i, pitch}.get());
+                val[1] = cap;
+                val[2] = cap * out.temperature[i];
+                val[3] = out.water[i];
+            }
+        }
+        transport_scatter_block<128, kG2PTile>(sm, P, g, g.bounds + 12, valid, st, val);
     }
 }
 
@@ -1102,6 +1153,12 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
     if (p.gas)
         BK_REQUIRE(p.transport && p.material == 1 && in->gas_moles && out->gas_moles && constants->gas_rate,
                    "bk_substep: gas mode needs transport, the Ding model and gas arrays");
+    if (p.transport_prescattered || p.transport_prescatter_next)
+        BK_REQUIRE(p.transport && !p.keep_transport_fields,
+                   "bk_substep: the transport prescatter needs transport and a grid update that clears the fields");
+    if (p.transport_prescatter_next)
+        BK_REQUIRE(!(p.surrogate && p.surrogate->packed) && (phases & BK_PHASE_MECHANICS),
+                   "bk_substep: the transport prescatter runs in the exact G2P kernel of a mechanics phase");
     if (p.n == 0) return BK_OK;
     Params P = to_params(p);
     GridPtrs g = grid_ptrs(*grid);
@@ -1134,12 +1191,14 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
             }
             if (int rc = check_launch("bk_substep/surface_owners")) return rc;
         }
-        {
-            int rec = profile_begin("transport_scatter", s);
-            k_transport_scatter<<<particle_blocks, kThreads, 0, s>>>(P, *in, *constants, g, flags->simulation);
-            profile_end(rec, s);
+        if (!p.transport_prescattered) {
+            {
+                int rec = profile_begin("transport_scatter", s);
+                k_transport_scatter<<<particle_blocks, kThreads, 0, s>>>(P, *in, *constants, g, flags->simulation);
+                profile_end(rec, s);
+            }
+            if (int rc = check_launch("bk_substep/transport_scatter")) return rc;
         }
-        if (int rc = check_launch("bk_substep/transport_scatter")) return rc;
         {
             int rec = profile_begin("diffuse", s);
             k_diffuse<<<box_blocks, kDiffThreads, 0, s>>>(P, g, flags->transport);
@@ -1177,7 +1236,8 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
             profile_end(rec, s);
         } else {
             int rec = profile_begin("g2p_return", s);
-            k_g2p_return<<<blocks_for(p.n, 128), 128, 0, s>>>(P, *in, *out, *constants, g, *diagnostics, *flags, sg);
+            const size_t smem = p.transport_prescatter_next ? sizeof(G2PTransportTile) : 0;
+            k_g2p_return<<<blocks_for(p.n, 128), 128, smem, s>>>(P, *in, *out, *constants, g, *diagnostics, *flags, sg);
             profile_end(rec, s);
         }
         if (int rc = check_launch("bk_substep/g2p_return")) return rc;

@@ -411,20 +411,24 @@ class MpmSimulator:
             self.result_recorder.Reset()
 
     # ---------------------------------------------------------------- step
-    def _substep(self, check):
+    def _substep(self, check, prescattered=False, prescatter_next=False):
         """One substep through the fused kernels; with ``check`` the device flags are read where the
-        reference synchronises (after the transport solve and after the return map)."""
+        reference synchronises (after the transport solve and after the return map).
+        ``prescattered``/``prescatter_next``: the transport fields of this substep were scattered
+        ahead by the previous one / scatter the next substep's ahead (SubstepEngine.run); only for
+        substeps run back to back inside one call, where nothing can change the state in between."""
         from .substep import PHASE_MECHANICS, PHASE_TRANSPORT
         was_settling = self.IsSettling
         original = self._current
         output = self._allocate_like_current(share_accumulators=False) if self.retain_history else self.next_state
         full = self.diagnostics == "full"
         if check and self.transport is not None:
-            self._engine.run(original, output, was_settling, PHASE_TRANSPORT, full)
+            self._engine.run(original, output, was_settling, PHASE_TRANSPORT, full, prescattered=prescattered)
             self.transport.CheckState()
-            self._engine.run(original, output, was_settling, PHASE_MECHANICS, full)
+            self._engine.run(original, output, was_settling, PHASE_MECHANICS, full, prescatter_next=prescatter_next)
         else:
-            self._engine.run(original, output, was_settling, PHASE_TRANSPORT | PHASE_MECHANICS, full)
+            self._engine.run(original, output, was_settling, PHASE_TRANSPORT | PHASE_MECHANICS, full,
+                             prescattered=prescattered, prescatter_next=prescatter_next)
         if check and isinstance(self.material, DingMaterial):
             self.material.CheckState()
         if self.transport is not None:
@@ -471,8 +475,10 @@ class MpmSimulator:
         if step_count < 1:
             raise ValueError("step_count must be positive")
         start = self.step_count
-        for _ in range(step_count):
-            self._substep(check=self.IsSettling)
+        ahead = self._engine.prescatter_allowed()
+        for k in range(step_count):
+            self._substep(check=self.IsSettling, prescattered=ahead and k > 0,
+                          prescatter_next=ahead and k + 1 < step_count)
         values = self._check_values()
         messages = []
         if isinstance(self.material, DingMaterial):
@@ -488,9 +494,11 @@ class MpmSimulator:
         return self.CheckState(values)
 
     def AdvanceUnchecked(self, step_count):
-        """Run substeps with no host synchronisation; flags stay on the device until CheckState/Advance."""
-        for _ in range(step_count):
-            self._substep(check=False)
+        """Run substeps with no host synchronisation; flags stay on the device until CheckState/Advance.
+        Within the call each substep's G2P scatters the next substep's transport fields ahead."""
+        ahead = self._engine.prescatter_allowed()
+        for k in range(step_count):
+            self._substep(check=False, prescattered=ahead and k > 0, prescatter_next=ahead and k + 1 < step_count)
 
     def StepSummary(self, out=None):
         """Device tensor (grid mass of the last substep, particle kinetic energy of the current

@@ -65,7 +65,8 @@ class BkSubstepParams(C.Structure):
                 ("water_stress", C.c_float), ("gas_ambient_pressure", C.c_float), ("density", C.c_float),
                 ("elastic_modulus", C.c_float), ("cfl_limit", C.c_float), ("gas_peak", C.c_float),
                 ("gas_width", C.c_float), ("surrogate", C.POINTER(BkReturnSurrogate)),
-                ("keep_transport_fields", C.c_int32)]
+                ("keep_transport_fields", C.c_int32), ("transport_prescattered", C.c_int32),
+                ("transport_prescatter_next", C.c_int32)]
 
 
 PHASE_TRANSPORT = 1
@@ -152,7 +153,8 @@ class SubstepEngine:
                        for _ in range(7)]
         self.node_dT_ratio = torch.zeros(R ** 3 if self.transport else 1, 2, dtype=torch.float64, device=dev)
         empty = [2 ** 31 - 1] * 3 + [-2 ** 31] * 3
-        self.bounds = torch.tensor(empty + empty, dtype=torch.int32, device=dev)
+        # the substep's box, the previous substep's, the transport box scattered ahead
+        self.bounds = torch.tensor(empty + empty + empty, dtype=torch.int32, device=dev)
         self.grid = BkGrid()
         self.grid.node_pm, self.grid.node_v = _p(self.node_pm), _p(self.node_v)
         for k in range(7):
@@ -275,7 +277,7 @@ class SubstepEngine:
             dTr = torch.zeros(R ** 3, 2, dtype=torch.float64, device=dev)
         tensors = dict(node_pm=torch.zeros(R ** 3, 4, dtype=torch.float32, device=dev),
                        node_v=torch.zeros(R ** 3, 4, dtype=torch.float32, device=dev),
-                       bounds=torch.tensor(empty + empty, dtype=torch.int32, device=dev),
+                       bounds=torch.tensor(empty + empty + empty, dtype=torch.int32, device=dev),
                        fields=fields, node_dT_ratio=dTr)  # kept alive with the grid
         grid = BkGrid()
         grid.node_pm, grid.node_v, grid.bounds = (_p(tensors[k]) for k in ("node_pm", "node_v", "bounds"))
@@ -285,9 +287,22 @@ class SubstepEngine:
         return grid, tensors
 
     # ---------------------------------------------------------------- launch
-    def run(self, state_in, state_out, settling, phases, full_diagnostics, grid=None, keep_fields=False):
+    def prescatter_allowed(self):
+        """Whether the G2P kernel may scatter the next substep's transport fields ahead (transport on,
+        exact return map)."""
+        sur = self.surrogate
+        return bool(self.transport) and not (sur is not None and sur.packed)
+
+    def run(self, state_in, state_out, settling, phases, full_diagnostics, grid=None, keep_fields=False,
+            prescattered=False, prescatter_next=False):
+        """One substep through bk_substep. ``prescattered``: the previous run scattered this substep's
+        transport fields ahead (its ``prescatter_next``), so the scalar P2G is skipped;
+        ``prescatter_next``: scatter the next substep's, which must start from ``state_out`` with
+        nothing changed in between."""
         p = self.params(settling)
         p.keep_transport_fields = int(keep_fields)
+        p.transport_prescattered = int(prescattered)
+        p.transport_prescatter_next = int(prescatter_next)
         cst = self.constants(settling)
         sin = state_struct(state_in, self.is_ding, self.transport, self.gas)
         sout = state_struct(state_out, self.is_ding, self.transport, self.gas)

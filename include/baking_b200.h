@@ -211,7 +211,9 @@ typedef struct BkGrid {
     double *node_dT_ratio;         /* R^3 x 2 doubles: temperature change, water change / node water */
     int32_t *bounds;               /* 12 ints (device): lo[3], hi[3] of the active node box being built,
                                       then lo[3], hi[3] of the last substep's box. Start as
-                                      {INT_MAX x3, INT_MIN x3, INT_MAX x3, INT_MIN x3} on a zero grid. */
+                                      {INT_MAX x3, INT_MIN x3, INT_MAX x3, INT_MIN x3} on a zero grid.
+                                      18 ints with the transport prescatter: then the box of the
+                                      fields scattered ahead for the next substep. */
 } BkGrid;
 
 /* Surface terms: the boundary-face vertices and the particles that own boundary faces. */
@@ -291,6 +293,15 @@ typedef struct BkSubstepParams {
     const BkReturnSurrogate *surrogate;  /* NULL: exact return map */
     int32_t keep_transport_fields;  /* 1: the grid update leaves the transport node fields in place
                                        (for bk_transport_adjoint, which clears them) */
+    int32_t transport_prescattered; /* 1: this substep's transport node fields (volume, capacity,
+                                       energy, water) and their node box (bounds[12..17]) were built by
+                                       the previous substep's G2P with transport_prescatter_next; the
+                                       scalar P2G kernel is skipped */
+    int32_t transport_prescatter_next; /* 1: the G2P kernel also scatters the next substep's transport
+                                       node fields from the state it writes, with their box in
+                                       bounds[12..17] (grid bounds of 18 ints). Valid only for a next
+                                       substep that starts from this output with nothing changed in
+                                       between; needs the exact return map (no surrogate). */
 } BkSubstepParams;
 
 #define BK_PHASE_TRANSPORT 1       /* surface terms, scalar P2G, diffusion */
