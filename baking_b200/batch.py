@@ -141,9 +141,15 @@ class SubstepGraphs:
     copy is queued), and ``Advance`` returns a ``StepResult`` for the slot, so a caller can read
     one substep's result while the next one runs. The graphs hold the simulator's arrays and
     parameters at capture time: refill parameter tensors in place between steps, and capture again
-    after replacing one."""
+    after replacing one.
 
-    def __init__(self, sim, inputs=(), host_results=False):
+    ``chained``: each substep's G2P also scatters the next substep's transport fields (volume,
+    capacity, energy, water), and each graph uses the fields the previous substep scattered instead
+    of running the scalar P2G. Valid while the simulator advances only through this object, with no
+    change to the particle state between substeps; ``inputs`` must then be parameters, not state
+    arrays (checked)."""
+
+    def __init__(self, sim, inputs=(), host_results=False, chained=False):
         if sim.IsSettling:
             raise ValueError("captured substeps start after settling (settling_duration_s = 0)")
         if sim.retain_history:
@@ -159,11 +165,20 @@ class SubstepGraphs:
         self.consumed = [None, None]   # events: the last graph that read staging set k finished
         self.graphs = None
         self._first = None
+        self.chained = bool(chained) and sim._engine.prescatter_allowed()
+        if self.chained:
+            state = {t.data_ptr() for st in (sim._current, sim.next_state)
+                     for t in _state_tensors_of(st)}
+            if any(t.data_ptr() in state for t in self.inputs):
+                raise ValueError("chained substeps take parameter inputs only, not particle state arrays")
 
-    def _record(self, state_in, state_out, parity):
+    def _record(self, state_in, state_out, parity, prescattered=None):
         for t, staged in zip(self.inputs, self.staging[parity]):
             t.copy_(staged)
-        BatchedSimulators._substep(self.sim, state_in, state_out)
+        chained = self.chained
+        BatchedSimulators._substep(self.sim, state_in, state_out,
+                                   prescattered=chained if prescattered is None else prescattered,
+                                   prescatter_next=chained)
         if self._host is not None:
             self.sim._engine.step_summary(state_out, out_ptr=self._host.device_ptr + 16 * parity)
         else:
@@ -183,11 +198,12 @@ class SubstepGraphs:
             for t, staged in zip(self.inputs, self.staging[k]):
                 staged.copy_(t)
         torch.cuda.synchronize()
-        self._record(a, b, 0)
+        self._record(a, b, 0, prescattered=False)  # the first chained substep scatters its own fields
         self._record(b, a, 1)
         torch.cuda.synchronize()
         sim.step_count += 2
         sim._stale = True
+        self._expect_step = sim.step_count
         graphs = {}
         for parity, (src, dst) in enumerate(((a, b), (b, a))):
             g = torch.cuda.CUDAGraph()
@@ -223,21 +239,30 @@ class SubstepGraphs:
             if self.loaded[parity] is not None:
                 main.wait_event(self.loaded[parity])
                 self.loaded[parity] = None
-            graph.replay()
+            if self.chained and sim.step_count != self._expect_step:
+                # The simulator was advanced outside this object since the last substep here, so no
+                # fields were scattered ahead: this substep runs eagerly with its own scalar P2G.
+                self._record(sim._current, nxt, parity, prescattered=False)
+            else:
+                graph.replay()
             done = torch.cuda.Event()
             done.record(main)
             self.consumed[parity] = done
             sim.next_state, sim._current = sim._current, nxt
             sim.step_count += 1
             sim._stale = True
+            self._expect_step = sim.step_count
             if self._host is not None:
                 result = StepResult(done, self._host.view[2 * parity:2 * parity + 2])
         return result if self._host is not None and steps > 0 else self.summary
 
 
 def _state_tensors(sim):
+    return _state_tensors_of(sim._current)
+
+
+def _state_tensors_of(st):
     from dataclasses import fields
-    st = sim._current
     out = []
     for holder in (st, st.material_state, st.transport_state):
         if holder is None:

@@ -371,13 +371,15 @@ def main():
 
     # End to end through the public API: pinned host inputs (the per-particle gas source rates) uploaded
     # for every substep, the substep (SubstepGraphs: one graph launch per substep, with the step-result
-    # reduction), and the step's result (grid mass, kinetic energy) read back to the host. Each
+    # reduction, chained so that each substep scatters the next one's transport fields ahead), and the
+    # step's result (grid mass, kinetic energy) read back to the host. Each
     # substep's upload runs on a copy stream while the substep before it computes; each result lands
     # in mapped host memory and is read while the next substep computes.
     from baking_b200.batch import SubstepGraphs
     host_rates = torch.from_numpy(scene.gas_source_rates).pin_memory()
     e2e_steps = max(1, min(args.steps, 100))
-    stepper = SubstepGraphs(sim, inputs=[sim.material.production_parameter], host_results=True).capture()
+    stepper = SubstepGraphs(sim, inputs=[sim.material.production_parameter], host_results=True,
+                            chained=True).capture()
     copy_stream = torch.cuda.Stream()
     torch.cuda.synchronize()
     if dist:

@@ -123,3 +123,34 @@ def test_substep_graphs_host_results():
     np.testing.assert_allclose(np.array(got), np.array(expected), rtol=1e-12)
     del stepper
     torch.cuda.synchronize()
+
+
+def test_chained_substep_graphs_match_eager_steps():
+    """SubstepGraphs(chained=True): every graph scatters the next substep's transport fields ahead and
+    uses the ones the previous substep scattered. Stepping the simulator outside the object in
+    between makes the next substep scatter its own fields. Both match eager stepping; a state
+    array given as an input is refused."""
+    import pytest
+    import torch
+    from baking_b200 import scenes
+    from baking_b200.batch import SubstepGraphs
+    sc = scenes.dough_ball(48, 20_000, seed=6, prestrain=0.05)
+    graphed = scenes.make_simulator(sc, diagnostics="lean")
+    eager = scenes.make_simulator(sc, diagnostics="lean")
+    with pytest.raises(ValueError):
+        SubstepGraphs(graphed, inputs=[graphed.current_state.transport_state.temperatures], chained=True)
+    stepper = SubstepGraphs(graphed, inputs=[graphed.material.production_parameter], chained=True).capture()
+    assert stepper.chained
+    stepper.Advance(5)
+    graphed.AdvanceUnchecked(3)   # outside the object: the next graph substep resynchronises
+    stepper.Advance(4)
+    for _ in range(14):
+        eager.Step()
+    assert graphed.step_count == eager.step_count == 14
+    dx = sc.simulation.grid_spacing
+    np.testing.assert_allclose(graphed.current_state.particle_positions.cpu().numpy(),
+                               eager.current_state.particle_positions.cpu().numpy(), rtol=0, atol=1e-4 * dx)
+    np.testing.assert_allclose(graphed.current_state.transport_state.temperatures.cpu().numpy(),
+                               eager.current_state.transport_state.temperatures.cpu().numpy(), rtol=1e-9)
+    del stepper
+    torch.cuda.synchronize()
