@@ -404,6 +404,7 @@ __global__ void k_check_finish(const double* __restrict__ partial, double* __res
     if (s == BK_CHECK_SIM_FLAG0 || s == BK_CHECK_SIM_FLAG1) v = (double)in.sim_flags[s - BK_CHECK_SIM_FLAG0];
     if (s >= BK_CHECK_DING_FLAG0 && s <= BK_CHECK_DING_FLAG2)
         v = in.ding_flags ? (double)in.ding_flags[s - BK_CHECK_DING_FLAG0] : 0.0;
+    if (s == BK_CHECK_SUBSTEP_STATUS) v = in.substep_status ? (double)in.substep_status[0] : 0.0;
     if (s == BK_CHECK_TRANSPORT_FLAG0 || s == BK_CHECK_TRANSPORT_FLAG1)
         v = in.transport_flags ? (double)in.transport_flags[s - BK_CHECK_TRANSPORT_FLAG0] : 0.0;
     if (s == BK_CHECK_RESIDUAL_MAX) {

@@ -57,6 +57,7 @@ struct Params {
     float ambient, density, elastic_modulus, cfl, peak, width;
     int keep_fields;
     int prescattered, prescatter_next;
+    int32_t* status;
 };
 
 Params to_params(const BkSubstepParams& p) {
@@ -86,6 +87,7 @@ Params to_params(const BkSubstepParams& p) {
     k.keep_fields = p.keep_transport_fields;
     k.prescattered = p.transport_prescattered;
     k.prescatter_next = p.transport_prescatter_next;
+    k.status = p.status;
     return k;
 }
 
@@ -505,12 +507,40 @@ __global__ void k_grid_update(Params P, GridPtrs g) {
 // per thread, then the warp-cooperative momentum scatter.
 // One particle's scatter record, six float4 (read as 128-bit broadcasts by the run loop):
 // {wx0 wx1 wx2 m} {wy0 wy1 wy2 q0} {wz0 wz1 wz2 q1} {A0 A1 A2 q2} {A3 A4 A5 -} {A6 A7 A8 -}.
+// The staged form first copies the block's particle planes (x, v, C, F and, for Ding, tau: 33
+// planes of 256 floats) into shared memory with bulk copies (cp.async.bulk, the TMA engine's 1-D
+// copy) issued by one thread and counted on an mbarrier, so the loads of a block are in flight
+// together and each thread then reads its particle's 33 values from shared memory; the scatter
+// records reuse that space once every thread has read it.
+constexpr int kP2GPlanes = 33;
 struct P2GSmem {
-    float4 rec[kThreads][6];
+    union {
+        float planes[kP2GPlanes][kThreads];  // x 0-2, v 3-5, C 6-14, F 15-23, tau 24-32
+        float4 rec[kThreads][6];
+    };
     float4 tile[kTileNodes];
+    unsigned long long mbar;
 };
 
+namespace stage {
+// Polls of a bulk copy's mbarrier before a block gives up (far beyond any copy's latency).
+constexpr uint32_t kWaitPolls = 1u << 22;
+
+__device__ __forceinline__ void arrive_expect_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// 1-D bulk copy global -> this CTA's shared memory, completing `bytes` on the mbarrier. Both
+// addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+}  // namespace stage
+
 // Four 256-thread blocks per SM (64 registers) measured faster than three at 77 registers.
+template <bool kStaged>
 __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
                                                  BkFlags flags, float* max_residuals) {
     __shared__ P2GSmem sm;
@@ -518,18 +548,61 @@ __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkSta
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t i = blockIdx.x * (int64_t)kThreads + tid;
     const int64_t pitch = P.pitch;
+    if constexpr (kStaged) {
+        // Planes are pitch-long with a pitch that is a multiple of 4 and 16-byte aligned bases (the
+        // host checks), so the block's range rounded up to 16 bytes stays inside each plane.
+        const uint32_t mbar = mlp::smem_addr(&sm.mbar);
+        if (tid == 0) mlp::mbar_init(mbar, 1);
+        __syncthreads();
+        const int64_t start = (int64_t)blockIdx.x * kThreads;
+        if (tid == 0) {
+            const int64_t count = P.n - start < kThreads ? P.n - start : kThreads;
+            const uint32_t bytes = (uint32_t)((count * 4 + 15) & ~15ll);
+            const int arrays = P.material == 1 ? 5 : 4;
+            const float* src[5] = {in.x, in.v, in.C, in.F, in.tau};
+            const int planes[5] = {3, 3, 9, 9, 9};
+            stage::arrive_expect_tx(mbar, bytes * (uint32_t)(P.material == 1 ? kP2GPlanes : kP2GPlanes - 9));
+            int k = 0;
+            for (int a = 0; a < arrays; ++a)
+                for (int c = 0; c < planes[a]; ++c, ++k)
+                    stage::copy(mlp::smem_addr(&sm.planes[k][0]), src[a] + c * pitch + start, bytes, mbar);
+        }
+        const bool arrived = __syncthreads_and(mlp::mbar_wait(mbar, 0, stage::kWaitPolls)) != 0;
+        if (!arrived) {
+            // Leave this block's particles unprocessed and report it; wait (bounded) for the copies
+            // still in flight into this block's shared memory before leaving.
+            if (tid == 0 && P.status) atomicExch(P.status, 1);
+            mlp::mbar_wait(mbar, 0, stage::kWaitPolls);
+            return;
+        }
+    }
+    // This particle's plane arrays: from the staged copies or from global memory.
+    auto ld_v3 = [&](const float* src, int plane0) {
+        if constexpr (kStaged) return V3{{sm.planes[plane0][tid], sm.planes[plane0 + 1][tid], sm.planes[plane0 + 2][tid]}};
+        else return load_v3(src, i, pitch);
+    };
+    auto ld_m3 = [&](const float* src, int plane0) {
+        if constexpr (kStaged) {
+            M3 r;
+#pragma unroll
+            for (int c = 0; c < 9; ++c) r.m[c] = sm.planes[plane0 + c][tid];
+            return r;
+        } else {
+            return load_m3(src, i, pitch);
+        }
+    };
     bool valid = false;
     Stencil st;
     st.b[0] = st.b[1] = st.b[2] = 0;
     float mass = 0.f, q[3] = {0.f, 0.f, 0.f}, A[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (i < P.n) {
-        V3 x = load_v3(in.x, i, pitch);
+        V3 x = ld_v3(in.x, 0);
         st = make_stencil(x, P.origin, P.dx, P.R);
         valid = st.valid;
         if (!valid) set_flag(flags.simulation, 1);
     }
     if (valid) {
-        M3 F = load_m3(in.F, i, pitch);
+        M3 F = ld_m3(in.F, 15);
         float J = det3(F);
         M3 tau;
         float T_mat = 0.f;
@@ -574,7 +647,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkSta
             if (P.material == 1) T_mat = in.material_temperature[i];
         }
         if (P.material == 1) {
-            tau = load_m3(in.tau, i, pitch);
+            tau = ld_m3(in.tau, 24);
             if (P.gas) {
                 float n = in.porosity[i];
                 if (n <= 0.0f || n >= 1.0f || !isfinite(n) || J <= 0.0f) {
@@ -612,8 +685,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkSta
             for (int e = 0; e < 9; ++e) tau.m[e] -= (e % 4) == 0 ? iso : iso * 0.0f;
         }
         float scale = P.dt * cst.volume[i] * 4.0f / (P.dx * P.dx);
-        M3 Cm = load_m3(in.C, i, pitch);
-        V3 vel = load_v3(in.v, i, pitch);
+        M3 Cm = ld_m3(in.C, 6);
+        V3 vel = ld_v3(in.v, 3);
 #pragma unroll
         for (int e = 0; e < 9; ++e) A[e] = mass * Cm.m[e] - scale * tau.m[e];
         // w (m v + A (o - l) dx) = w (q + A dx o) with q = m v - A l dx.
@@ -623,6 +696,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkSta
 #pragma unroll
         for (int e = 0; e < 9; ++e) A[e] *= P.dx;
     }
+    if constexpr (kStaged) __syncthreads();  // every thread has read its planes: the records reuse them
     {
         float w[3][3];
 #pragma unroll
@@ -1215,8 +1289,16 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
         if (int rc = check_launch("bk_substep/clear_previous")) return rc;
         {
             int rec = profile_begin("p2g", s);
-            k_p2g<<<particle_blocks, kThreads, 0, s>>>(P, *in, *out, *constants, g, *flags,
-                                                   diagnostics->max_residuals);
+            // Bulk staging needs 16-byte aligned plane starts: a pitch that is a multiple of 4 floats
+            // and 16-byte aligned array bases.
+            const uintptr_t bases = (uintptr_t)in->x | (uintptr_t)in->v | (uintptr_t)in->C | (uintptr_t)in->F |
+                                    (p.material == 1 ? (uintptr_t)in->tau : 0);
+            if (p.pitch % 4 == 0 && (bases & 15) == 0)
+                k_p2g<true><<<particle_blocks, kThreads, 0, s>>>(P, *in, *out, *constants, g, *flags,
+                                                                 diagnostics->max_residuals);
+            else
+                k_p2g<false><<<particle_blocks, kThreads, 0, s>>>(P, *in, *out, *constants, g, *flags,
+                                                                  diagnostics->max_residuals);
             profile_end(rec, s);
         }
         if (int rc = check_launch("bk_substep/p2g")) return rc;

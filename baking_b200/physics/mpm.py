@@ -526,6 +526,9 @@ class MpmSimulator:
         """physics/mpm.py:243-308: the same checks, messages and returned summary. ``values`` are the
         reduction's results when the caller already has them (Advance)."""
         v = self._check_values() if values is None else values
+        if v["substep_status"]:
+            raise RuntimeError("a substep kernel gave up waiting for a device copy or tensor-core result; "
+                               "its particles were left unprocessed")
         if v["sim_flag0"]:
             raise RuntimeError("nonpositive/nonfinite J; reduce dt or inspect loading and sampling")
         if v["sim_flag1"]:

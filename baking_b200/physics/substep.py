@@ -66,7 +66,7 @@ class BkSubstepParams(C.Structure):
                 ("elastic_modulus", C.c_float), ("cfl_limit", C.c_float), ("gas_peak", C.c_float),
                 ("gas_width", C.c_float), ("surrogate", C.POINTER(BkReturnSurrogate)),
                 ("keep_transport_fields", C.c_int32), ("transport_prescattered", C.c_int32),
-                ("transport_prescatter_next", C.c_int32)]
+                ("transport_prescatter_next", C.c_int32), ("status", P)]
 
 
 PHASE_TRANSPORT = 1
@@ -81,14 +81,15 @@ class BkCheckInputs(C.Structure):
                 ("resolution", C.c_int32), ("water_enabled", C.c_int32), ("density", C.c_float),
                 ("water_density", C.c_float), ("water_stress", C.c_float), ("gas_modulus", C.c_float),
                 ("initial_porosity", C.c_float), ("node_pm", P), ("box", P), ("vertex_count", C.c_int64),
-                ("vertex_pitch", C.c_int64), ("vertices", P), ("tet_count", C.c_int64), ("tets", P)]
+                ("vertex_pitch", C.c_int64), ("vertices", P), ("tet_count", C.c_int64), ("tets", P),
+                ("substep_status", P)]
 
 
 # Slots of bk_check_state (include/baking_b200.h, BK_CHECK_*).
 CHECK_SLOTS = ("sim_flag0", "sim_flag1", "ding_flag0", "ding_flag1", "ding_flag2", "transport_flag0",
                "transport_flag1", "nonfinite_state", "j_min", "j_max", "outside_stencil", "speed_max", "gas_wave_max",
                "water_wave2_max", "nonfinite_ding", "residual_max", "particle_volume", "total_mass", "kinetic_energy",
-               "grid_mass", "nonfinite_vertices", "inverted_tets")
+               "grid_mass", "nonfinite_vertices", "inverted_tets", "substep_status")
 CHECK_BLOCKS = 296
 
 _SIGS = {
@@ -161,6 +162,7 @@ class SubstepEngine:
             self.grid.fields[k] = _p(self.fields[k])
         self.grid.node_dT_ratio, self.grid.bounds = _p(self.node_dT_ratio), _p(self.bounds)
         self.max_residuals = torch.zeros(2, dtype=torch.float32, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)  # BkSubstepParams.status
         self.surface = BkSurface()
         if self.transport:
             self._build_surface()
@@ -303,6 +305,7 @@ class SubstepEngine:
         p.keep_transport_fields = int(keep_fields)
         p.transport_prescattered = int(prescattered)
         p.transport_prescatter_next = int(prescatter_next)
+        p.status = _p(self.status)
         cst = self.constants(settling)
         sin = state_struct(state_in, self.is_ding, self.transport, self.gas)
         sout = state_struct(state_out, self.is_ding, self.transport, self.gas)
@@ -384,6 +387,7 @@ class SubstepEngine:
         verts = sim.vertex_positions
         c.vertex_count, c.vertex_pitch, c.vertices = verts.shape[0], arrays.layout_pitch(verts), _p(verts)
         c.tet_count, c.tets = self._check_tets.shape[0], _p(self._check_tets)
+        c.substep_status = _p(self.status)
         _lib.call_raw(self.lib.bk_check_state, "bk_check_state", C.byref(c), _p(self._check_out),
                       _p(self._check_scratch), _lib.stream_handle())
         return dict(zip(CHECK_SLOTS, self._check_out.tolist()))

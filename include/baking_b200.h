@@ -302,6 +302,9 @@ typedef struct BkSubstepParams {
                                        bounds[12..17] (grid bounds of 18 ints). Valid only for a next
                                        substep that starts from this output with nothing changed in
                                        between; needs the exact return map (no surrogate). */
+    int32_t *status;                /* optional (device, 1 int, may be NULL): set to 1 when a kernel gave
+                                       up a bounded wait (a bulk copy into shared memory or a
+                                       tensor-core completion) and left its particles unprocessed */
 } BkSubstepParams;
 
 #define BK_PHASE_TRANSPORT 1       /* surface terms, scalar P2G, diffusion */
@@ -545,6 +548,7 @@ enum {
     BK_CHECK_GRID_MASS,              /* node masses of the last substep's active box */
     BK_CHECK_NONFINITE_VERTICES,     /* mesh vertices with a nonfinite coordinate */
     BK_CHECK_INVERTED_TETS,          /* tets with signed volume <= 0 (or a vertex index out of range) */
+    BK_CHECK_SUBSTEP_STATUS,         /* BkSubstepParams.status (a bounded wait gave up) */
     BK_CHECK_SLOTS
 };
 
@@ -574,6 +578,7 @@ typedef struct {
     const float *vertices;                /* 3 planes of vertex_pitch floats */
     int64_t tet_count;
     const int32_t *tets;                  /* tet_count x 4 vertex ids */
+    const int32_t *substep_status;        /* BkSubstepParams.status, or NULL */
 } BkCheckInputs;
 
 /* out: BK_CHECK_SLOTS doubles (device); scratch: BK_MEASURE_BLOCKS * BK_CHECK_SLOTS doubles (device).
