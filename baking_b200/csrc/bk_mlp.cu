@@ -101,8 +101,12 @@ __global__ void __launch_bounds__(kRows) k_mlp_grad(int64_t batch, const float* 
     const int64_t i = (int64_t)blockIdx.x * kRows + t;
     const bool active = i < batch;
     const float inv_count = 1.0f / (float)(batch * kOutputs);
-    for (int k = 0; k < kFeatures; ++k)
-        s.X[k * kStride + t] = active ? bf16_round((features[i * 8 + k] - nm.in_mean[k]) / nm.in_scale[k]) : 0.f;
+    for (int k = 0; k < kFeatures; ++k) {
+        // the inference's two-term BF16 input: bf16(x) + bf16(x - bf16(x))
+        const float x = active ? (features[i * 8 + k] - nm.in_mean[k]) / nm.in_scale[k] : 0.f;
+        const float hi = bf16_round(x);
+        s.X[k * kStride + t] = hi + bf16_round(x - hi);
+    }
     __syncthreads();
     // forward: layer 1
     for (int j = 0; j < kHidden; ++j) {
@@ -227,7 +231,10 @@ __global__ void k_mlp_pack(const float* __restrict__ params, unsigned char* __re
     auto put = [&](int off, float x) { *reinterpret_cast<__nv_bfloat16*>(blob + off) = __float2bfloat16_rn(x); };
     if (t < kHidden * kIn) {  // W1^T: n x k (64 x 16)
         int n = t / kIn, k = t % kIn;
-        put(kW1Offset + operand_offset(n, k, kIn), k < kFeatures ? params[kP_W1 + k * kHidden + n] : 0.f);
+        // Columns 0-6 multiply the BF16 inputs, columns 8-14 the BF16 remainders x - bf16(x) of the
+        // same inputs (tile_eval): the same weights, so the layer sees x to ~16 bits, not 8.
+        const int f = k < kFeatures ? k : (k >= 8 && k < 8 + kFeatures ? k - 8 : -1);
+        put(kW1Offset + operand_offset(n, k, kIn), f >= 0 ? params[kP_W1 + f * kHidden + n] : 0.f);
     }
     if (t < kHidden * kHidden) {  // W2^T: 64 x 64
         int n = t / kHidden, k = t % kHidden;

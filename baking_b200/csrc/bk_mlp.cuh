@@ -216,12 +216,18 @@ __device__ inline bool tile_eval(TileSmem& s, const float* x, bool active, float
     const int row = threadIdx.x;
     const uint32_t lane_base = s.tmem_base + ((uint32_t)(row & ~31) << 16);
     {
-        float v[8];
+        // Layer-1 input (K = 16): the BF16 inputs in columns 0-6 and their BF16 remainders
+        // x - bf16(x) in columns 8-14, which the packed W1 multiplies by the same weights, so the
+        // first layer sees each input to ~16 significant bits instead of BF16's 8.
+        float v[8], r[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = (active && k < kFeatures) ? x[k] : 0.0f;
+        for (int k = 0; k < 8; ++k) {
+            const float xk = (active && k < kFeatures) ? x[k] : 0.0f;
+            v[k] = __bfloat162float(__float2bfloat16_rn(xk));
+            r[k] = xk - v[k];
+        }
         store_row8(s.act, row, 0, kIn, v);
-        float z[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        store_row8(s.act, row, 8, kIn, z);
+        store_row8(s.act, row, 8, kIn, r);
     }
     bool ok = tile_layer(s, kW1Offset, kIn, kHidden, phase++);
     const float* b1 = reinterpret_cast<const float*>(s.blob + kB1Offset);

@@ -1,7 +1,8 @@
 """CPU restatement of the return-map surrogate MLP (7 -> 64 -> 64 -> 3, SiLU) -- test infrastructure.
 
 The checker for the device kernels in ``baking_b200/csrc/bk_mlp.cu``: the forward pass with the
-tensor-core rounding (BF16 inputs, weights and hidden activations; FP32 accumulation and biases),
+tensor-core rounding (inputs as two BF16 terms, BF16 weights and hidden activations; FP32
+accumulation and biases),
 the gradient of the mean-squared loss through that forward (rounding treated as identity), one
 Adam step and the packed operand layout. The reference has no learned component, so there is no
 reference call site to pin this against: it is pinned by float64 finite differences of its own
@@ -57,12 +58,20 @@ def normalise(features, in_mean, in_scale):
     return ((f - np.asarray(in_mean, np.float32)[:FEATURES]) / np.asarray(in_scale, np.float32)[:FEATURES]).astype(np.float32)
 
 
+def two_term(x):
+    """The layer-1 input as the tensor cores see it: bf16(x) + bf16(x - bf16(x)) (the inputs and
+    their BF16 remainders share the first layer's weights)."""
+    x = np.asarray(x, np.float32)
+    hi = bf16(x)
+    return hi.astype(np.float64) + bf16((x - hi).astype(np.float32)).astype(np.float64)
+
+
 def forward(params, x, keep=False, exact=False):
     """Network outputs (in units of out_scale) for normalised inputs x[n, 7]. ``exact`` skips the
     BF16 rounding (float64 throughout), for checking the gradient formulas by finite differences."""
     W1, b1, W2, b2, W3, b3 = unpack(params)
     r = (lambda a: np.asarray(a, np.float64)) if exact else (lambda a: bf16(np.asarray(a, np.float32)).astype(np.float64))
-    xb = r(x)
+    xb = np.asarray(x, np.float64) if exact else two_term(x)
     z1 = xb @ r(W1) + b1
     h1 = r(_silu(z1))
     z2 = h1 @ r(W2) + b2
@@ -122,7 +131,8 @@ def pack(params):
 
     for n in range(HIDDEN):
         for k in range(16):
-            put(operand_offset(n, k, 16), W1[k, n] if k < FEATURES else 0.0)
+            f = k if k < FEATURES else (k - 8 if 8 <= k < 8 + FEATURES else -1)
+            put(operand_offset(n, k, 16), W1[f, n] if f >= 0 else 0.0)
         for k in range(HIDDEN):
             put(2048 + operand_offset(n, k, HIDDEN), W2[k, n])
     for n in range(16):
