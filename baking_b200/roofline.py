@@ -71,7 +71,13 @@ def fused_bytes(kernel, engine, active_nodes):
         if ding:
             per += 36 + 4 + 4 + (8 if tr else 4)    # Fe, porosity, gelled, temperature read
             per += 36 + 36 + 4 + 4                  # Fe, tau, porosity, gelled written
-        return per * n + 16 * active_nodes
+        node = 16
+        if engine.prescatter_allowed():
+            # Inside an Advance call the kernel also scatters the next substep's transport fields:
+            # V0 4, capacity 8, water 8 read (temperature counted above); 4 node fields written.
+            per += 4 + 8 + 8
+            node += 32
+        return per * n + node * active_nodes
     return None
 
 
