@@ -56,7 +56,7 @@ struct Params {
     float conductivity, diffusivity, s0, water_stress;
     float ambient, density, elastic_modulus, cfl, peak, width;
     int keep_fields;
-    int prescattered, prescatter_next;
+    int prescattered, prescatter_next, prescatter_stale;
     int32_t* status;
 };
 
@@ -87,6 +87,7 @@ Params to_params(const BkSubstepParams& p) {
     k.keep_fields = p.keep_transport_fields;
     k.prescattered = p.transport_prescattered;
     k.prescatter_next = p.transport_prescatter_next;
+    k.prescatter_stale = p.transport_prescatter_stale;
     k.status = p.status;
     return k;
 }
@@ -446,6 +447,22 @@ __global__ void __launch_bounds__(kDiffThreads) k_diffuse(Params P, GridPtrs g, 
             }
         }
         __syncthreads();
+    }
+}
+
+// Fields scattered ahead for a substep that runs its own scalar P2G instead (the state may have
+// changed in between): zero the volume, capacity, energy and water fields over their box.
+__global__ void k_clear_prescatter(Params P, GridPtrs g) {
+    int lo[3], ext[3];
+    int64_t count;
+    if (!box_of(g.bounds + 12, P.R, lo, ext, count)) return;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+        int c2 = lo[2] + (int)(t % ext[2]);
+        int c1 = lo[1] + (int)((t / ext[2]) % ext[1]);
+        int c0 = lo[0] + (int)(t / ((int64_t)ext[2] * ext[1]));
+        int64_t i = node_index(c0, c1, c2, P.R);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) g.f[k][i] = 0.0;
     }
 }
 
@@ -1227,7 +1244,7 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
     if (p.gas)
         BK_REQUIRE(p.transport && p.material == 1 && in->gas_moles && out->gas_moles && constants->gas_rate,
                    "bk_substep: gas mode needs transport, the Ding model and gas arrays");
-    if (p.transport_prescattered || p.transport_prescatter_next)
+    if (p.transport_prescattered || p.transport_prescatter_next || p.transport_prescatter_stale)
         BK_REQUIRE(p.transport && !p.keep_transport_fields,
                    "bk_substep: the transport prescatter needs transport and a grid update that clears the fields");
     if (p.transport_prescatter_next)
@@ -1266,6 +1283,10 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
             if (int rc = check_launch("bk_substep/surface_owners")) return rc;
         }
         if (!p.transport_prescattered) {
+            if (p.transport_prescatter_stale) {
+                k_clear_prescatter<<<box_blocks, kThreads, 0, s>>>(P, g);
+                if (int rc = check_launch("bk_substep/clear_prescatter")) return rc;
+            }
             {
                 int rec = profile_begin("transport_scatter", s);
                 k_transport_scatter<<<particle_blocks, kThreads, 0, s>>>(P, *in, *constants, g, flags->simulation);

@@ -66,7 +66,8 @@ class BkSubstepParams(C.Structure):
                 ("elastic_modulus", C.c_float), ("cfl_limit", C.c_float), ("gas_peak", C.c_float),
                 ("gas_width", C.c_float), ("surrogate", C.POINTER(BkReturnSurrogate)),
                 ("keep_transport_fields", C.c_int32), ("transport_prescattered", C.c_int32),
-                ("transport_prescatter_next", C.c_int32), ("status", P)]
+                ("transport_prescatter_next", C.c_int32), ("transport_prescatter_stale", C.c_int32),
+                ("status", P)]
 
 
 PHASE_TRANSPORT = 1
@@ -163,6 +164,9 @@ class SubstepEngine:
         self.grid.node_dT_ratio, self.grid.bounds = _p(self.node_dT_ratio), _p(self.bounds)
         self.max_residuals = torch.zeros(2, dtype=torch.float32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)  # BkSubstepParams.status
+        # True while the simulator's own grid holds transport fields scattered ahead that no substep
+        # has used yet (the last substep run on it had prescatter_next, or a chained graph did).
+        self.prescatter_pending = False
         self.surface = BkSurface()
         if self.transport:
             self._build_surface()
@@ -306,6 +310,13 @@ class SubstepEngine:
         p.transport_prescattered = int(prescattered)
         p.transport_prescatter_next = int(prescatter_next)
         p.status = _p(self.status)
+        own_grid = grid is None
+        if own_grid and (phases & PHASE_TRANSPORT) and self.transport:
+            if prescattered and not self.prescatter_pending:
+                raise RuntimeError("no transport fields were scattered ahead for this substep")
+            # fields scattered ahead that this substep does not use are cleared first
+            p.transport_prescatter_stale = int(self.prescatter_pending and not prescattered)
+            self.prescatter_pending = False
         cst = self.constants(settling)
         sin = state_struct(state_in, self.is_ding, self.transport, self.gas)
         sout = state_struct(state_out, self.is_ding, self.transport, self.gas)
@@ -323,6 +334,8 @@ class SubstepEngine:
                                  C.byref(self.surface), C.byref(diag), C.byref(self.flags), int(phases), stream)
         if rc != 0:
             raise RuntimeError(f"bk_substep failed ({rc}): {self.lib.bk_last_error().decode(errors='replace')}")
+        if own_grid and (phases & PHASE_MECHANICS):
+            self.prescatter_pending = bool(prescatter_next)
 
     def step_summary(self, state, out=None, out_ptr=None):
         """(grid mass of the last substep, kinetic energy of ``state``) as a float64 device tensor,

@@ -302,6 +302,9 @@ typedef struct BkSubstepParams {
                                        bounds[12..17] (grid bounds of 18 ints). Valid only for a next
                                        substep that starts from this output with nothing changed in
                                        between; needs the exact return map (no surrogate). */
+    int32_t transport_prescatter_stale; /* 1 with transport_prescattered = 0: fields an earlier G2P
+                                       scattered ahead (box in bounds[12..17]) are still on the grid
+                                       and are cleared before this substep's scalar P2G */
     int32_t *status;                /* optional (device, 1 int, may be NULL): set to 1 when a kernel gave
                                        up a bounded wait (a bulk copy into shared memory or a
                                        tensor-core completion) and left its particles unprocessed */
