@@ -164,8 +164,12 @@ __device__ BlockBox block_box(int* bounds, bool valid, const int* b, int tile_no
         bb.tiled = count <= tile_nodes;
         bb.count = bb.tiled ? (int)count : 0;
         if (threadIdx.x < 3) {
-            atomicMin(bounds + threadIdx.x, s_box[threadIdx.x]);
-            atomicMax(bounds + 3 + threadIdx.x, s_box[3 + threadIdx.x]);
+            // The shared box only widens (min of lo, max of hi), so a value read through L2 that is
+            // older than the current one is never narrower: a block whose box lies inside it
+            // skips the atomics, and thousands of blocks stop contending for six addresses.
+            const int t = threadIdx.x;
+            if (s_box[t] < __ldcg(bounds + t)) atomicMin(bounds + t, s_box[t]);
+            if (s_box[3 + t] > __ldcg(bounds + 3 + t)) atomicMax(bounds + 3 + t, s_box[3 + t]);
         }
     }
     return bb;
