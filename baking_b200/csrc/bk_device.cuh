@@ -261,104 +261,137 @@ BK_DEV void svd3_fast(const M3d& A, M3d& U, double s[3], M3d& V) {
     }
 }
 
-// 3x3 SVD A = U diag(s) V^T for the return map, and the principal log stretches e = log(s).
-//
-// The reference computes the SVD of the float32 trial gradient in float64 and rounds U, s and V to
-// float32 before using them (physics/materials/ding.py:106-109). Here:
-// * V: the eigenvectors of M = A^T A - I by cyclic Jacobi (Jacobi 1846; Golub-Van Loan 8.5) in
-//   float32, where M is formed in float64 from the float32 A and rounded once. Forming A^T A - I in
-//   float64 keeps M, whose entries are of the size of the strain, to float32 relative accuracy, so
-//   the eigenvalues q_c = s_c^2 - 1 come out with float32 relative accuracy even for strains of
-//   1e-6, where s itself differs from 1 by a few float32 ulps.
-// * s: s_c = 1 + q_c / (1 + sqrt(1 + q_c)) rounded once to float32, i.e. the reference's float32
-//   rounding of its float64 singular value (an exact sum rounded once), and e_c = log(s_c) as the
-//   reference takes the log of that rounded value. Below s^2 = 1/2 (compression beyond 0.7, where
-//   M no longer carries s^2 to relative accuracy) s_c is the norm of the column A v_c.
-// * U = A V diag(1 / |A v_c|).
-// Nearly equal singular values leave their singular vectors mixed by ~2^-24 / gap; the return map
-// uses the factors only through isotropic functions (U f(s) V^T, U g(s) U^T), which do not depend
-// on how the vectors are chosen within such a subspace: their change stays at float32 rounding.
-// Rank-deficient input (a zero singular value) falls back to the float64 one-sided solver.
+// 3x3 SVD A = U diag(s) V^T in float32 by one-sided Jacobi (Hestenes 1958), iterated to float32
+// convergence. The reference computes its SVD in float64 and rounds U, s and V to float32 before
+// using them (physics/materials/ding.py:106-109); a converged float32 Jacobi SVD carries errors of
+// the same few-ulp size, with a third of the registers and latency of the float64 solve.
+// Rank-deficient input (a zero singular value) falls back to the float64 solver. e = log(s), the
+// principal log stretches, as the reference takes the log of its rounded singular values.
 BK_DEV void svd3f(const M3& A, M3& U, float s[3], M3& V, float e[3]) {
-    float S[3][3];
+    float b[9];
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = i; j < 3; ++j) {
-            const double m = (double)A.m[i] * (double)A.m[j] + (double)A.m[3 + i] * (double)A.m[3 + j] +
-                             (double)A.m[6 + i] * (double)A.m[6 + j] - (i == j ? 1.0 : 0.0);
-            S[i][j] = S[j][i] = (float)m;
-        }
-    float fro = 0.0f;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) fro = fmaf(S[i][j], S[i][j], fro);
-    float v[3][3] = {{1.f, 0.f, 0.f}, {0.f, 1.f, 0.f}, {0.f, 0.f, 1.f}};
-    for (int sweep = 0; sweep < 5; ++sweep) {
+    for (int e = 0; e < 9; ++e) b[e] = A.m[e];
+    float v[9] = {1.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f, 1.f};
+    for (int sweep = 0; sweep < 6; ++sweep) {
         bool rotated = false;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const int p = k == 2 ? 1 : 0;
             const int q = k == 0 ? 1 : 2;
-            const int r = 3 - p - q;
-            const float apq = S[p][q];
-            if (apq * apq <= 1e-15f * fro) continue;
-            rotated = true;
-            const float theta = (S[q][q] - S[p][p]) / (2.0f * apq);
-            const float t = fabsf(theta) > 1e18f ? 0.5f / theta
-                                                 : copysignf(1.0f, theta) / (fabsf(theta) + sqrtf(fmaf(theta, theta, 1.0f)));
-            const float c = rsqrtf(fmaf(t, t, 1.0f));
-            const float sn = t * c;
-            S[p][p] -= t * apq;
-            S[q][q] += t * apq;
-            S[p][q] = S[q][p] = 0.0f;
-            const float arp = S[r][p], arq = S[r][q];
-            S[r][p] = S[p][r] = c * arp - sn * arq;
-            S[r][q] = S[q][r] = sn * arp + c * arq;
+            float alpha = 0.f, beta = 0.f, gamma = 0.f;
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-                const float vp = v[i][p], vq = v[i][q];
-                v[i][p] = c * vp - sn * vq;
-                v[i][q] = sn * vp + c * vq;
+            for (int r = 0; r < 3; ++r) {
+                alpha = fmaf(b[3 * r + p], b[3 * r + p], alpha);
+                beta = fmaf(b[3 * r + q], b[3 * r + q], beta);
+                gamma = fmaf(b[3 * r + p], b[3 * r + q], gamma);
+            }
+            // Columns orthogonal to 1e-6 (|gamma| <= 1e-6 sqrt(alpha beta)) are enough: the float64
+            // sweep below takes the off-diagonal terms from there to ~1e-12 / gap.
+            if (gamma * gamma <= 1e-12f * alpha * beta) continue;
+            rotated = true;
+            float zeta = (beta - alpha) / (2.0f * gamma);
+            float t = fabsf(zeta) > 1e18f ? 0.5f / zeta
+                                           : copysignf(1.0f, zeta) / (fabsf(zeta) + sqrtf(fmaf(zeta, zeta, 1.0f)));
+            float c = rsqrtf(fmaf(t, t, 1.0f));
+            float sn = c * t;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                float bp = b[3 * r + p], bq = b[3 * r + q];
+                b[3 * r + p] = c * bp - sn * bq;
+                b[3 * r + q] = sn * bp + c * bq;
+                float vp = v[3 * r + p], vq = v[3 * r + q];
+                v[3 * r + p] = c * vp - sn * vq;
+                v[3 * r + q] = sn * vp + c * vq;
             }
         }
         if (!rotated) break;
     }
+    // Finish in float64. The float32 rotations leave the columns of B = A V orthogonal to ~2^-24,
+    // but nearly equal singular values (small elastic strains) make float32 mix their singular
+    // vectors by ~2^-24 / gap. One float64 Jacobi sweep from this start reduces the off-diagonal
+    // terms to ~2^-48 / gap (Jacobi's quadratic convergence), after which s = |B_i| and U = B / s
+    // agree with the float64 SVD to float32 rounding.
+    // The accumulated float32 rotations are orthonormal only to ~1e-7, which would scale s by as
+    // much; re-orthonormalise them in float64 first (Gram-Schmidt, third column = cross product).
+    double vv[9], bb[9];
+    {
+        double c0[3] = {v[0], v[3], v[6]}, c1[3] = {v[1], v[4], v[7]};
+        double n0 = rsqrt(c0[0] * c0[0] + c0[1] * c0[1] + c0[2] * c0[2]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) c0[i] *= n0;
+        double d01 = c0[0] * c1[0] + c0[1] * c1[1] + c0[2] * c1[2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) c1[i] -= d01 * c0[i];
+        double n1 = rsqrt(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) c1[i] *= n1;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            vv[3 * i] = c0[i];
+            vv[3 * i + 1] = c1[i];
+        }
+        vv[2] = c0[1] * c1[2] - c0[2] * c1[1];
+        vv[5] = c0[2] * c1[0] - c0[0] * c1[2];
+        vv[8] = c0[0] * c1[1] - c0[1] * c1[0];
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            bb[3 * r + c] = (double)A.m[3 * r] * vv[c] + (double)A.m[3 * r + 1] * vv[3 + c] +
+                            (double)A.m[3 * r + 2] * vv[6 + c];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int p = k == 2 ? 1 : 0;
+        const int q = k == 0 ? 1 : 2;
+        double alpha = 0, beta = 0, gamma = 0;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            alpha += bb[3 * r + p] * bb[3 * r + p];
+            beta += bb[3 * r + q] * bb[3 * r + q];
+            gamma += bb[3 * r + p] * bb[3 * r + q];
+        }
+        if (gamma * gamma <= 1e-30 * alpha * beta) continue;
+        // tan of the rotation angle, t = 2 gamma sign(d) / (|d| + sqrt(d^2 + 4 gamma^2)), d = beta - alpha.
+        double d = beta - alpha;
+        double t = 2.0 * gamma / (d >= 0.0 ? d + sqrt(d * d + 4.0 * gamma * gamma) : d - sqrt(d * d + 4.0 * gamma * gamma));
+        double c = rsqrt(1.0 + t * t);
+        double sn = c * t;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            double bp = bb[3 * r + p], bq = bb[3 * r + q];
+            bb[3 * r + p] = c * bp - sn * bq;
+            bb[3 * r + q] = sn * bp + c * bq;
+            double vp = vv[3 * r + p], vq = vv[3 * r + q];
+            vv[3 * r + p] = c * vp - sn * vq;
+            vv[3 * r + q] = sn * vp + c * vq;
+        }
+    }
     bool degenerate = false;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        float b[3];
+        double n2 = bb[c] * bb[c] + bb[3 + c] * bb[3 + c] + bb[6 + c] * bb[6 + c];
+        degenerate |= !(n2 > 1e-30);
+        double inv = rsqrt(n2);
+        s[c] = (float)(n2 * inv);
 #pragma unroll
-        for (int r = 0; r < 3; ++r) b[r] = A.m[3 * r] * v[0][c] + A.m[3 * r + 1] * v[1][c] + A.m[3 * r + 2] * v[2][c];
-        const float n2 = b[0] * b[0] + b[1] * b[1] + b[2] * b[2];
-        degenerate |= !(n2 > 1e-30f);
-        const float inv = rsqrtf(n2);
-#pragma unroll
-        for (int r = 0; r < 3; ++r) U.m[3 * r + c] = b[r] * inv;
-        const float q = S[c][c];
-        const float sigma = q >= -0.5f ? 1.0f + q / (1.0f + sqrtf(1.0f + q)) : n2 * inv;
-        s[c] = sigma;
-        e[c] = logf(sigma);
+        for (int r = 0; r < 3; ++r) U.m[3 * r + c] = (float)(bb[3 * r + c] * inv);
     }
 #pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) V.m[3 * i + j] = v[i][j];
+    for (int e = 0; e < 9; ++e) V.m[e] = (float)vv[e];
     if (degenerate) {
         M3d Ad, Ud, Vd;
         double sd[3];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) Ad.m[k] = (double)A.m[k];
+        for (int e = 0; e < 9; ++e) Ad.m[e] = (double)A.m[e];
         svd3(Ad, Ud, sd, Vd);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) { U.m[k] = (float)Ud.m[k]; V.m[k] = (float)Vd.m[k]; }
+        for (int e = 0; e < 9; ++e) { U.m[e] = (float)Ud.m[e]; V.m[e] = (float)Vd.m[e]; }
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            s[k] = (float)sd[k];
-            e[k] = logf(s[k]);
-        }
+        for (int k = 0; k < 3; ++k) s[k] = (float)sd[k];
     }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) e[k] = logf(s[k]);
 }
 
 // ------------------------------------------------- physics/transfer.py:4-28
