@@ -80,7 +80,7 @@ BK_DEV M3 inverse3(const M3& a) {
 // plane rotations orthogonalise A's columns; column norms are the singular values.
 // Out of line: the hot kernels reach it only for rank-deficient input, and inlining it there would
 // put its code between their hot instructions.
-__device__ __noinline__ void svd3(const M3d& A, M3d& U, double s[3], M3d& V) {
+static __device__ __noinline__ void svd3(const M3d& A, M3d& U, double s[3], M3d& V) {
     double b[9];
 #pragma unroll
     for (int e = 0; e < 9; ++e) b[e] = A.m[e];
@@ -547,7 +547,7 @@ BK_DEV double porosity_prediction_slope(double n, float qf, float pf, float df, 
 }
 
 // The reference's 64-step bisection of n -> prediction(n) on [0, 1 - 1e-9] (porous_return.py:51-61).
-__device__ __noinline__ float solve_porosity_bisection(float q, float p, float d, float h, float e, double Vp, float n0,
+static __device__ __noinline__ float solve_porosity_bisection(float q, float p, float d, float h, float e, double Vp, float n0,
                                       double* warm = nullptr) {
     double lo = 0.0, hi = 1.0 - 1.0e-9;
     for (int it = 0; it < 64; ++it) {
