@@ -443,35 +443,83 @@ __global__ void k_tadj_diffuse(TParams P, BkGridFields g, const int32_t* __restr
 }
 
 // ------------------------------------------------------------------ scatter
-// Node fields (volume V0 det F, capacity, capacity T, W) += w (...) for every particle.
+// Node fields (volume V0 det F, capacity, capacity T, W) += w (...) for every particle: the
+// reverse of that scatter is a 27-node gather of the four field adjoints. The block first stages
+// the adjoints of its particles' node box in shared memory (when the box fits kScatterTile nodes),
+// so that the gathers read shared memory.
+constexpr int kScatterTile = 512;
+
 __global__ void __launch_bounds__(kThreads) k_tadj_scatter(TParams P, BkState in, BkConstants cst, BkGridFields g,
                                                          BkAdjointTransport a, const BkAdjointState adj) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
+    __shared__ double s_bar[4][kScatterTile];
+    __shared__ int s_box[6];
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + tid;
     const int64_t pitch = P.pitch;
-    Stencil st = make_stencil(load_v3(in.x, i, pitch), P.origin, P.dx, P.R);
-    if (!st.valid) return;
+    Stencil st;
+    st.valid = false;
+    st.b[0] = st.b[1] = st.b[2] = 0;
+    if (i < P.n) st = make_stencil(load_v3(in.x, i, pitch), P.origin, P.dx, P.R);
+    const bool valid = i < P.n && st.valid;
+    // the block's node box
+    if (tid < 6) s_box[tid] = tid < 3 ? INT_MAX : INT_MIN;
+    __syncthreads();
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        const int lo = __reduce_min_sync(0xffffffffu, valid ? st.b[ax] : INT_MAX);
+        const int hi = __reduce_max_sync(0xffffffffu, valid ? st.b[ax] + 2 : INT_MIN);
+        if (lane == 0 && lo != INT_MAX) {
+            atomicMin(&s_box[ax], lo);
+            atomicMax(&s_box[3 + ax], hi);
+        }
+    }
+    __syncthreads();
+    int lo[3] = {0, 0, 0}, ext[3] = {1, 1, 1};
+    int count = 0;
+    if (s_box[0] != INT_MAX) {
+        long long c = 1;
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            lo[ax] = s_box[ax];
+            ext[ax] = s_box[3 + ax] - s_box[ax] + 1;
+            c *= ext[ax];
+        }
+        count = c <= kScatterTile ? (int)c : 0;
+    }
+    for (int t = tid; t < count; t += kThreads) {
+        const int z = t % ext[2], y = (t / ext[2]) % ext[1], x = t / (ext[2] * ext[1]);
+        const int64_t node = node_index(lo[0] + x, lo[1] + y, lo[2] + z, P.R);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) s_bar[f][t] = g.field_bar[f][node];
+    }
+    __syncthreads();  // uniform: every thread reaches it
+    if (!valid) return;
     const M3 F = load_m3(in.F, i, pitch);
     const double vol = (double)cst.volume[i] * (double)det3(F);
     const double cap = cst.capacity[i], T = in.temperature[i], W = in.water[i];
     double volb = 0.0, Tb = 0.0, Wb = 0.0;
     const float inv_dx = 1.f / P.dx;
     float xg[3] = {0.f, 0.f, 0.f};
-#pragma unroll 1
+#pragma unroll 3
     for (int j = 0; j < 27; ++j) {
         int ox, oy, oz;
         node_offset(j, ox, oy, oz);
         float dw[3];
         const double w = (double)weight_and_grad(st, ox, oy, oz, inv_dx, dw);
-        const int64_t node = node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R);
-        const double f0 = g.field_bar[0][node], f1 = g.field_bar[1][node], f2 = g.field_bar[2][node],
-                     f3 = g.field_bar[3][node];
+        double f0, f1, f2, f3;
+        if (count > 0) {
+            const int t = ((st.b[0] + ox - lo[0]) * ext[1] + (st.b[1] + oy - lo[1])) * ext[2] + (st.b[2] + oz - lo[2]);
+            f0 = s_bar[0][t]; f1 = s_bar[1][t]; f2 = s_bar[2][t]; f3 = s_bar[3][t];
+        } else {
+            const int64_t node = node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R);
+            f0 = g.field_bar[0][node]; f1 = g.field_bar[1][node]; f2 = g.field_bar[2][node]; f3 = g.field_bar[3][node];
+        }
         volb += w * f0;
         Tb += w * cap * f2;
         Wb += w * f3;
-        const float s = (float)(vol * f0 + cap * f1 + cap * T * f2 + W * f3);
+        const float sv = (float)(vol * f0 + cap * f1 + cap * T * f2 + W * f3);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) xg[c] += dw[c] * s;
+        for (int c = 0; c < 3; ++c) xg[c] += dw[c] * sv;
     }
     a.temperature_in[i] += Tb;
     a.water_in[i] += Wb;
