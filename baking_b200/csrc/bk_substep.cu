@@ -163,7 +163,7 @@ __device__ BlockBox block_box(int* bounds, bool valid, const int* b, int tile_no
         }
         bb.tiled = count <= tile_nodes;
         bb.count = bb.tiled ? (int)count : 0;
-        if (threadIdx.x < 3 && bounds) {
+        if (threadIdx.x < 3) {
             // The shared box only widens (min of lo, max of hi), so a value read through L2 that is
             // older than the current one is never narrower: a block whose box lies inside it
             // skips the atomics, and thousands of blocks stop contending for six addresses.
@@ -622,15 +622,6 @@ __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkSta
         valid = st.valid;
         if (!valid) set_flag(flags.simulation, 1);
     }
-    const BlockBox bb = block_box(g.bounds, valid, st.b);  // synchronises the block
-    // The block's node box of (dT, dW/W) staged in the momentum tile's space: the 27-node scalar
-    // gathers below then read shared memory instead of global memory.
-    double2* const sdtr = reinterpret_cast<double2*>(sm.tile);
-    const bool dtr_staged = P.transport && bb.count > 0;  // uniform across the block
-    if (dtr_staged) {
-        for (int t = tid; t < bb.count; t += kThreads) sdtr[t] = __ldg(g.dTr + tile_node(bb, t, P.R));
-        __syncthreads();
-    }
     if (valid) {
         M3 F = ld_m3(in.F, 15);
         float J = det3(F);
@@ -647,9 +638,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkSta
 #pragma unroll
                     for (int oz = 0; oz < 3; ++oz) {
                         double w = (double)(st.w[0][ox] * st.w[1][oy] * st.w[2][oz]);
-                        double2 d = dtr_staged
-                                        ? sdtr[tile_index(bb, st.b[0] + ox, st.b[1] + oy, st.b[2] + oz)]
-                                        : __ldg(g.dTr + node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R));
+                        double2 d = __ldg(g.dTr + node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R));
                         dTp += w * d.x;
                         ratio += w * d.y;
                     }
@@ -728,7 +717,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkSta
 #pragma unroll
         for (int e = 0; e < 9; ++e) A[e] *= P.dx;
     }
-    __syncthreads();  // every thread has read its planes and scalar nodes: records and tile reuse them
+    if constexpr (kStaged) __syncthreads();  // every thread has read its planes: the records reuse them
     {
         float w[3][3];
 #pragma unroll
@@ -742,6 +731,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkSta
         sm.rec[tid][4] = make_float4(A[3], A[4], A[5], 0.f);
         sm.rec[tid][5] = make_float4(A[6], A[7], A[8], 0.f);
     }
+    const BlockBox bb = block_box(g.bounds, valid, st.b);  // synchronises the block
     for (int t = tid; t < bb.count; t += kThreads) sm.tile[t] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
     long long key = valid ? pack_base(st.b) : -1;
@@ -810,10 +800,8 @@ __device__ __forceinline__ void atomic_max_nonneg(float* addr, float value) {
 // v = sum w v_i and C = 4/dx^2 sum w v_i (o_i - l) dx, accumulated as the moments
 // S = sum w v_i and M_c = sum w v_i o_ic with the stencil offsets o_i in {0, 1, 2} known at compile
 // time; C_rc = 4/dx (M_rc - l_c S_r).
-// With `vtile` the block's node velocities over `vbox` are staged in shared memory and read there.
 __device__ __forceinline__ bool g2p_gather(const Params& P, const BkState& in, const BkState& out, const GridPtrs& g,
-                                           const BkFlags& flags, int64_t i, M3& Fn, M3& Cn,
-                                           const float4* vtile = nullptr, const BlockBox* vbox = nullptr) {
+                                           const BkFlags& flags, int64_t i, M3& Fn, M3& Cn) {
     const int64_t pitch = P.pitch;
     V3 xi = load_v3(in.x, i, pitch);
     Stencil st = make_stencil(xi, P.origin, P.dx, P.R);
@@ -821,8 +809,6 @@ __device__ __forceinline__ bool g2p_gather(const Params& P, const BkState& in, c
     float nv[3] = {0.f, 0.f, 0.f}, mo[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     const float4* vbase = g.v + node_index(st.b[0], st.b[1], st.b[2], P.R);
     const int64_t R = P.R;
-    const float4* tbase = vtile ? vtile + tile_index(*vbox, st.b[0], st.b[1], st.b[2]) : nullptr;
-    const int ty = vtile ? vbox->ext[2] : 0, tx = vtile ? vbox->ext[1] * vbox->ext[2] : 0;
 #pragma unroll
     for (int ox = 0; ox < 3; ++ox)
 #pragma unroll
@@ -831,7 +817,7 @@ __device__ __forceinline__ bool g2p_gather(const Params& P, const BkState& in, c
 #pragma unroll
             for (int oz = 0; oz < 3; ++oz) {
                 float w = wxy * st.w[2][oz];
-                float4 u = tbase ? tbase[ox * tx + oy * ty + oz] : __ldg(vbase + (ox * R + oy) * R + oz);
+                float4 u = __ldg(vbase + (ox * R + oy) * R + oz);
                 float wu[3] = {w * u.x, w * u.y, w * u.z};
 #pragma unroll
                 for (int r = 0; r < 3; ++r) {
@@ -1018,10 +1004,9 @@ __device__ bool ding_surrogate(const DingParamsDev& D, const DingPrelude& d, flo
 // yielding particles on the sampling stride append (features, return) rows.
 __device__ __forceinline__ void g2p_return_particle(const Params& P, const BkState& in, const BkState& out,
                                                     const BkConstants& cst, const GridPtrs& g, const BkDiagnostics& diag,
-                                                    const BkFlags& flags, const SurrogateDev& sg, int64_t i,
-                                                    const float4* vtile, const BlockBox* vbox) {
+                                                    const BkFlags& flags, const SurrogateDev& sg, int64_t i) {
     M3 Fn, Cn;
-    if (!g2p_gather(P, in, out, g, flags, i, Fn, Cn, vtile, vbox)) return;
+    if (!g2p_gather(P, in, out, g, flags, i, Fn, Cn)) return;
     if (P.material != 1) return;
     const int64_t pitch = P.pitch;
     float T = P.transport ? (float)out.temperature[i] : in.material_temperature[i];
@@ -1054,10 +1039,6 @@ __device__ __forceinline__ void g2p_return_particle(const Params& P, const BkSta
 // Shared-memory node tile of the transport prescatter in k_g2p_return (128 particles per block).
 constexpr int kG2PTile = 256;
 using G2PTransportTile = TransportTile<128, kG2PTile>;
-// Node velocities of a block's box staged for the G2P gather (the same dynamic shared memory, which
-// the prescatter reuses afterwards).
-constexpr int kG2PVelTile = 256;
-constexpr size_t kG2PVelBytes = kG2PVelTile * sizeof(float4);
 
 __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
                                                    BkDiagnostics diag, BkFlags flags, SurrogateDev sg) {
@@ -1067,29 +1048,13 @@ __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkS
         g.bounds[6 + threadIdx.x] = g.bounds[threadIdx.x];
         g.bounds[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
     }
-    // Stage the node velocities of the block's stencil box (when it fits the tile) so that the 27
-    // gathers of each particle read shared memory.
-    extern __shared__ __align__(16) unsigned char g2p_smem[];
-    float4* const vtile = reinterpret_cast<float4*>(g2p_smem);
-    bool valid0 = false;
-    Stencil st0;
-    st0.b[0] = st0.b[1] = st0.b[2] = 0;
-    if (i < P.n) {
-        st0 = make_stencil(load_v3(in.x, i, P.pitch), P.origin, P.dx, P.R);
-        valid0 = st0.valid;
-    }
-    const BlockBox vbox = block_box(nullptr, valid0, st0.b, kG2PVelTile);  // synchronises the block
-    if (vbox.count > 0) {
-        for (int t = threadIdx.x; t < vbox.count; t += blockDim.x) vtile[t] = __ldg(g.v + tile_node(vbox, t, P.R));
-        __syncthreads();
-    }
-    if (i < P.n) g2p_return_particle(P, in, out, cst, g, diag, flags, sg, i, vbox.count > 0 ? vtile : nullptr, &vbox);
+    if (i < P.n) g2p_return_particle(P, in, out, cst, g, diag, flags, sg, i);
     if (P.prescatter_next) {
-        __syncthreads();  // the velocity tile is read: the prescatter reuses its memory
         // The next substep's scalar P2G (thermal_water.py:108-137) from the state just written:
         // x' and F' by this thread (read back with plain loads), T' and W' by this substep's P2G.
         // The grid update has zeroed the transport fields over this substep's box and restarted
         // the prescatter box bounds[12..17]. Uniform branch: every thread of the block scatters.
+        extern __shared__ __align__(16) unsigned char g2p_smem[];
         G2PTransportTile& sm = *reinterpret_cast<G2PTransportTile*>(g2p_smem);
         const int64_t pitch = P.pitch;
         bool valid = false;
@@ -1378,8 +1343,7 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
             profile_end(rec, s);
         } else {
             int rec = profile_begin("g2p_return", s);
-            const size_t smem = p.transport_prescatter_next && sizeof(G2PTransportTile) > kG2PVelBytes
-                                    ? sizeof(G2PTransportTile) : kG2PVelBytes;
+            const size_t smem = p.transport_prescatter_next ? sizeof(G2PTransportTile) : 0;
             k_g2p_return<<<blocks_for(p.n, 128), 128, smem, s>>>(P, *in, *out, *constants, g, *diagnostics, *flags, sg);
             profile_end(rec, s);
         }
