@@ -230,37 +230,22 @@ __global__ void k_refresh_gas(int64_t n, int64_t pitch, const double* __restrict
 }
 
 // ----------------------------------------------- mesh_tracking.py:13-38
-__global__ void k_reconstruct_vertices(int64_t nv, int64_t pitch, const float* __restrict__ x,
-                                       const float* __restrict__ F, int64_t vpitch,
-                                       const float* __restrict__ ref_vertices, const int32_t* __restrict__ offsets,
-                                       const int32_t* __restrict__ particles, const float* __restrict__ weights,
-                                       int64_t bpitch, const float* __restrict__ ref_offsets,
-                                       float* __restrict__ out) {
-    int64_t vtx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (vtx >= nv) return;
-    int b0 = offsets[vtx], b1 = offsets[vtx + 1];
-    if (b0 == b1) {
-        store_v3(out, vtx, vpitch, load_v3(ref_vertices, vtx, vpitch));
-        return;
-    }
-    auto predict = [&](int b, float* r) {
-        int p = particles[b];
-        M3 f = load_m3(F, p, pitch);
-        V3 xp = load_v3(x, p, pitch), o = load_v3(ref_offsets, b, bpitch);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) r[a] = xp.v[a] + (f.m[3 * a] * o.v[0] + f.m[3 * a + 1] * o.v[1] + f.m[3 * a + 2] * o.v[2]);
-    };
-    float anchor[3], disp[3] = {0, 0, 0};
-    predict(b0, anchor);
-    for (int b = b0; b < b1; ++b) {
-        float pred[3];
-        predict(b, pred);
-        float w = weights[b];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) disp[a] += w * (pred[a] - anchor[a]);
-    }
-    V3 o{{anchor[0] + disp[0], anchor[1] + disp[1], anchor[2] + disp[2]}};
-    store_v3(out, vtx, vpitch, o);
+// One block per vertex (a vertex of a finely sampled mesh binds hundreds to thousands of particles:
+// a block keeps enough of their gathers in flight and reduces the weighted sum), the block size
+// chosen from the mean bindings per vertex.
+template <int kVB>
+__global__ void __launch_bounds__(kVB) k_reconstruct_vertices(int64_t pitch, const float* __restrict__ x,
+                                                            const float* __restrict__ F, int64_t vpitch,
+                                                            const float* __restrict__ ref_vertices,
+                                                            const int32_t* __restrict__ offsets,
+                                                            const int32_t* __restrict__ particles,
+                                                            const float* __restrict__ weights, int64_t bpitch,
+                                                            const float* __restrict__ ref_offsets,
+                                                            float* __restrict__ out) {
+    const int vtx = blockIdx.x;
+    const float v = vertex_block<kVB>(offsets, particles, weights, ref_offsets, bpitch, ref_vertices, vpitch, x, F,
+                                      pitch, vtx);
+    if (threadIdx.x < 3) out[threadIdx.x * vpitch + vtx] = v;
 }
 
 // --------------------------------------------- thermal_water.py:77-92
@@ -658,9 +643,26 @@ int bk_reconstruct_mesh_vertices(int64_t vertex_count, int64_t pitch, const floa
     BK_EMPTY_OK(vertex_count);
     BK_REQUIRE(x && F && reference_vertices && offsets && particles && weights && reference_offsets && out_vertices,
                "bk_reconstruct_mesh_vertices: null pointer");
-    k_reconstruct_vertices<<<blocks_for(vertex_count), kBlock, 0, S(stream)>>>(
-        vertex_count, pitch, x, F, vertex_pitch, reference_vertices, offsets, particles, weights, binding_pitch,
-        reference_offsets, out_vertices);
+    BK_REQUIRE(vertex_count <= INT32_MAX, "bk_reconstruct_mesh_vertices: too many vertices");
+    const unsigned nv = (unsigned)vertex_count;
+    // binding_pitch bounds the total bindings: the launch-size hint of vertex_block_threads
+    switch (vertex_block_threads(vertex_count, binding_pitch)) {
+        case 256:
+            k_reconstruct_vertices<256><<<nv, 256, 0, S(stream)>>>(pitch, x, F, vertex_pitch, reference_vertices, offsets,
+                                                                  particles, weights, binding_pitch, reference_offsets,
+                                                                  out_vertices);
+            break;
+        case 128:
+            k_reconstruct_vertices<128><<<nv, 128, 0, S(stream)>>>(pitch, x, F, vertex_pitch, reference_vertices, offsets,
+                                                                  particles, weights, binding_pitch, reference_offsets,
+                                                                  out_vertices);
+            break;
+        default:
+            k_reconstruct_vertices<32><<<nv, 32, 0, S(stream)>>>(pitch, x, F, vertex_pitch, reference_vertices, offsets,
+                                                                particles, weights, binding_pitch, reference_offsets,
+                                                                out_vertices);
+            break;
+    }
     return check_launch("bk_reconstruct_mesh_vertices");
 }
 

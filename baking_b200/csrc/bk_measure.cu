@@ -165,13 +165,24 @@ __global__ void __launch_bounds__(kThreads) k_measure(BkMeasureInputs in, double
     }
 }
 
+// One slot's block partials reduced by one warp: lane l combines partials l, l + 32, ... in that
+// order, then a fixed butterfly combines the lanes (a deterministic order, whatever the schedule).
+__device__ __forceinline__ double warp_slot_reduce(int op, const double* __restrict__ partial, int blocks, int stride,
+                                                   int slot) {
+    const int lane = threadIdx.x & 31;
+    double v = op == kMin ? INFINITY : (op == kMax ? -INFINITY : 0.0);
+    for (int b = lane; b < blocks; b += 32) v = combine(op, v, partial[(int64_t)b * stride + slot]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = combine(op, v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
 __global__ void k_measure_finish(const double* __restrict__ partial, double* __restrict__ out, int blocks,
                                  int has_ding, int has_gas, int has_transport, int has_mesh) {
-    const int s = threadIdx.x;
-    if (s >= kSlots) return;
+    const int s = blockIdx.x;  // one warp per slot
     const int op = slot_op(s);
-    double v = partial[s];
-    for (int b = 1; b < blocks; ++b) v = combine(op, v, partial[(int64_t)b * kSlots + s]);
+    double v = warp_slot_reduce(op, partial, blocks, kSlots, s);
+    if (threadIdx.x != 0) return;
     const bool ding = s >= BK_MEASURE_MATERIAL_T_SUM && s <= BK_MEASURE_GELLED;
     const bool gas = s >= BK_MEASURE_GAS_TOTAL && s <= BK_MEASURE_PORE_VOLUME;
     const bool transport = s >= BK_MEASURE_T_MIN && s <= BK_MEASURE_SATURATION_MAX;
@@ -231,11 +242,9 @@ __global__ void __launch_bounds__(kThreads) k_step_summary(int64_t n, int64_t pi
 }
 
 __global__ void k_step_summary_finish(const double* __restrict__ partial, double* __restrict__ out, int blocks) {
-    const int k = threadIdx.x;
-    if (k >= 2) return;
-    double v = 0.0;
-    for (int b = 0; b < blocks; ++b) v += partial[2 * b + k];
-    out[k] = v;
+    const int k = blockIdx.x;  // one warp per value
+    const double v = warp_slot_reduce(kSum, partial, blocks, 2, k);
+    if (threadIdx.x == 0) out[k] = v;
 }
 
 // ------------------------------------------------------------------ CheckState
@@ -396,11 +405,10 @@ __global__ void __launch_bounds__(kThreads) k_check_state(BkCheckInputs in, doub
 
 __global__ void k_check_finish(const double* __restrict__ partial, double* __restrict__ out, int blocks,
                                BkCheckInputs in) {
-    const int s = threadIdx.x;
-    if (s >= kCheckSlots) return;
+    const int s = blockIdx.x;  // one warp per slot
     const int op = check_op(s);
-    double v = partial[s];
-    for (int b = 1; b < blocks; ++b) v = combine(op, v, partial[(int64_t)b * kCheckSlots + s]);
+    double v = warp_slot_reduce(op, partial, blocks, kCheckSlots, s);
+    if (threadIdx.x != 0) return;
     if (s == BK_CHECK_SIM_FLAG0 || s == BK_CHECK_SIM_FLAG1) v = (double)in.sim_flags[s - BK_CHECK_SIM_FLAG0];
     if (s >= BK_CHECK_DING_FLAG0 && s <= BK_CHECK_DING_FLAG2)
         v = in.ding_flags ? (double)in.ding_flags[s - BK_CHECK_DING_FLAG0] : 0.0;
@@ -434,7 +442,7 @@ extern "C" int bk_step_summary(const BkSubstepParams* params, const BkState* sta
                                                           reinterpret_cast<const float4*>(grid->node_pm),
                                                           grid->bounds + 6, p.resolution, scratch);
     if (int rc = check_launch("bk_step_summary")) return rc;
-    k_step_summary_finish<<<1, 32, 0, s>>>(scratch, out, BK_MEASURE_BLOCKS);
+    k_step_summary_finish<<<2, 32, 0, s>>>(scratch, out, BK_MEASURE_BLOCKS);
     return check_launch("bk_step_summary/finish");
 }
 
@@ -455,7 +463,7 @@ extern "C" int bk_measure_state(const BkMeasureInputs* in, double* out, double* 
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     k_measure<<<BK_MEASURE_BLOCKS, kThreads, 0, s>>>(m, scratch);
     if (int rc = check_launch("bk_measure_state")) return rc;
-    k_measure_finish<<<1, 64, 0, s>>>(scratch, out, BK_MEASURE_BLOCKS, m.porosity != nullptr, m.gas_moles != nullptr,
+    k_measure_finish<<<kSlots, 32, 0, s>>>(scratch, out, BK_MEASURE_BLOCKS, m.porosity != nullptr, m.gas_moles != nullptr,
                                       m.temperature != nullptr, m.vertex_count > 0);
     return check_launch("bk_measure_state/finish");
 }
@@ -479,6 +487,6 @@ extern "C" int bk_check_state(const BkCheckInputs* in, double* out, double* scra
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     k_check_state<<<BK_MEASURE_BLOCKS, kThreads, 0, s>>>(c, scratch);
     if (int rc = check_launch("bk_check_state")) return rc;
-    k_check_finish<<<1, 32, 0, s>>>(scratch, out, BK_MEASURE_BLOCKS, c);
+    k_check_finish<<<kCheckSlots, 32, 0, s>>>(scratch, out, BK_MEASURE_BLOCKS, c);
     return check_launch("bk_check_state/finish");
 }
