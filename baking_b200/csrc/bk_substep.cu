@@ -1155,7 +1155,10 @@ __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkSta
         }
         if (sg.path_counts && path >= 0) atomicAdd(&s_counts[path], 1);
         __syncthreads();
-        if (ts.failed) break;  // read after a barrier, so every thread takes the same branch
+        if (ts.failed) {  // read after a barrier, so every thread takes the same branch
+            if (threadIdx.x == 0 && P.status) atomicExch(P.status, 1);  // later tiles stay unprocessed
+            break;
+        }
     }
     mlp::tile_teardown(ts);
     if (sg.path_counts && threadIdx.x < 3 && s_counts[threadIdx.x]) atomicAdd(sg.path_counts + threadIdx.x, s_counts[threadIdx.x]);
