@@ -153,7 +153,12 @@ def test_recorder_regions_follow_the_order(tmp_path):
     sim.SortParticles()
     after = rec.Measure()
     for key, value in before.items():
-        if isinstance(value, float):
+        if key == "energy_balance_error_j":
+            # energy - initial energy - heat exchanged: a difference of float64 sums over the
+            # particles, which a new summation order moves at the rounding level of the sums
+            scale = abs(before["thermal_energy_j"])
+            assert after[key] == pytest.approx(value, abs=1e-11 * scale), key
+        elif isinstance(value, float):
             assert after[key] == pytest.approx(value, rel=1e-9, abs=1e-12), key
         else:
             assert after[key] == value, key
