@@ -2,20 +2,27 @@
 
 Each instance keeps its own state, grid and parameters (different particle counts, grids, oven
 temperatures). Two substeps of every instance -- state A -> B and B -> A, which brings the
-ping-pong states back -- are captured once into a CUDA graph, instances spread over several
-streams so that the kernels of small bodies run side by side on the GPU. ``Advance`` replays
-the graph: one host call per two substeps of the whole batch, no per-kernel launch cost.
+ping-pong states back -- are captured once into a CUDA graph. ``Advance`` replays the graph: one
+host call per two substeps of the whole batch, no per-kernel launch cost.
+
+With ``launch="table"`` (the default) each stage of the substep is ONE launch for the whole batch
+over a device table of the instances (``bk_batch_create``/``bk_batch_substep``): 8-10 launches per
+substep whatever the batch size, each filling the GPU with the blocks of every instance. With
+``launch="streams"`` every instance launches its own kernels, spread over several streams so that
+the kernels of small bodies run side by side.
 """
 from __future__ import annotations
+
+import ctypes
 
 import torch
 
 from . import _lib
-from .physics.substep import PHASE_MECHANICS, PHASE_TRANSPORT
+from .physics.substep import PHASE_MECHANICS, PHASE_TRANSPORT, BkBatchInstance
 
 
 class BatchedSimulators:
-    def __init__(self, simulators, streams=8):
+    def __init__(self, simulators, streams=8, launch="table"):
         self.sims = list(simulators)
         if not self.sims:
             raise ValueError("no simulators")
@@ -24,9 +31,14 @@ class BatchedSimulators:
                 raise ValueError("batched simulators must be past settling (settling_duration_s = 0)")
             if sim.retain_history:
                 raise ValueError("batched simulators keep no history")
+        if launch not in ("table", "streams"):
+            raise ValueError(f"launch must be 'table' or 'streams', not {launch!r}")
+        self.launch = launch
         self.device = self.sims[0].device
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(max(1, int(streams)))]
         self.graph = None
+        self._table = None      # bk_batch_create handle
+        self._layout = None     # the state pairs (and surrogates) the table and the graph were made for
         self.particle_count = sum(s.particle_data.particle_count for s in self.sims)
 
     @staticmethod
@@ -38,7 +50,51 @@ class BatchedSimulators:
         if sim.transport is not None:
             eng.accumulate_surface(state_out.transport_state)
 
+    def _current_layout(self):
+        return tuple((id(sim._current), id(sim.next_state), id(sim._engine.surrogate)) for sim in self.sims)
+
+    def _ensure_layout(self):
+        """(Re)build the instance table, and drop a captured graph, when a simulator's ping-pong
+        pair or surrogate is not the one they were made for (an odd number of substeps taken
+        outside the batch swaps the pair)."""
+        layout = self._current_layout()
+        if layout == self._layout:
+            return
+        self.graph = None
+        self._free_table()
+        if self.launch == "table":
+            lib = self.sims[0]._engine.lib
+            table = (BkBatchInstance * len(self.sims))()
+            for k, sim in enumerate(self.sims):
+                table[k] = sim._engine.batch_instance(sim._current, sim.next_state)
+            handle = ctypes.c_void_p()
+            _lib.call_raw(lib.bk_batch_create, "bk_batch_create", table, len(self.sims), ctypes.byref(handle))
+            self._table = handle
+        self._layout = layout
+
+    def _free_table(self):
+        if self._table is not None and self._table.value:
+            self.sims[0]._engine.lib.bk_batch_destroy(self._table)
+        self._table = None
+
+    def __del__(self):
+        try:
+            self._free_table()
+        except Exception:
+            pass
+
     def _record(self):
+        self._ensure_layout()
+        if self.launch == "table":
+            # parity 0 steps every instance A -> B and scatters B's transport fields ahead;
+            # parity 1 steps B -> A on them
+            lib = self.sims[0]._engine.lib
+            stream = _lib.stream_handle()
+            phases = PHASE_TRANSPORT | PHASE_MECHANICS
+            for parity, prescattered, ahead in ((0, 0, 1), (1, 1, 0)):
+                _lib.call_raw(lib.bk_batch_substep, "bk_batch_substep", self._table, parity, phases, prescattered,
+                              ahead, stream)
+            return
         main = torch.cuda.current_stream()
         for k, sim in enumerate(self.sims):
             s = self.streams[k % len(self.streams)]
@@ -54,6 +110,7 @@ class BatchedSimulators:
     def capture(self):
         """Build the graph (the simulators' kernels run once outside capture first, to load and
         configure every kernel; that run advances each instance by two substeps)."""
+        self._ensure_layout()
         torch.cuda.synchronize()
         self._record()
         torch.cuda.synchronize()
@@ -74,6 +131,8 @@ class BatchedSimulators:
         if steps % 2:
             raise ValueError("steps must be even (the graph holds a pair of ping-pong substeps)")
         if graph:
+            if self._current_layout() != self._layout:
+                self._ensure_layout()  # drops a graph made for other state pairs
             if self.graph is None:
                 self.capture()
             for _ in range(steps // 2):

@@ -269,6 +269,11 @@ BK_DEV void svd3_fast(const M3d& A, M3d& U, double s[3], M3d& V) {
 // the same few-ulp size, with a third of the registers and latency of the float64 solve.
 // Rank-deficient input (a zero singular value) falls back to the float64 solver. e = log(s), the
 // principal log stretches, as the reference takes the log of its rounded singular values.
+// kPolish = false stops after the float32 sweeps (columns orthogonal to ~2e-7): the factors then
+// reproduce A to float32 rounding, but nearly equal singular values leave their singular vectors
+// mixed by ~2^-24 / gap, so U, s and V no longer round like the reference's. The surrogate return
+// (an approximation to ~1e-3 by construction) takes that form.
+template <bool kPolish = true>
 BK_DEV void svd3f(const M3& A, M3& U, float s[3], M3& V, float e[3]) {
     float b[9];
 #pragma unroll
@@ -287,9 +292,10 @@ BK_DEV void svd3f(const M3& A, M3& U, float s[3], M3& V, float e[3]) {
                 beta = fmaf(b[3 * r + q], b[3 * r + q], beta);
                 gamma = fmaf(b[3 * r + p], b[3 * r + q], gamma);
             }
-            // Columns orthogonal to 1e-6 (|gamma| <= 1e-6 sqrt(alpha beta)) are enough: the float64
-            // sweep below takes the off-diagonal terms from there to ~1e-12 / gap.
-            if (gamma * gamma <= 1e-12f * alpha * beta) continue;
+            // Columns orthogonal to 1e-6 (|gamma| <= 1e-6 sqrt(alpha beta)) are enough when the
+            // float64 sweep below takes the off-diagonal terms from there to ~1e-12 / gap; without
+            // it the sweeps go on to ~2e-7, the float32 rounding level.
+            if (gamma * gamma <= (kPolish ? 1e-12f : 4e-14f) * alpha * beta) continue;
             rotated = true;
             float zeta = (beta - alpha) / (2.0f * gamma);
             float t = fabsf(zeta) > 1e18f ? 0.5f / zeta
@@ -307,6 +313,34 @@ BK_DEV void svd3f(const M3& A, M3& U, float s[3], M3& V, float e[3]) {
             }
         }
         if (!rotated) break;
+    }
+    if constexpr (!kPolish) {
+        bool degenerate = false;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const float n2 = b[c] * b[c] + b[3 + c] * b[3 + c] + b[6 + c] * b[6 + c];
+            degenerate |= !(n2 > 1e-30f);
+            const float inv = rsqrtf(n2);
+            s[c] = n2 * inv;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) U.m[3 * r + c] = b[3 * r + c] * inv;
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) V.m[k] = v[k];
+        if (degenerate) {
+            M3d Ad, Ud, Vd;
+            double sd[3];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) Ad.m[k] = (double)A.m[k];
+            svd3(Ad, Ud, sd, Vd);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) { U.m[k] = (float)Ud.m[k]; V.m[k] = (float)Vd.m[k]; }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) s[k] = (float)sd[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) e[k] = logf(s[k]);
+        return;
     }
     // Finish in float64. The float32 rotations leave the columns of B = A V orthogonal to ~2^-24,
     // but nearly equal singular values (small elastic strains) make float32 mix their singular
@@ -705,6 +739,7 @@ struct DingPrelude {
     int gel;
 };
 
+template <bool kPolish = true>
 BK_DEV bool ding_prelude(const DingParamsDev& P, const M3& Fe_old, float por, int gel, const M3& C_new, float T,
                          float eta_base, int32_t* flags, DingPrelude& d) {
     if (!isfinite(por) || por < 0.0f || por >= 1.0f) { set_flag(flags, 0); return false; }
@@ -723,7 +758,7 @@ BK_DEV bool ding_prelude(const DingParamsDev& P, const M3& Fe_old, float por, in
     for (int e = 0; e < 9; ++e) G.m[e] = P.dt * C_new.m[e] + ((e % 4) == 0 ? 1.0f : 0.0f);
     const M3 trial = matmul(G, Fe_old);
     d.det_trial = det3(trial);
-    svd3f(trial, d.U, d.s, d.V, d.e);
+    svd3f<kPolish>(trial, d.U, d.s, d.V, d.e);
     d.ty = ty;
     d.eta = eta;
     d.T_eff = Teff;

@@ -24,9 +24,12 @@
 // The active node box (min/max stencil node of the current particles) bounds
 // every dense grid pass; the grid passes leave the scatter fields zeroed behind
 // them, so no dense memset is needed between substeps.
+#include <algorithm>
 #include <cfloat>
 #include <climits>
 #include <cstdio>
+#include <type_traits>
+#include <vector>
 
 #include "baking_b200.h"
 #include "bk_common.h"
@@ -110,6 +113,21 @@ GridPtrs grid_ptrs(const BkGrid& g) {
     return r;
 }
 
+// The block a kernel body runs as: its index among the blocks given to its simulator and their
+// number. A plain launch gives one simulator the whole grid; a batched launch (below) splits its
+// grid between the simulators of an instance table.
+struct Slot {
+    int block, blocks;
+};
+__device__ __forceinline__ Slot grid_slot() { return Slot{(int)blockIdx.x, (int)gridDim.x}; }
+
+// How a kernel body takes its parameter structs: by value from a plain launch's parameter space
+// (a reference to a kernel parameter would make the compiler copy it to local memory), by
+// reference to the batched launch's shared-memory entry (a value copy would hold every field in
+// registers).
+template <class T, bool kRef>
+using Arg = typename std::conditional<kRef, const T&, const T>::type;
+
 // Stencil node j in 0..26 -> offsets (j / 9, (j / 3) % 3, j % 3), the reference's loop order.
 __device__ __forceinline__ void node_offset(int j, int& ox, int& oy, int& oz) {
     ox = j / 9;
@@ -189,20 +207,28 @@ __device__ __forceinline__ int64_t tile_node(const BlockBox& bb, int t, int R) {
 // ------------------------------------------------------------------ surface
 // geometry/mesh_tracking.py:13-38 restricted to the vertices of boundary faces; one block per
 // vertex (a vertex binds thousands of particles: a block keeps enough gathers in flight).
-template <int kBlock>
-__global__ void __launch_bounds__(kBlock) k_surface_vertices(Params P, const float* __restrict__ x,
-                                                          const float* __restrict__ F, BkSurface sf) {
-    const int vid = sf.vertex_ids[blockIdx.x];
+template <int kBlock, bool kRef = false>
+__device__ __forceinline__ void surface_vertices_body(Arg<Params, kRef> P, const float* __restrict__ x,
+                                                      const float* __restrict__ F, Arg<BkSurface, kRef> sf, Slot sl) {
+    const int vid = sf.vertex_ids[sl.block];
     const float v = vertex_block<kBlock>(sf.binding_offsets, sf.binding_particles, sf.binding_weights,
                                            sf.reference_offsets, sf.binding_pitch, sf.reference_vertices,
                                            sf.vertex_pitch, x, F, P.pitch, vid);
     if (threadIdx.x < 3) sf.vertices[threadIdx.x * sf.vertex_pitch + vid] = v;
 }
 
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock) k_surface_vertices(Params P, const float* __restrict__ x,
+                                                          const float* __restrict__ F, BkSurface sf) {
+    surface_vertices_body<kBlock>(P, x, F, sf, grid_slot());
+}
+
 // physics/thermal_water.py:77-92 (face areas, tray contact) and the surface terms of :108-122,
 // per face-owning particle, scattered into the heat/loss/exchange node fields.
-__global__ void k_surface_owners(Params P, BkState in, BkConstants cst, BkSurface sf, GridPtrs g, int32_t* sim_flags) {
-    int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+template <bool kRef = false>
+__device__ __forceinline__ void surface_owners_body(Arg<Params, kRef> P, Arg<BkState, kRef> in, Arg<BkConstants, kRef> cst,
+                                                    Arg<BkSurface, kRef> sf, Arg<GridPtrs, kRef> g, int32_t* sim_flags, Slot sl) {
+    int64_t o = sl.block * (int64_t)blockDim.x + threadIdx.x;
     if (o >= sf.owner_count) return;
     const int64_t vp = sf.vertex_pitch, pitch = P.pitch;
     int p = sf.owners[o];
@@ -250,14 +276,23 @@ __global__ void k_surface_owners(Params P, BkState in, BkConstants cst, BkSurfac
     }
 }
 
+__global__ void k_surface_owners(Params P, BkState in, BkConstants cst, BkSurface sf, GridPtrs g, int32_t* sim_flags) {
+    surface_owners_body(P, in, cst, sf, g, sim_flags, grid_slot());
+}
+
 // ---------------------------------------------------------- transport P2G
 // physics/thermal_water.py:108-137 (volume, capacity, energy, water), warp-cooperative per stencil run.
 // The block routine scatters its threads' particles; each thread passes its stencil, whether it is
 // valid, and its four values (V0 det F, capacity, capacity T, W). Every thread of the block calls it.
+// A run's sums are formed in float32 and added to the float64 node fields (the reference adds each
+// particle's float64 term): within a run of at most 32 particles that moves a node sum by ~1e-7
+// relative, and the node temperature E/C by ~3e-5 K, whose flux over a substep changes
+// temperatures by ~1e-13 K. The run loop then issues float32 multiply-adds and one 16-byte
+// broadcast load per particle instead of float64 ones and a conversion per node.
 template <int kT, int kTile>
 struct TransportTile {
     float w[kT][9];
-    double val[kT][4];
+    float4 val[kT];
     double tile[4][kTile];
 };
 
@@ -265,8 +300,8 @@ template <int kT, int kTile>
 __device__ void transport_scatter_block(TransportTile<kT, kTile>& sm, const Params& P, const GridPtrs& g, int* box,
                                         bool valid, const Stencil& st, const double* val) {
     const int tid = threadIdx.x, lane = tid & 31;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) sm.val[tid][k] = valid ? val[k] : 0.0;
+    sm.val[tid] = valid ? make_float4((float)val[0], (float)val[1], (float)val[2], (float)val[3])
+                        : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -288,20 +323,23 @@ __device__ void transport_scatter_block(TransportTile<kT, kTile>& sm, const Para
         int e = starts ? __ffs(starts) - 1 : 32;
         int b0 = __shfl_sync(kFull, st.b[0], s), b1 = __shfl_sync(kFull, st.b[1], s), b2 = __shfl_sync(kFull, st.b[2], s);
         if (lane < 27) {
-            double acc[4] = {0.0, 0.0, 0.0, 0.0};
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
             for (int k = warp_base + s; k < warp_base + e; ++k) {
-                double w = (double)(sm.w[k][ox] * sm.w[k][3 + oy] * sm.w[k][6 + oz]);
-#pragma unroll
-                for (int f = 0; f < 4; ++f) acc[f] += w * sm.val[k][f];
+                const float w = sm.w[k][ox] * sm.w[k][3 + oy] * sm.w[k][6 + oz];
+                const float4 v = sm.val[k];
+                acc[0] = fmaf(w, v.x, acc[0]);
+                acc[1] = fmaf(w, v.y, acc[1]);
+                acc[2] = fmaf(w, v.z, acc[2]);
+                acc[3] = fmaf(w, v.w, acc[3]);
             }
             if (bb.tiled) {
                 int t = tile_index(bb, b0 + ox, b1 + oy, b2 + oz);
 #pragma unroll
-                for (int f = 0; f < 4; ++f) atomicAdd(&sm.tile[f][t], acc[f]);
+                for (int f = 0; f < 4; ++f) atomicAdd(&sm.tile[f][t], (double)acc[f]);
             } else {
                 int64_t node = node_index(b0 + ox, b1 + oy, b2 + oz, P.R);
 #pragma unroll
-                for (int f = 0; f < 4; ++f) atomicAdd(g.f[f] + node, acc[f]);
+                for (int f = 0; f < 4; ++f) atomicAdd(g.f[f] + node, (double)acc[f]);
             }
         }
     }
@@ -314,10 +352,13 @@ __device__ void transport_scatter_block(TransportTile<kT, kTile>& sm, const Para
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkState in, BkConstants cst, GridPtrs g,
-                                                               int32_t* sim_flags) {
-    __shared__ TransportTile<kThreads, kTileNodes> sm;
-    const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+using ScatterTile = TransportTile<kThreads, kTileNodes>;
+
+template <bool kRef = false>
+__device__ __forceinline__ void transport_scatter_body(ScatterTile& sm, Arg<Params, kRef> P, Arg<BkState, kRef> in,
+                                                       Arg<BkConstants, kRef> cst, Arg<GridPtrs, kRef> g, int32_t* sim_flags,
+                                                       Slot sl) {
+    const int64_t i = sl.block * (int64_t)kThreads + threadIdx.x;
     const int64_t pitch = P.pitch;
     bool valid = false;
     Stencil st;
@@ -336,6 +377,12 @@ __global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkStat
         val[3] = in.water[i];
     }
     transport_scatter_block<kThreads, kTileNodes>(sm, P, g, g.bounds, valid, st, val);
+}
+
+__global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkState in, BkConstants cst, GridPtrs g,
+                                                               int32_t* sim_flags) {
+    __shared__ ScatterTile sm;
+    transport_scatter_body(sm, P, in, cst, g, sim_flags, grid_slot());
 }
 
 // ------------------------------------------------------------ grid passes
@@ -369,9 +416,18 @@ constexpr int kDiffThreads = kDiffX * kDiffY * kDiffZ;
 constexpr int kHaloX = kDiffX + 2, kHaloY = kDiffY + 2, kHaloZ = kDiffZ + 2;
 constexpr int kHaloNodes = kHaloX * kHaloY * kHaloZ;
 
-__global__ void __launch_bounds__(kDiffThreads) k_diffuse(Params P, GridPtrs g, int32_t* errors) {
-    __shared__ double s_V[kHaloNodes], s_T[kHaloNodes], s_S[kHaloNodes];
-    __shared__ unsigned char s_ok[kHaloNodes];
+struct DiffuseSmem {
+    double V[kHaloNodes], T[kHaloNodes], S[kHaloNodes];
+    unsigned char ok[kHaloNodes];
+};
+
+template <bool kRef = false>
+__device__ __forceinline__ void diffuse_body(DiffuseSmem& sm, Arg<Params, kRef> P, Arg<GridPtrs, kRef> g, int32_t* errors,
+                                             Slot sl) {
+    double* s_V = sm.V;
+    double* s_T = sm.T;
+    double* s_S = sm.S;
+    unsigned char* s_ok = sm.ok;
     int lo[3], ext[3];
     int64_t count;
     // The node box of the transport fields: built by this substep's scalar P2G, or by the previous
@@ -388,7 +444,7 @@ __global__ void __launch_bounds__(kDiffThreads) k_diffuse(Params P, GridPtrs g, 
     const int tiles = tiles_x * tiles_y * tiles_z;
     const int tid = threadIdx.x;
     const int tz = tid % kDiffZ, ty = (tid / kDiffZ) % kDiffY, tx = tid / (kDiffZ * kDiffY);
-    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    for (int tile = sl.block; tile < tiles; tile += sl.blocks) {
         const int t0[3] = {lo[0] + (tile / (tiles_z * tiles_y)) * kDiffX, lo[1] + ((tile / tiles_z) % tiles_y) * kDiffY,
                            lo[2] + (tile % tiles_z) * kDiffZ};
         // Stage the tile and its halo (nodes outside the grid are marked empty, like the reference's
@@ -454,13 +510,19 @@ __global__ void __launch_bounds__(kDiffThreads) k_diffuse(Params P, GridPtrs g, 
     }
 }
 
+__global__ void __launch_bounds__(kDiffThreads) k_diffuse(Params P, GridPtrs g, int32_t* errors) {
+    __shared__ DiffuseSmem sm;
+    diffuse_body(sm, P, g, errors, grid_slot());
+}
+
 // Fields scattered ahead for a substep that runs its own scalar P2G instead (the state may have
 // changed in between): zero the volume, capacity, energy and water fields over their box.
-__global__ void k_clear_prescatter(Params P, GridPtrs g) {
+template <bool kRef = false>
+__device__ __forceinline__ void clear_prescatter_body(Arg<Params, kRef> P, Arg<GridPtrs, kRef> g, Slot sl) {
     int lo[3], ext[3];
     int64_t count;
     if (!box_of(g.bounds + 12, P.R, lo, ext, count)) return;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t t = sl.block * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)sl.blocks * blockDim.x) {
         int c2 = lo[2] + (int)(t % ext[2]);
         int c1 = lo[1] + (int)((t / ext[2]) % ext[1]);
         int c0 = lo[0] + (int)(t / ((int64_t)ext[2] * ext[1]));
@@ -470,14 +532,17 @@ __global__ void k_clear_prescatter(Params P, GridPtrs g) {
     }
 }
 
+__global__ void k_clear_prescatter(Params P, GridPtrs g) { clear_prescatter_body(P, g, grid_slot()); }
+
 // GridState.Clear (physics/grid.py:14-17) restricted to the previous substep's active box, the only
 // nodes holding nonzero momentum, mass or velocity; the grid of the last substep stays readable
 // until the next one starts.
-__global__ void k_clear_previous(Params P, GridPtrs g) {
+template <bool kRef = false>
+__device__ __forceinline__ void clear_previous_body(Arg<Params, kRef> P, Arg<GridPtrs, kRef> g, Slot sl) {
     int lo[3], ext[3];
     int64_t count;
     if (!box_of(g.bounds + 6, P.R, lo, ext, count)) return;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t t = sl.block * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)sl.blocks * blockDim.x) {
         int c2 = lo[2] + (int)(t % ext[2]);
         int c1 = lo[1] + (int)((t / ext[2]) % ext[1]);
         int c0 = lo[0] + (int)(t / ((int64_t)ext[2] * ext[1]));
@@ -487,16 +552,19 @@ __global__ void k_clear_previous(Params P, GridPtrs g) {
     }
 }
 
+__global__ void k_clear_previous(Params P, GridPtrs g) { clear_previous_body(P, g, grid_slot()); }
+
 // physics/grid.py:20-38 over the active box; clears the transport scatter fields behind it.
-__global__ void k_grid_update(Params P, GridPtrs g) {
+template <bool kRef = false>
+__device__ __forceinline__ void grid_update_body(Arg<Params, kRef> P, Arg<GridPtrs, kRef> g, Slot sl) {
     int lo[3], ext[3];
     int64_t count;
     // The G2P that follows builds the next substep's transport box in bounds[12..17]: restart it
     // empty (this substep's diffusion, its only reader, has finished; no block here reads it).
-    if (P.prescatter_next && blockIdx.x == 0 && threadIdx.x < 6) g.bounds[12 + threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
+    if (P.prescatter_next && sl.block == 0 && threadIdx.x < 6) g.bounds[12 + threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
     if (!box_of(g.bounds, P.R, lo, ext, count)) return;
     const int R = P.R, bc = P.bc;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t t = sl.block * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)sl.blocks * blockDim.x) {
         int c[3];
         c[2] = lo[2] + (int)(t % ext[2]);
         c[1] = lo[1] + (int)((t / ext[2]) % ext[1]);
@@ -521,6 +589,8 @@ __global__ void k_grid_update(Params P, GridPtrs g) {
         }
     }
 }
+
+__global__ void k_grid_update(Params P, GridPtrs g) { grid_update_body(P, g, grid_slot()); }
 
 // ------------------------------------------------------------- fused P2G
 // Scalar G2P (thermal_water.py:206-229), local gas source (:238-245), gas stress (gas.py:16-35),
@@ -561,13 +631,13 @@ __device__ __forceinline__ void copy(uint32_t dst, const void* src, uint32_t byt
 }  // namespace stage
 
 // Four 256-thread blocks per SM (64 registers) measured faster than three at 77 registers.
-template <bool kStaged>
-__global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
-                                                 BkFlags flags, float* max_residuals) {
-    __shared__ P2GSmem sm;
-    if (blockIdx.x == 0 && threadIdx.x < 2) max_residuals[threadIdx.x] = 0.0f;
+template <bool kStaged, bool kRef = false>
+__device__ __forceinline__ void p2g_body(P2GSmem& sm, Arg<Params, kRef> P, Arg<BkState, kRef> in, Arg<BkState, kRef> out,
+                                         Arg<BkConstants, kRef> cst, Arg<GridPtrs, kRef> g, Arg<BkFlags, kRef> flags,
+                                         float* max_residuals, Slot sl) {
+    if (sl.block == 0 && threadIdx.x < 2) max_residuals[threadIdx.x] = 0.0f;
     const int tid = threadIdx.x, lane = tid & 31;
-    const int64_t i = blockIdx.x * (int64_t)kThreads + tid;
+    const int64_t i = sl.block * (int64_t)kThreads + tid;
     const int64_t pitch = P.pitch;
     if constexpr (kStaged) {
         // Planes are pitch-long with a pitch that is a multiple of 4 and 16-byte aligned bases (the
@@ -575,7 +645,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkSta
         const uint32_t mbar = mlp::smem_addr(&sm.mbar);
         if (tid == 0) mlp::mbar_init(mbar, 1);
         __syncthreads();
-        const int64_t start = (int64_t)blockIdx.x * kThreads;
+        const int64_t start = (int64_t)sl.block * kThreads;
         if (tid == 0) {
             const int64_t count = P.n - start < kThreads ? P.n - start : kThreads;
             const uint32_t bytes = (uint32_t)((count * 4 + 15) & ~15ll);
@@ -784,6 +854,13 @@ __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkSta
         if (v.w == 0.0f && v.x == 0.0f && v.y == 0.0f && v.z == 0.0f) continue;
         atomicAdd(g.pm + tile_node(bb, t, P.R), v);
     }
+}
+
+template <bool kStaged>
+__global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
+                                                 BkFlags flags, float* max_residuals) {
+    __shared__ P2GSmem sm;
+    p2g_body<kStaged>(sm, P, in, out, cst, g, flags, max_residuals, grid_slot());
 }
 
 // ------------------------------------------------------ fused G2P + return
@@ -1040,10 +1117,13 @@ __device__ __forceinline__ void g2p_return_particle(const Params& P, const BkSta
 constexpr int kG2PTile = 256;
 using G2PTransportTile = TransportTile<128, kG2PTile>;
 
-__global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
-                                                   BkDiagnostics diag, BkFlags flags, SurrogateDev sg) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (blockIdx.x == 0 && threadIdx.x < 6) {
+template <bool kRef = false>
+__device__ __forceinline__ void g2p_return_body(unsigned char* g2p_smem, Arg<Params, kRef> P, Arg<BkState, kRef> in,
+                                                Arg<BkState, kRef> out, Arg<BkConstants, kRef> cst, Arg<GridPtrs, kRef> g,
+                                                Arg<BkDiagnostics, kRef> diag, Arg<BkFlags, kRef> flags, Arg<SurrogateDev, kRef> sg,
+                                                Slot sl) {
+    const int64_t i = sl.block * (int64_t)blockDim.x + threadIdx.x;
+    if (sl.block == 0 && threadIdx.x < 6) {
         // This substep's box becomes the box the next substep clears; the active box restarts empty.
         g.bounds[6 + threadIdx.x] = g.bounds[threadIdx.x];
         g.bounds[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
@@ -1054,7 +1134,6 @@ __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkS
         // x' and F' by this thread (read back with plain loads), T' and W' by this substep's P2G.
         // The grid update has zeroed the transport fields over this substep's box and restarted
         // the prescatter box bounds[12..17]. Uniform branch: every thread of the block scatters.
-        extern __shared__ __align__(16) unsigned char g2p_smem[];
         G2PTransportTile& sm = *reinterpret_cast<G2PTransportTile*>(g2p_smem);
         const int64_t pitch = P.pitch;
         bool valid = false;
@@ -1078,26 +1157,36 @@ __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkS
     }
 }
 
+__global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
+                                                   BkDiagnostics diag, BkFlags flags, SurrogateDev sg) {
+    extern __shared__ __align__(16) unsigned char g2p_smem[];
+    g2p_return_body(g2p_smem, P, in, out, cst, g, diag, flags, sg, grid_slot());
+}
+
 // G2P + return map with the learned surrogate: a persistent CTA walks 128-particle tiles and
 // evaluates the network for each on the tensor cores (bk_mlp.cuh), so the weights are staged,
 // the tensor memory allocated and the mbarrier initialised once per CTA. Yielding particles inside
 // the training range take the surrogate's return; all others (elastic, out of range, invalid
-// porosity) the exact map.
-__global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkState in, BkState out, BkConstants cst,
-                                                             GridPtrs g, BkDiagnostics diag, BkFlags flags,
-                                                             SurrogateDev sg) {
+// porosity) the exact map. The trial gradient's SVD stops at float32 convergence (svd3f<false>):
+// its float64 finishing sweep only matters at the reference's rounding level, far below the
+// network's error.
+template <bool kRef = false>
+__device__ __forceinline__ void g2p_return_surrogate_body(Arg<Params, kRef> P, Arg<BkState, kRef> in, Arg<BkState, kRef> out,
+                                                          Arg<BkConstants, kRef> cst, Arg<GridPtrs, kRef> g,
+                                                          Arg<BkDiagnostics, kRef> diag, Arg<BkFlags, kRef> flags,
+                                                          Arg<SurrogateDev, kRef> sg, Slot sl) {
     __shared__ mlp::TileSmem ts;
     __shared__ int s_counts[3];
     mlp::tile_setup(ts, sg.blob);
     if (threadIdx.x < 3) s_counts[threadIdx.x] = 0;
-    if (blockIdx.x == 0 && threadIdx.x < 6) {
+    if (sl.block == 0 && threadIdx.x < 6) {
         g.bounds[6 + threadIdx.x] = g.bounds[threadIdx.x];
         g.bounds[threadIdx.x] = threadIdx.x < 3 ? INT_MAX : INT_MIN;
     }
     __syncthreads();
     const int64_t pitch = P.pitch;
     uint32_t phase = 0;
-    for (int64_t base = (int64_t)blockIdx.x * 128; base < P.n; base += (int64_t)gridDim.x * 128) {
+    for (int64_t base = (int64_t)sl.block * 128; base < P.n; base += (int64_t)sl.blocks * 128) {
         const int64_t i = base + threadIdx.x;
         M3 Fn, Cn;
         bool ding = false, use_mlp = false;
@@ -1107,7 +1196,7 @@ __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkSta
         if (i < P.n && g2p_gather(P, in, out, g, flags, i, Fn, Cn) && P.material == 1) {
             T = P.transport ? (float)out.temperature[i] : in.material_temperature[i];
             por = in.porosity[i];
-            ding = ding_prelude(P.ding, load_m3(in.Fe, i, pitch), por, in.gelled[i], Cn, T,
+            ding = ding_prelude<false>(P.ding, load_m3(in.Fe, i, pitch), por, in.gelled[i], Cn, T,
                                 __ldg(cst.viscosity_parameter), flags.ding, d);
             if (ding && !ding_elastic(P.ding, d, por)) {
                 order3(d.e, perm);
@@ -1164,6 +1253,12 @@ __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkSta
     if (sg.path_counts && threadIdx.x < 3 && s_counts[threadIdx.x]) atomicAdd(sg.path_counts + threadIdx.x, s_counts[threadIdx.x]);
 }
 
+__global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkState in, BkState out, BkConstants cst,
+                                                             GridPtrs g, BkDiagnostics diag, BkFlags flags,
+                                                             SurrogateDev sg) {
+    g2p_return_surrogate_body(P, in, out, cst, g, diag, flags, sg, grid_slot());
+}
+
 // ------------------------------------------------------------ materialize
 __global__ void k_materialize(Params P, BkState s, BkConstants cst, float* Fp, float* T_mat, float* rho,
                               float* yield, float* visc, double* gas_p, double* sat, float* mass) {
@@ -1216,15 +1311,12 @@ __global__ void k_surface_accumulate(int64_t owners_n, const int32_t* __restrict
 
 unsigned blocks_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
 
-}  // namespace
-
-extern "C" {
-
 #define BK_REQUIRE(cond, msg) do { if (!(cond)) return fail(BK_ERR_ARGUMENT, msg); } while (0)
 
-int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, const BkConstants* constants,
-               BkGrid* grid, BkSurface* surface, BkDiagnostics* diagnostics, BkFlags* flags, int32_t phases,
-               void* stream) {
+// The argument checks of bk_substep (also applied to every instance of a batch).
+int check_substep_args(const BkSubstepParams* params, const BkState* in, const BkState* out,
+                       const BkConstants* constants, const BkGrid* grid, const BkSurface* surface,
+                       const BkDiagnostics* diagnostics, const BkFlags* flags, int32_t phases) {
     BK_REQUIRE(params && in && out && constants && grid && diagnostics && flags, "bk_substep: null argument");
     const BkSubstepParams& p = *params;
     BK_REQUIRE(p.n >= 0 && p.pitch >= p.n, "bk_substep: bad particle count/pitch");
@@ -1257,6 +1349,18 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
     if (p.transport_prescatter_next)
         BK_REQUIRE(!(p.surrogate && p.surrogate->packed) && (phases & BK_PHASE_MECHANICS),
                    "bk_substep: the transport prescatter runs in the exact G2P kernel of a mechanics phase");
+    return BK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, const BkConstants* constants,
+               BkGrid* grid, BkSurface* surface, BkDiagnostics* diagnostics, BkFlags* flags, int32_t phases,
+               void* stream) {
+    if (int rc = check_substep_args(params, in, out, constants, grid, surface, diagnostics, flags, phases)) return rc;
+    const BkSubstepParams& p = *params;
     if (p.n == 0) return BK_OK;
     Params P = to_params(p);
     GridPtrs g = grid_ptrs(*grid);
@@ -1386,6 +1490,346 @@ int bk_materialize(const BkSubstepParams* params, const BkState* state, const Bk
         to_params(p), *state, *constants, plastic_gradients, material_temperature, reference_density, yield_stress,
         viscosity, gas_pressure, saturation, particle_mass);
     return check_launch("bk_materialize");
+}
+
+}  // extern "C"
+
+// ===================================================================== batched substeps
+// Many independent simulators advanced by one launch per stage: each block of a batched launch
+// finds its instance in a device table (a binary search over the stage's first-block prefix),
+// copies that instance's entry into shared memory and runs the same kernel body as a plain
+// launch, with its index among the instance's blocks. The blocks an instance gets per stage are
+// the ones its own launch would use (particles, vertices, owners), or for the node-box passes a
+// share that grows with its particle count, so a batch of small bodies fills the GPU.
+namespace {
+
+enum BatchStage { kStVertices, kStOwners, kStScatter, kStDiffuse, kStClear, kStP2G, kStGrid, kStG2P, kStSurrogate,
+                  kStAccumulate, kBatchStages };
+
+struct BatchEntry {
+    Params P;
+    BkState in, out;
+    BkConstants cst;
+    GridPtrs g;
+    BkSurface sf;
+    BkDiagnostics diag;
+    BkFlags flags;
+    SurrogateDev sg;
+    double *water_losses, *heat_exchanges;  // surface accumulators of `out`
+    float accumulate_dt;
+    int prescatter_ok;                      // takes part in the transport prescatter
+};
+static_assert(sizeof(BatchEntry) % 4 == 0, "entries are copied as 4-byte words");
+
+struct BatchArgs {
+    const BatchEntry* entries;  // [2][count]: parity 0 steps states[0] -> states[1], parity 1 back
+    const uint32_t* first;      // [kBatchStages][count + 1]: first block of each instance per stage
+    int count, parity, prescattered, prescatter_next;
+};
+
+// The instance that owns this block in `stage` (the last one whose first block is at or below
+// blockIdx.x, which skips instances given no blocks) and the block's slot within it.
+__device__ __forceinline__ Slot batch_find(const BatchArgs& b, int stage, int& k) {
+    const uint32_t* f = b.first + (size_t)stage * (b.count + 1);
+    int lo = 0, hi = b.count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(f + mid) <= blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    k = lo;
+    const uint32_t f0 = __ldg(f + lo), f1 = __ldg(f + lo + 1);
+    return Slot{(int)(blockIdx.x - f0), (int)(f1 - f0)};
+}
+
+// Copies the block's entry into shared memory with this call's prescatter flags. Every thread of
+// the block calls it (it synchronises the block).
+__device__ __forceinline__ Slot batch_load(const BatchArgs& b, int stage, BatchEntry& e) {
+    int k;
+    const Slot sl = batch_find(b, stage, k);
+    const int* src = reinterpret_cast<const int*>(b.entries + (size_t)b.parity * b.count + k);
+    int* dst = reinterpret_cast<int*>(&e);
+    for (int w = threadIdx.x; w < (int)(sizeof(BatchEntry) / 4); w += blockDim.x) dst[w] = __ldg(src + w);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        e.P.prescattered = b.prescattered && e.prescatter_ok;
+        e.P.prescatter_next = b.prescatter_next && e.prescatter_ok;
+        e.P.prescatter_stale = 0;
+    }
+    __syncthreads();
+    return sl;
+}
+
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock) kb_surface_vertices(BatchArgs b) {
+    __shared__ BatchEntry e;
+    const Slot sl = batch_load(b, kStVertices, e);
+    surface_vertices_body<kBlock, true>(e.P, e.in.x, e.in.F, e.sf, sl);
+}
+
+__global__ void __launch_bounds__(128) kb_surface_owners(BatchArgs b) {
+    __shared__ BatchEntry e;
+    const Slot sl = batch_load(b, kStOwners, e);
+    surface_owners_body<true>(e.P, e.in, e.cst, e.sf, e.g, e.flags.simulation, sl);
+}
+
+__global__ void __launch_bounds__(kThreads) kb_transport_scatter(BatchArgs b) {
+    __shared__ BatchEntry e;
+    __shared__ ScatterTile sm;
+    const Slot sl = batch_load(b, kStScatter, e);
+    if (e.P.prescattered) return;  // fields scattered ahead by this instance's previous G2P
+    transport_scatter_body<true>(sm, e.P, e.in, e.cst, e.g, e.flags.simulation, sl);
+}
+
+__global__ void __launch_bounds__(kDiffThreads) kb_diffuse(BatchArgs b) {
+    __shared__ BatchEntry e;
+    __shared__ DiffuseSmem sm;
+    const Slot sl = batch_load(b, kStDiffuse, e);
+    diffuse_body<true>(sm, e.P, e.g, e.flags.transport, sl);
+}
+
+__global__ void __launch_bounds__(kThreads) kb_clear_previous(BatchArgs b) {
+    __shared__ BatchEntry e;
+    const Slot sl = batch_load(b, kStClear, e);
+    clear_previous_body<true>(e.P, e.g, sl);
+}
+
+template <bool kStaged>
+__global__ void __launch_bounds__(kThreads, 4) kb_p2g(BatchArgs b) {
+    __shared__ BatchEntry e;
+    __shared__ P2GSmem sm;
+    const Slot sl = batch_load(b, kStP2G, e);
+    p2g_body<kStaged, true>(sm, e.P, e.in, e.out, e.cst, e.g, e.flags, e.diag.max_residuals, sl);
+}
+
+__global__ void __launch_bounds__(kThreads) kb_grid_update(BatchArgs b) {
+    __shared__ BatchEntry e;
+    const Slot sl = batch_load(b, kStGrid, e);
+    grid_update_body<true>(e.P, e.g, sl);
+}
+
+__global__ void __launch_bounds__(128, 8) kb_g2p_return(BatchArgs b) {
+    __shared__ BatchEntry e;
+    extern __shared__ __align__(16) unsigned char g2p_smem[];
+    const Slot sl = batch_load(b, kStG2P, e);
+    g2p_return_body<true>(g2p_smem, e.P, e.in, e.out, e.cst, e.g, e.diag, e.flags, e.sg, sl);
+}
+
+__global__ void __launch_bounds__(128, 4) kb_g2p_return_surrogate(BatchArgs b) {
+    __shared__ BatchEntry e;
+    const Slot sl = batch_load(b, kStSurrogate, e);
+    g2p_return_surrogate_body<true>(e.P, e.in, e.out, e.cst, e.g, e.diag, e.flags, e.sg, sl);
+}
+
+__global__ void __launch_bounds__(kThreads) kb_surface_accumulate(BatchArgs b) {
+    __shared__ BatchEntry e;
+    const Slot sl = batch_load(b, kStAccumulate, e);
+    const int64_t o = sl.block * (int64_t)blockDim.x + threadIdx.x;
+    if (o >= e.sf.owner_count) return;
+    const int p = e.sf.owners[o];
+    e.water_losses[p] += (double)e.accumulate_dt * e.sf.owner_loss[o];
+    e.heat_exchanges[p] += (double)e.accumulate_dt * e.sf.owner_heat[o];
+}
+
+}  // namespace
+
+struct BkBatch {
+    int count = 0;
+    BatchEntry* entries = nullptr;  // device [2][count]
+    uint32_t* first = nullptr;      // device [kBatchStages][count + 1]
+    uint32_t total[kBatchStages] = {};
+    int vertex_block = 32;
+    bool staged = true;             // every instance allows the bulk-staged P2G
+    bool all_prescatter = true;     // every transport instance takes part in the prescatter
+    bool any_transport = false;
+};
+
+extern "C" {
+
+int bk_batch_create(const BkBatchInstance* instances, int32_t count, BkBatch** batch) {
+    BK_REQUIRE(instances && batch && count > 0, "bk_batch_create: null argument or empty batch");
+    *batch = nullptr;
+    int device = 0, sms = 148;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    std::vector<BatchEntry> entries(2 * (size_t)count);
+    std::vector<uint32_t> first((size_t)kBatchStages * (count + 1), 0);
+    int64_t particles = 0, vertices = 0, bindings = 0;
+    for (int k = 0; k < count; ++k) particles += instances[k].params.n;
+    BkBatch host;
+    host.count = count;
+    for (int k = 0; k < count; ++k) {
+        const BkBatchInstance& in = instances[k];
+        const BkSubstepParams& p = in.params;
+        const bool surrogate = p.surrogate && p.surrogate->packed && p.material == 1;
+        for (int parity = 0; parity < 2; ++parity) {
+            const BkState& a = in.states[parity];
+            const BkState& b = in.states[1 - parity];
+            BkSubstepParams q = p;
+            q.transport_prescattered = q.transport_prescatter_next = q.transport_prescatter_stale = 0;
+            if (int rc = check_substep_args(&q, &a, &b, &in.constants, &in.grid, &in.surface, &in.diagnostics,
+                                            &in.flags, BK_PHASE_TRANSPORT | BK_PHASE_MECHANICS))
+                return rc;
+            if (p.transport)
+                BK_REQUIRE(in.water_losses[1 - parity] && in.heat_exchanges[1 - parity],
+                           "bk_batch_create: missing surface accumulators");
+            BatchEntry& e = entries[(size_t)parity * count + k];
+            e.P = to_params(q);
+            e.in = a;
+            e.out = b;
+            e.cst = in.constants;
+            e.g = grid_ptrs(in.grid);
+            e.sf = in.surface;
+            e.diag = in.diagnostics;
+            e.flags = in.flags;
+            e.sg = surrogate_dev(surrogate ? p.surrogate : nullptr);
+            e.water_losses = in.water_losses[1 - parity];
+            e.heat_exchanges = in.heat_exchanges[1 - parity];
+            e.accumulate_dt = p.time_step;
+            e.prescatter_ok = p.transport && !p.keep_transport_fields && !surrogate;
+            const uintptr_t bases = (uintptr_t)a.x | (uintptr_t)a.v | (uintptr_t)a.C | (uintptr_t)a.F |
+                                    (p.material == 1 ? (uintptr_t)a.tau : 0);
+            host.staged = host.staged && p.pitch % 4 == 0 && (bases & 15) == 0;
+        }
+        host.any_transport = host.any_transport || p.transport;
+        if (p.transport && (p.keep_transport_fields || surrogate)) host.all_prescatter = false;
+        uint32_t blocks[kBatchStages] = {};
+        const int64_t n = p.n;
+        if (n > 0) {
+            if (p.transport) {
+                blocks[kStVertices] = (uint32_t)in.surface.vertex_count;
+                blocks[kStOwners] = blocks_for(in.surface.owner_count, 128);
+                blocks[kStScatter] = blocks_for(n, kThreads);
+                blocks[kStAccumulate] = blocks_for(in.surface.owner_count, kThreads);
+                vertices += in.surface.vertex_count;
+                bindings += in.surface.binding_count;
+            }
+            // node-box passes: about one block per 2048 particles (256 nodes at 8 particles a cell)
+            const uint32_t box = (uint32_t)std::min<int64_t>(std::max<int64_t>(1, (n + 2047) / 2048), 4 * sms);
+            if (p.transport) blocks[kStDiffuse] = box;
+            blocks[kStClear] = box;
+            blocks[kStP2G] = blocks_for(n, kThreads);
+            blocks[kStGrid] = box;
+            if (surrogate) {
+                // a persistent share of 4 CTAs per SM in proportion to the particles
+                const int64_t share = std::max<int64_t>(1, (int64_t)(4.0 * sms * (double)n / (double)particles + 0.5));
+                blocks[kStSurrogate] = (uint32_t)std::min<int64_t>(share, blocks_for(n, 128));
+            } else {
+                blocks[kStG2P] = blocks_for(n, 128);
+            }
+        }
+        for (int st = 0; st < kBatchStages; ++st) {
+            uint32_t* f = first.data() + (size_t)st * (count + 1);
+            BK_REQUIRE((uint64_t)f[k] + blocks[st] < (1ull << 31), "bk_batch_create: too many blocks in one stage");
+            f[k + 1] = f[k] + blocks[st];
+        }
+    }
+    for (int st = 0; st < kBatchStages; ++st) host.total[st] = first[(size_t)st * (count + 1) + count];
+    host.vertex_block = vertex_block_threads(vertices, bindings);
+    BkBatch* out = new BkBatch(host);
+    if (cudaMalloc(&out->entries, entries.size() * sizeof(BatchEntry)) != cudaSuccess ||
+        cudaMalloc(&out->first, first.size() * sizeof(uint32_t)) != cudaSuccess) {
+        cudaFree(out->entries);
+        cudaFree(out->first);
+        delete out;
+        cudaGetLastError();
+        return fail(BK_ERR_LAUNCH, "bk_batch_create: device allocation failed");
+    }
+    if (cudaMemcpy(out->entries, entries.data(), entries.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(out->first, first.data(), first.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+        bk_batch_destroy(out);
+        return fail(BK_ERR_LAUNCH, "bk_batch_create: table upload failed");
+    }
+    *batch = out;
+    return BK_OK;
+}
+
+int bk_batch_substep(BkBatch* batch, int32_t parity, int32_t phases, int32_t prescattered, int32_t prescatter_next,
+                     void* stream) {
+    BK_REQUIRE(batch && (parity == 0 || parity == 1), "bk_batch_substep: bad batch or parity");
+    BK_REQUIRE(!prescatter_next || (phases & BK_PHASE_MECHANICS),
+               "bk_batch_substep: the transport prescatter runs in the G2P kernel of a mechanics phase");
+    const BkBatch& B = *batch;
+    const BatchArgs a{B.entries, B.first, B.count, parity, prescattered ? 1 : 0, prescatter_next ? 1 : 0};
+    const uint32_t* T = B.total;
+    cudaStream_t s = S(stream);
+    if ((phases & BK_PHASE_TRANSPORT) && B.any_transport) {
+        if (T[kStVertices]) {
+            int rec = profile_begin("batch_surface_vertices", s);
+            switch (B.vertex_block) {
+                case 256: kb_surface_vertices<256><<<T[kStVertices], 256, 0, s>>>(a); break;
+                case 128: kb_surface_vertices<128><<<T[kStVertices], 128, 0, s>>>(a); break;
+                default: kb_surface_vertices<32><<<T[kStVertices], 32, 0, s>>>(a); break;
+            }
+            profile_end(rec, s);
+            if (int rc = check_launch("bk_batch_substep/surface_vertices")) return rc;
+        }
+        if (T[kStOwners]) {
+            int rec = profile_begin("batch_surface_owners", s);
+            kb_surface_owners<<<T[kStOwners], 128, 0, s>>>(a);
+            profile_end(rec, s);
+            if (int rc = check_launch("bk_batch_substep/surface_owners")) return rc;
+        }
+        if (T[kStScatter] && !(prescattered && B.all_prescatter)) {
+            int rec = profile_begin("batch_transport_scatter", s);
+            kb_transport_scatter<<<T[kStScatter], kThreads, 0, s>>>(a);
+            profile_end(rec, s);
+            if (int rc = check_launch("bk_batch_substep/transport_scatter")) return rc;
+        }
+        if (T[kStDiffuse]) {
+            int rec = profile_begin("batch_diffuse", s);
+            kb_diffuse<<<T[kStDiffuse], kDiffThreads, 0, s>>>(a);
+            profile_end(rec, s);
+            if (int rc = check_launch("bk_batch_substep/diffuse")) return rc;
+        }
+    }
+    if (phases & BK_PHASE_MECHANICS) {
+        if (T[kStClear]) {
+            int rec = profile_begin("batch_clear_previous", s);
+            kb_clear_previous<<<T[kStClear], kThreads, 0, s>>>(a);
+            profile_end(rec, s);
+            if (int rc = check_launch("bk_batch_substep/clear_previous")) return rc;
+        }
+        if (T[kStP2G]) {
+            int rec = profile_begin("batch_p2g", s);
+            if (B.staged) kb_p2g<true><<<T[kStP2G], kThreads, 0, s>>>(a);
+            else kb_p2g<false><<<T[kStP2G], kThreads, 0, s>>>(a);
+            profile_end(rec, s);
+            if (int rc = check_launch("bk_batch_substep/p2g")) return rc;
+        }
+        if (T[kStGrid]) {
+            int rec = profile_begin("batch_grid_update", s);
+            kb_grid_update<<<T[kStGrid], kThreads, 0, s>>>(a);
+            profile_end(rec, s);
+            if (int rc = check_launch("bk_batch_substep/grid_update")) return rc;
+        }
+        if (T[kStG2P]) {
+            int rec = profile_begin("batch_g2p_return", s);
+            const size_t smem = prescatter_next ? sizeof(G2PTransportTile) : 0;
+            kb_g2p_return<<<T[kStG2P], 128, smem, s>>>(a);
+            profile_end(rec, s);
+            if (int rc = check_launch("bk_batch_substep/g2p_return")) return rc;
+        }
+        if (T[kStSurrogate]) {
+            int rec = profile_begin("batch_g2p_return_surrogate", s);
+            kb_g2p_return_surrogate<<<T[kStSurrogate], 128, 0, s>>>(a);
+            profile_end(rec, s);
+            if (int rc = check_launch("bk_batch_substep/g2p_return_surrogate")) return rc;
+        }
+    }
+    if ((phases & BK_PHASE_TRANSPORT) && T[kStAccumulate]) {
+        kb_surface_accumulate<<<T[kStAccumulate], kThreads, 0, s>>>(a);
+        if (int rc = check_launch("bk_batch_substep/surface_accumulate")) return rc;
+    }
+    return BK_OK;
+}
+
+int bk_batch_destroy(BkBatch* batch) {
+    if (!batch) return BK_OK;
+    cudaFree(batch->entries);
+    cudaFree(batch->first);
+    delete batch;
+    return BK_OK;
 }
 
 }  // extern "C"

@@ -73,6 +73,13 @@ class BkSubstepParams(C.Structure):
 PHASE_TRANSPORT = 1
 PHASE_MECHANICS = 2
 
+
+class BkBatchInstance(C.Structure):
+    _fields_ = [("params", BkSubstepParams), ("states", BkState * 2), ("water_losses", P * 2),
+                ("heat_exchanges", P * 2), ("constants", BkConstants), ("grid", BkGrid), ("surface", BkSurface),
+                ("diagnostics", BkDiagnostics), ("flags", BkFlags)]
+
+
 class BkCheckInputs(C.Structure):
     _fields_ = [("n", C.c_int64), ("pitch", C.c_int64), ("x", P), ("v", P), ("F", P), ("C", P),
                 ("reference_volume", P), ("mass", P), ("dry_mass", P), ("water", P), ("temperature", P),
@@ -98,6 +105,9 @@ _SIGS = {
     "bk_substep": [P] * 8 + [C.c_int32, P],
     "bk_materialize": [P] * 11 + [P],
     "bk_surface_accumulate": [P, C.c_float, P, P, P],
+    "bk_batch_create": [P, C.c_int32, P],
+    "bk_batch_substep": [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P],
+    "bk_batch_destroy": [P],
 }
 
 
@@ -291,6 +301,27 @@ class SubstepEngine:
         for k in range(7):
             grid.fields[k] = _p(fields[k])
         return grid, tensors
+
+    def batch_instance(self, state_a, state_b):
+        """This simulator as one entry of a bk_batch_create table: the ping-pong pair (state_a,
+        state_b), its grid, surface, flags and constants (past settling, lean diagnostics)."""
+        if self.prescatter_pending:
+            raise RuntimeError("transport fields are scattered ahead for a substep outside the batch")
+        inst = BkBatchInstance()
+        p = self.params(False)
+        p.status = _p(self.status)
+        inst.params = p
+        for k, st in enumerate((state_a, state_b)):
+            inst.states[k] = state_struct(st, self.is_ding, self.transport, self.gas)
+            if self.transport:
+                inst.water_losses[k] = _p(st.transport_state.water_losses)
+                inst.heat_exchanges[k] = _p(st.transport_state.heat_exchanges)
+        inst.constants = self.constants(False)
+        inst.grid = self.grid
+        inst.surface = self.surface
+        inst.diagnostics.max_residuals = _p(self.max_residuals)
+        inst.flags = self.flags
+        return inst
 
     # ---------------------------------------------------------------- launch
     def prescatter_allowed(self):

@@ -69,6 +69,9 @@ def parse():
     p.add_argument("--resolution", type=int, default=128)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-variants", action="store_true", help="skip the surrogate and fwd+bwd forms")
+    p.add_argument("--surrogate-only", type=int, metavar="STEPS", default=None,
+                   help="time only STEPS substeps of the yielding loaf with the learned return map attached "
+                        "(for profiling the surrogate kernel)")
     p.add_argument("--clock-window", type=float, default=CLOCK_WINDOW_S,
                    help="seconds of untimed substeps (on a second copy of the loaf) sampled for clocks before "
                         "the timed region; 0 skips them (profiling runs)")
@@ -306,6 +309,22 @@ def main():
     scene = box_loaf(args.resolution, args.particles, seed=rank)
     sim = make_simulator(scene, diagnostics="lean")
     n = scene.particle_count
+    if args.surrogate_only:
+        from baking_b200.surrogate import LoadReturnSurrogate, ReturnMapSurrogate
+        loaf = box_loaf(args.resolution, args.particles, seed=rank, initial_temperature=318.15, prestrain=0.08)
+        ysim = make_simulator(loaf, diagnostics="lean")
+        sur = ReturnMapSurrogate(LoadReturnSurrogate(ROOT / "baking_b200" / "data" / "return_surrogate_box_loaf.npz"))
+        sur.attach(ysim)
+        ysim.AdvanceUnchecked(max(1, args.warmup))
+        t, _ = _timed(lambda: ysim.AdvanceUnchecked(args.surrogate_only), dist, torch.cuda.current_stream())
+        ysim.CheckState()
+        if rank == 0:
+            print(json.dumps({"metric": "surrogate particle-substeps/s (yielding loaf)", "unit": UNIT,
+                              "value": world * loaf.particle_count * args.surrogate_only / t,
+                              "steps": args.surrogate_only, "paths": sur.statistics()}))
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.rollout_only:
         steps, every = args.rollout_only
         out = rollout_variant(sim, dist, torch.cuda.current_stream(), world,
@@ -499,8 +518,10 @@ def _timed(fn, dist, stream):
 def batched(args, rank, dist, net, count=64, steps=200):
     """64 independent dough balls (particles ~ U[5k, 200k], grids from {32, 48, 64, 96}^3, oven
     ~ U[150, 220] C, prestrain ~ U[0.04, 0.1] so that they yield), advanced together under one
-    captured CUDA graph: exact return map, then the surrogate from the same initial states, and the
-    exact map launched kernel by kernel without the graph."""
+    captured CUDA graph of batched launches (one launch per stage for all 64, over the instance
+    table): exact return map, then the surrogate from the same initial states; also the exact map
+    with every instance launching its own kernels on 8 streams under a graph, and the batched
+    launches without the graph."""
     import torch
     from baking_b200.batch import BatchedSimulators, RestoreStates, SnapshotStates
     from baking_b200.scenes import dough_batch, make_simulator
@@ -519,6 +540,11 @@ def batched(args, rank, dist, net, count=64, steps=200):
     exact.CheckState()
     del exact
     RestoreStates(sims, saved)
+    streams = BatchedSimulators(sims, launch="streams").capture()
+    RestoreStates(sims, saved)
+    t_streams, _ = _timed(lambda: streams.Advance(steps), dist, stream)
+    del streams
+    RestoreStates(sims, saved)
     surs = [ReturnMapSurrogate(net).attach(s) for s in sims]
     fast = BatchedSimulators(sims).capture()
     RestoreStates(sims, saved)
@@ -528,11 +554,13 @@ def batched(args, rank, dist, net, count=64, steps=200):
     fast.CheckState()
     paths = [sum(s.statistics()[k] for s in surs) for k in ("elastic", "surrogate", "exact_yielding")]
     return {"value": world * n * steps / t_exact, "unit": UNIT, "surrogate": world * n * steps / t_sur,
-            "without_graph": world * n * 20 / t_launch, "instances": count, "particles": n, "steps": steps,
+            "without_graph": world * n * 20 / t_launch, "per_instance_launches": world * n * steps / t_streams,
+            "instances": count, "particles": n, "steps": steps,
             "surrogate_paths": dict(zip(("elastic", "surrogate", "exact_yielding"), paths)),
             "roofline": step_roofline(n, active, steps, t_exact),
             "surrogate_roofline": step_roofline(n, active, steps, t_sur),
-            "scene": "dough balls (loaf dough: Ding + gas + thermal-water), dt 5e-5, one CUDA graph per 2 substeps"}
+            "scene": "dough balls (loaf dough: Ding + gas + thermal-water), dt 5e-5, one CUDA graph per 2 substeps",
+            "launch": "one launch per stage for all instances over a device instance table"}
 
 
 def rollout_variant(sim, dist, stream, world, scene, fb_steps=64, every=FWD_BWD_CHECKPOINT_EVERY):

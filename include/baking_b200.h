@@ -334,6 +334,41 @@ BK_API int bk_substep_static_grid(const BkSubstepParams *params, const BkState *
                                   const BkConstants *constants, BkDiagnostics *diagnostics, BkFlags *flags,
                                   void *stream);
 
+/* ---- Batched substeps over an instance table (no counterpart in the reference) ----
+   Many independent simulators (own particles, grids, parameters) advanced by ONE launch per stage
+   of bk_substep instead of one per stage and simulator: each block of a batched launch finds its
+   instance in a device table and runs the plain kernel's body on it. An instance gets the blocks
+   its own launch would use (particles, surface vertices, face owners) and, for the node-box passes,
+   about one block per 2048 particles. Each instance holds its two ping-pong states: parity 0 steps
+   states[0] -> states[1], parity 1 steps states[1] -> states[0]. Instances with transport need
+   18-int grid bounds (the transport prescatter) and the surface accumulators of both states, which
+   bk_batch_substep advances like bk_surface_accumulate after each transport phase. An instance
+   whose params carry a surrogate runs the surrogate G2P kernel, the others the exact one. The
+   transport_prescattered/_next/_stale fields and the phases are ignored in `params`: the flags of
+   bk_batch_substep apply to every transport instance without a surrogate, and an instance's
+   fields must not be left scattered ahead by an earlier bk_substep (the batch never clears them). */
+typedef struct BkBatchInstance {
+    BkSubstepParams params;
+    BkState states[2];
+    double *water_losses[2], *heat_exchanges[2];   /* surface accumulators of states[k] (transport) */
+    BkConstants constants;
+    BkGrid grid;
+    BkSurface surface;
+    BkDiagnostics diagnostics;
+    BkFlags flags;
+} BkBatchInstance;
+
+typedef struct BkBatch BkBatch;
+
+/* Checks every instance as bk_substep would (both parities) and uploads the table (about 1 KB per
+   instance and parity, allocated on the current device; the call synchronises). The device
+   arrays named by the instances must outlive the batch. */
+BK_API int bk_batch_create(const BkBatchInstance *instances, int32_t count, BkBatch **batch);
+/* One substep of every instance, 8-10 launches on `stream` (capturable in a CUDA graph). */
+BK_API int bk_batch_substep(BkBatch *batch, int32_t parity, int32_t phases, int32_t prescattered,
+                            int32_t prescatter_next, void *stream);
+BK_API int bk_batch_destroy(BkBatch *batch);
+
 /* Per-kernel timing of the fused entry points with CUDA events on the launching stream.
    bk_profile_start clears old records and starts recording; bk_profile_stop stops;
    bk_profile_report waits for the events and writes, per kernel name (name_capacity bytes each),

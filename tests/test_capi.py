@@ -79,3 +79,18 @@ def test_permute_particles_rejects_bad_arguments_before_any_device_work():
     table[0].data = 4096 + 4
     assert fn(1000, 256, 1, ctypes.addressof(table), aligned, 1 << 40, None) != 0
     assert "element size" in lib.bk_last_error().decode()
+
+
+def test_batch_entry_points_reject_bad_arguments_without_a_gpu():
+    """bk_batch_create refuses a null or empty table and bk_batch_substep a null batch or a parity
+    other than 0 and 1, before any CUDA call; destroying a null batch is a no-op."""
+    from baking_b200.physics import substep
+    lib = substep._declare()
+    handle = ctypes.c_void_p()
+    assert lib.bk_batch_create(None, 0, ctypes.byref(handle)) != 0
+    assert "empty batch" in lib.bk_last_error().decode()
+    table = (substep.BkBatchInstance * 1)()
+    assert lib.bk_batch_create(table, 0, ctypes.byref(handle)) != 0
+    assert lib.bk_batch_substep(None, 0, 3, 0, 0, None) != 0
+    assert "parity" in lib.bk_last_error().decode()
+    assert lib.bk_batch_destroy(None) == 0

@@ -11,29 +11,85 @@ def bodies(prestrain=(0.0, 0.0)):
     return scenes.dough_batch(6, seed=3, particles=(5_000, 20_000), resolutions=(32, 48), prestrain=prestrain)
 
 
+def _compare(batched, single, scs, steps):
+    for b, s, sc in zip(batched, single, scs):
+        assert b.step_count == s.step_count == steps
+        xb = b.current_state.particle_positions.cpu().numpy()
+        xs = s.current_state.particle_positions.cpu().numpy()
+        dx = sc.simulation.grid_spacing
+        np.testing.assert_allclose(xb, xs, rtol=0, atol=1e-4 * dx)
+        tb, ts = b.current_state.transport_state, s.current_state.transport_state
+        Tb = tb.temperatures.cpu().numpy()
+        np.testing.assert_allclose(Tb, ts.temperatures.cpu().numpy(), rtol=1e-6)
+        assert Tb.max() > sc.transport.initial_temperature_k   # the oven is heating each body
+        for name in ("water_masses", "heat_exchanges", "water_losses"):
+            np.testing.assert_allclose(getattr(tb, name).cpu().numpy(), getattr(ts, name).cpu().numpy(),
+                                       rtol=1e-5, atol=1e-12, err_msg=name)
+        np.testing.assert_allclose(b.current_state.material_state.porosities.cpu().numpy(),
+                                   s.current_state.material_state.porosities.cpu().numpy(), rtol=0, atol=1e-6)
+
+
+@pytest.mark.parametrize("launch", ["table", "streams"])
 @pytest.mark.parametrize("prestrain", [(0.0, 0.0), (0.04, 0.1)])
-def test_graph_replay_matches_individual_advance(prestrain):
+def test_graph_replay_matches_individual_advance(prestrain, launch):
     from baking_b200 import scenes
     from baking_b200.batch import BatchedSimulators
     scs = bodies(prestrain)
     batched = [scenes.make_simulator(s, diagnostics="lean") for s in scs]
     single = [scenes.make_simulator(s, diagnostics="lean") for s in scs]
-    batch = BatchedSimulators(batched, streams=4).capture()   # capture runs two substeps
+    batch = BatchedSimulators(batched, streams=4, launch=launch).capture()   # capture runs two substeps
     batch.Advance(10)
     for sim in single:
         sim.AdvanceUnchecked(12)
-    for b, s, sc in zip(batched, single, scs):
-        assert b.step_count == s.step_count == 12
-        xb = b.current_state.particle_positions.cpu().numpy()
-        xs = s.current_state.particle_positions.cpu().numpy()
-        dx = sc.simulation.grid_spacing
-        np.testing.assert_allclose(xb, xs, rtol=0, atol=1e-4 * dx)
-        Tb = b.current_state.transport_state.temperatures.cpu().numpy()
-        Ts = s.current_state.transport_state.temperatures.cpu().numpy()
-        np.testing.assert_allclose(Tb, Ts, rtol=1e-6)
-        assert Tb.max() > sc.transport.initial_temperature_k   # the oven is heating each body
+    _compare(batched, single, scs, 12)
     for st in batch.CheckState():
         assert st["step_count"] == 12
+
+
+def test_instance_table_without_graph_and_after_outside_steps():
+    """The table launch stepped eagerly (graph=False), then after one substep taken outside the
+    batch (which swaps every ping-pong pair, so the table is rebuilt), against the bodies advanced
+    one by one; the per-stage launches each cover the whole batch."""
+    from baking_b200 import _lib, scenes
+    from baking_b200.batch import BatchedSimulators
+    scs = bodies((0.04, 0.1))
+    batched = [scenes.make_simulator(s, diagnostics="lean") for s in scs]
+    single = [scenes.make_simulator(s, diagnostics="lean") for s in scs]
+    batch = BatchedSimulators(batched, launch="table")
+    timer = _lib.KernelTimer()
+    with timer:
+        batch.Advance(4, graph=False)
+    kernels = timer.summary()
+    assert kernels["batch_p2g"]["count"] == 4 and kernels["batch_g2p_return"]["count"] == 4
+    assert kernels["batch_transport_scatter"]["count"] == 2   # the second of each pair is scattered ahead
+    assert "p2g" not in kernels
+    for sim in batched:
+        sim.AdvanceUnchecked(1)
+    batch.Advance(4)
+    for sim in single:
+        sim.AdvanceUnchecked(9)
+    _compare(batched, single, scs, 9)
+
+
+def test_instance_table_with_surrogate_on_some_instances():
+    """Instances with the learned return map take the surrogate G2P kernel, the others the exact
+    one, in the same batched substep; each matches its body advanced alone."""
+    from baking_b200 import scenes
+    from baking_b200.batch import BatchedSimulators
+    from baking_b200.surrogate import LoadReturnSurrogate, ReturnMapSurrogate
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    net = LoadReturnSurrogate(root / "baking_b200" / "data" / "return_surrogate_box_loaf.npz")
+    scs = bodies((0.04, 0.1))
+    batched = [scenes.make_simulator(s, diagnostics="lean") for s in scs]
+    single = [scenes.make_simulator(s, diagnostics="lean") for s in scs]
+    for k in (0, 2, 4):
+        ReturnMapSurrogate(net).attach(batched[k])
+        ReturnMapSurrogate(net).attach(single[k])
+    BatchedSimulators(batched, launch="table").Advance(6)
+    for sim in single:
+        sim.AdvanceUnchecked(6)
+    _compare(batched, single, scs, 6)
 
 
 def test_snapshot_restore_repeats_a_run():
