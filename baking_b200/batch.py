@@ -46,9 +46,8 @@ class BatchedSimulators:
         eng = sim._engine
         ahead = eng.prescatter_allowed()
         eng.run(state_in, state_out, False, PHASE_TRANSPORT | PHASE_MECHANICS, False,
-                prescattered=ahead and prescattered, prescatter_next=ahead and prescatter_next)
-        if sim.transport is not None:
-            eng.accumulate_surface(state_out.transport_state)
+                prescattered=ahead and prescattered, prescatter_next=ahead and prescatter_next,
+                accumulate=state_out.transport_state if sim.transport is not None else None)
 
     def _current_layout(self):
         return tuple((id(sim._current), id(sim.next_state), id(sim._engine.surrogate)) for sim in self.sims)

@@ -224,32 +224,42 @@ __global__ void __launch_bounds__(kBlock) k_surface_vertices(Params P, const flo
 }
 
 // physics/thermal_water.py:77-92 (face areas, tray contact) and the surface terms of :108-122,
-// per face-owning particle, scattered into the heat/loss/exchange node fields.
+// one warp per face-owning particle: lane 0 sums the owner's faces in order, every lane forms the
+// owner's rates, lane j < 27 adds stencil node j's share (27 atomics in parallel instead of one
+// thread issuing 81 in turn). With accumulators set in `sf`, lane 0 also advances the owner's
+// water-loss and heat-exchange accumulators (thermal_water.py:225-226), which bk_surface_accumulate
+// does otherwise.
+constexpr int kOwnerThreads = 128;
 template <bool kRef = false>
 __device__ __forceinline__ void surface_owners_body(Arg<Params, kRef> P, Arg<BkState, kRef> in, Arg<BkConstants, kRef> cst,
                                                     Arg<BkSurface, kRef> sf, Arg<GridPtrs, kRef> g, int32_t* sim_flags, Slot sl) {
-    int64_t o = sl.block * (int64_t)blockDim.x + threadIdx.x;
-    if (o >= sf.owner_count) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t o = (sl.block * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (o >= sf.owner_count) return;  // whole warps
     const int64_t vp = sf.vertex_pitch, pitch = P.pitch;
-    int p = sf.owners[o];
+    const int p = sf.owners[o];
     double exposed = 0.0, contact = 0.0;
-    for (int f = sf.owner_face_offsets[o]; f < sf.owner_face_offsets[o + 1]; ++f) {
-        double q[3][3];
+    if (lane == 0) {
+        for (int f = sf.owner_face_offsets[o]; f < sf.owner_face_offsets[o + 1]; ++f) {
+            double q[3][3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            int vid = sf.faces[3 * f + k];
+            for (int k = 0; k < 3; ++k) {
+                int vid = sf.faces[3 * f + k];
 #pragma unroll
-            for (int a = 0; a < 3; ++a) q[k][a] = (double)sf.vertices[a * vp + vid];
+                for (int a = 0; a < 3; ++a) q[k][a] = (double)sf.vertices[a * vp + vid];
+            }
+            double e1[3] = {q[1][0] - q[0][0], q[1][1] - q[0][1], q[1][2] - q[0][2]};
+            double e2[3] = {q[2][0] - q[0][0], q[2][1] - q[0][1], q[2][2] - q[0][2]};
+            double nr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+            double len = sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]);
+            double area = 0.5 * len;
+            double cy = (q[0][1] + q[1][1] + q[2][1]) / 3.0;
+            if (cy <= (double)(sf.floor_height + sf.contact_distance) && nr[1] < -0.2 * len) contact += area;
+            else exposed += area;
         }
-        double e1[3] = {q[1][0] - q[0][0], q[1][1] - q[0][1], q[1][2] - q[0][2]};
-        double e2[3] = {q[2][0] - q[0][0], q[2][1] - q[0][1], q[2][2] - q[0][2]};
-        double nr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
-        double len = sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]);
-        double area = 0.5 * len;
-        double cy = (q[0][1] + q[1][1] + q[2][1]) / 3.0;
-        if (cy <= (double)(sf.floor_height + sf.contact_distance) && nr[1] < -0.2 * len) contact += area;
-        else exposed += area;
     }
+    exposed = __shfl_sync(kFull, exposed, 0);
+    contact = __shfl_sync(kFull, contact, 0);
     double vol = (double)cst.volume[p] * (double)det3(load_m3(in.F, p, pitch));
     double T = in.temperature[p], W = in.water[p];
     double sat = W / ((double)P.water_density * vol);
@@ -260,14 +270,22 @@ __device__ __forceinline__ void surface_owners_body(Arg<Params, kRef> P, Arg<BkS
                 - (double)P.latent * loss;
     double exch = h * exposed + (double)P.tray_transfer * contact;
     if (P.water_enabled) exch += (double)(P.latent * P.surface_loss) * sat * exposed;
-    sf.owner_heat[o] = heat;
-    sf.owner_loss[o] = loss;
+    if (lane == 0) {
+        sf.owner_heat[o] = heat;
+        sf.owner_loss[o] = loss;
+        if (sf.accumulate_water_losses) {
+            sf.accumulate_water_losses[p] += (double)sf.accumulate_time_step * loss;
+            sf.accumulate_heat_exchanges[p] += (double)sf.accumulate_time_step * heat;
+        }
+    }
     Stencil st = make_stencil(load_v3(in.x, p, pitch), P.origin, P.dx, P.R);
-    if (!st.valid) { set_flag(sim_flags, 1); return; }
-#pragma unroll 1
-    for (int j = 0; j < 27; ++j) {
+    if (!st.valid) {
+        if (lane == 0) set_flag(sim_flags, 1);
+        return;
+    }
+    if (lane < 27) {
         int ox, oy, oz;
-        node_offset(j, ox, oy, oz);
+        node_offset(lane, ox, oy, oz);
         double w = (double)(st.w[0][ox] * st.w[1][oy] * st.w[2][oz]);
         int64_t node = node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R);
         atomicAdd(g.f[4] + node, w * heat);
@@ -1387,8 +1405,8 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
         if (surface->owner_count > 0) {
             {
                 int rec = profile_begin("surface_owners", s);
-                k_surface_owners<<<blocks_for(surface->owner_count, 128), 128, 0, s>>>(P, *in, *constants, *surface, g,
-                                                                                  flags->simulation);
+                k_surface_owners<<<blocks_for(surface->owner_count * 32, kOwnerThreads), kOwnerThreads, 0, s>>>(
+                    P, *in, *constants, *surface, g, flags->simulation);
                 profile_end(rec, s);
             }
             if (int rc = check_launch("bk_substep/surface_owners")) return rc;
@@ -1504,7 +1522,7 @@ int bk_materialize(const BkSubstepParams* params, const BkState* state, const Bk
 namespace {
 
 enum BatchStage { kStVertices, kStOwners, kStScatter, kStDiffuse, kStClear, kStP2G, kStGrid, kStG2P, kStSurrogate,
-                  kStAccumulate, kBatchStages };
+                  kBatchStages };
 
 struct BatchEntry {
     Params P;
@@ -1514,10 +1532,8 @@ struct BatchEntry {
     BkSurface sf;
     BkDiagnostics diag;
     BkFlags flags;
-    SurrogateDev sg;
-    double *water_losses, *heat_exchanges;  // surface accumulators of `out`
-    float accumulate_dt;
-    int prescatter_ok;                      // takes part in the transport prescatter
+    SurrogateDev sg;   // sf carries the surface accumulators of `out`
+    int prescatter_ok;  // takes part in the transport prescatter
 };
 static_assert(sizeof(BatchEntry) % 4 == 0, "entries are copied as 4-byte words");
 
@@ -1566,7 +1582,7 @@ __global__ void __launch_bounds__(kBlock) kb_surface_vertices(BatchArgs b) {
     surface_vertices_body<kBlock, true>(e.P, e.in.x, e.in.F, e.sf, sl);
 }
 
-__global__ void __launch_bounds__(128) kb_surface_owners(BatchArgs b) {
+__global__ void __launch_bounds__(kOwnerThreads) kb_surface_owners(BatchArgs b) {
     __shared__ BatchEntry e;
     const Slot sl = batch_load(b, kStOwners, e);
     surface_owners_body<true>(e.P, e.in, e.cst, e.sf, e.g, e.flags.simulation, sl);
@@ -1620,16 +1636,6 @@ __global__ void __launch_bounds__(128, 4) kb_g2p_return_surrogate(BatchArgs b) {
     g2p_return_surrogate_body<true>(e.P, e.in, e.out, e.cst, e.g, e.diag, e.flags, e.sg, sl);
 }
 
-__global__ void __launch_bounds__(kThreads) kb_surface_accumulate(BatchArgs b) {
-    __shared__ BatchEntry e;
-    const Slot sl = batch_load(b, kStAccumulate, e);
-    const int64_t o = sl.block * (int64_t)blockDim.x + threadIdx.x;
-    if (o >= e.sf.owner_count) return;
-    const int p = e.sf.owners[o];
-    e.water_losses[p] += (double)e.accumulate_dt * e.sf.owner_loss[o];
-    e.heat_exchanges[p] += (double)e.accumulate_dt * e.sf.owner_heat[o];
-}
-
 }  // namespace
 
 struct BkBatch {
@@ -1679,12 +1685,12 @@ int bk_batch_create(const BkBatchInstance* instances, int32_t count, BkBatch** b
             e.cst = in.constants;
             e.g = grid_ptrs(in.grid);
             e.sf = in.surface;
+            e.sf.accumulate_water_losses = p.transport ? in.water_losses[1 - parity] : nullptr;
+            e.sf.accumulate_heat_exchanges = p.transport ? in.heat_exchanges[1 - parity] : nullptr;
+            e.sf.accumulate_time_step = p.time_step;
             e.diag = in.diagnostics;
             e.flags = in.flags;
             e.sg = surrogate_dev(surrogate ? p.surrogate : nullptr);
-            e.water_losses = in.water_losses[1 - parity];
-            e.heat_exchanges = in.heat_exchanges[1 - parity];
-            e.accumulate_dt = p.time_step;
             e.prescatter_ok = p.transport && !p.keep_transport_fields && !surrogate;
             const uintptr_t bases = (uintptr_t)a.x | (uintptr_t)a.v | (uintptr_t)a.C | (uintptr_t)a.F |
                                     (p.material == 1 ? (uintptr_t)a.tau : 0);
@@ -1697,9 +1703,8 @@ int bk_batch_create(const BkBatchInstance* instances, int32_t count, BkBatch** b
         if (n > 0) {
             if (p.transport) {
                 blocks[kStVertices] = (uint32_t)in.surface.vertex_count;
-                blocks[kStOwners] = blocks_for(in.surface.owner_count, 128);
+                blocks[kStOwners] = blocks_for(in.surface.owner_count * 32, kOwnerThreads);
                 blocks[kStScatter] = blocks_for(n, kThreads);
-                blocks[kStAccumulate] = blocks_for(in.surface.owner_count, kThreads);
                 vertices += in.surface.vertex_count;
                 bindings += in.surface.binding_count;
             }
@@ -1766,7 +1771,7 @@ int bk_batch_substep(BkBatch* batch, int32_t parity, int32_t phases, int32_t pre
         }
         if (T[kStOwners]) {
             int rec = profile_begin("batch_surface_owners", s);
-            kb_surface_owners<<<T[kStOwners], 128, 0, s>>>(a);
+            kb_surface_owners<<<T[kStOwners], kOwnerThreads, 0, s>>>(a);
             profile_end(rec, s);
             if (int rc = check_launch("bk_batch_substep/surface_owners")) return rc;
         }
@@ -1816,10 +1821,6 @@ int bk_batch_substep(BkBatch* batch, int32_t parity, int32_t phases, int32_t pre
             profile_end(rec, s);
             if (int rc = check_launch("bk_batch_substep/g2p_return_surrogate")) return rc;
         }
-    }
-    if ((phases & BK_PHASE_TRANSPORT) && T[kStAccumulate]) {
-        kb_surface_accumulate<<<T[kStAccumulate], kThreads, 0, s>>>(a);
-        if (int rc = check_launch("bk_batch_substep/surface_accumulate")) return rc;
     }
     return BK_OK;
 }

@@ -427,11 +427,13 @@ class MpmSimulator:
             self.transport.CheckState()
             self._engine.run(original, output, was_settling, PHASE_MECHANICS, full, prescatter_next=prescatter_next)
         else:
+            # unchecked: the surface kernel advances the accumulators (nothing can reject the substep)
             self._engine.run(original, output, was_settling, PHASE_TRANSPORT | PHASE_MECHANICS, full,
-                             prescattered=prescattered, prescatter_next=prescatter_next)
+                             prescattered=prescattered, prescatter_next=prescatter_next,
+                             accumulate=output.transport_state if self.transport is not None else None)
         if check and isinstance(self.material, DingMaterial):
             self.material.CheckState()
-        if self.transport is not None:
+        if check and self.transport is not None:
             self._engine.accumulate_surface(output.transport_state)
         if self.retain_history:
             self.state_history.append(output)

@@ -39,7 +39,8 @@ class BkSurface(C.Structure):
                 ("binding_weights", P), ("binding_pitch", C.c_int64), ("reference_offsets", P),
                 ("vertex_pitch", C.c_int64), ("vertices", P), ("reference_vertices", P), ("owner_count", C.c_int64),
                 ("owners", P), ("owner_face_offsets", P), ("faces", P), ("owner_heat", P), ("owner_loss", P),
-                ("floor_height", C.c_float), ("contact_distance", C.c_float), ("binding_count", C.c_int64)]
+                ("floor_height", C.c_float), ("contact_distance", C.c_float), ("binding_count", C.c_int64),
+                ("accumulate_water_losses", P), ("accumulate_heat_exchanges", P), ("accumulate_time_step", C.c_float)]
 
 
 class BkDiagnostics(C.Structure):
@@ -331,11 +332,12 @@ class SubstepEngine:
         return bool(self.transport) and not (sur is not None and sur.packed)
 
     def run(self, state_in, state_out, settling, phases, full_diagnostics, grid=None, keep_fields=False,
-            prescattered=False, prescatter_next=False):
+            prescattered=False, prescatter_next=False, accumulate=None):
         """One substep through bk_substep. ``prescattered``: the previous run scattered this substep's
         transport fields ahead (its ``prescatter_next``), so the scalar P2G is skipped;
         ``prescatter_next``: scatter the next substep's, which must start from ``state_out`` with
-        nothing changed in between."""
+        nothing changed in between. ``accumulate``: a transport state whose water-loss and
+        heat-exchange accumulators the surface kernel advances (in place of accumulate_surface)."""
         p = self.params(settling)
         p.keep_transport_fields = int(keep_fields)
         p.transport_prescattered = int(prescattered)
@@ -360,9 +362,17 @@ class SubstepEngine:
             diag.porosity_residuals = _p(m.porosity_residuals)
         # (under a KernelTimer the library times bk_substep's kernels one by one)
         stream = _lib.stream_handle()
-        rc = self.lib.bk_substep(C.byref(p), C.byref(sin), C.byref(sout), C.byref(cst),
-                                 C.byref(self.grid if grid is None else grid),
-                                 C.byref(self.surface), C.byref(diag), C.byref(self.flags), int(phases), stream)
+        sf = self.surface
+        if accumulate is not None and self.transport and (phases & PHASE_TRANSPORT):
+            sf.accumulate_water_losses = _p(accumulate.water_losses)
+            sf.accumulate_heat_exchanges = _p(accumulate.heat_exchanges)
+            sf.accumulate_time_step = self.sim.simulation_config.time_step
+        try:
+            rc = self.lib.bk_substep(C.byref(p), C.byref(sin), C.byref(sout), C.byref(cst),
+                                     C.byref(self.grid if grid is None else grid),
+                                     C.byref(sf), C.byref(diag), C.byref(self.flags), int(phases), stream)
+        finally:
+            sf.accumulate_water_losses = sf.accumulate_heat_exchanges = None
         if rc != 0:
             raise RuntimeError(f"bk_substep failed ({rc}): {self.lib.bk_last_error().decode(errors='replace')}")
         if own_grid and (phases & PHASE_MECHANICS):

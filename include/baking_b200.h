@@ -236,6 +236,11 @@ typedef struct BkSurface {
     float floor_height, contact_distance;
     int64_t binding_count;         /* total bindings of the vertex_ids vertices, a launch-size hint
                                       (0: unknown, one warp per vertex) */
+    double *accumulate_water_losses, *accumulate_heat_exchanges;  /* optional (NULL: not here): the
+                                      surface kernel of bk_substep also advances the owners'
+                                      accumulators by accumulate_time_step * their rates, which
+                                      bk_surface_accumulate does otherwise after the substep */
+    float accumulate_time_step;
 } BkSurface;
 
 /* Optional full per-particle outputs of the reference kernels (NULL pointers are skipped). */
@@ -342,7 +347,8 @@ BK_API int bk_substep_static_grid(const BkSubstepParams *params, const BkState *
    about one block per 2048 particles. Each instance holds its two ping-pong states: parity 0 steps
    states[0] -> states[1], parity 1 steps states[1] -> states[0]. Instances with transport need
    18-int grid bounds (the transport prescatter) and the surface accumulators of both states, which
-   bk_batch_substep advances like bk_surface_accumulate after each transport phase. An instance
+   bk_batch_substep advances in its surface kernel (the instances' own accumulate_* fields are
+   ignored). An instance
    whose params carry a surrogate runs the surrogate G2P kernel, the others the exact one. The
    transport_prescattered/_next/_stale fields and the phases are ignored in `params`: the flags of
    bk_batch_substep apply to every transport instance without a surrogate, and an instance's
