@@ -373,9 +373,12 @@ __device__ void transport_scatter_block(TransportTile<kT, kTile>& sm, const Para
 using ScatterTile = TransportTile<kThreads, kTileNodes>;
 
 template <bool kRef = false>
-__device__ __forceinline__ void transport_scatter_body(ScatterTile& sm, Arg<Params, kRef> P, Arg<BkState, kRef> in,
+__device__ __forceinline__ void transport_scatter_body(Arg<Params, kRef> P, Arg<BkState, kRef> in,
                                                        Arg<BkConstants, kRef> cst, Arg<GridPtrs, kRef> g, int32_t* sim_flags,
                                                        Slot sl) {
+    // Shared memory is declared in the bodies, not passed in: through a reference the compiler may
+    // not see that it is shared memory and issue generic loads, stores and atomics.
+    __shared__ ScatterTile sm;
     const int64_t i = sl.block * (int64_t)kThreads + threadIdx.x;
     const int64_t pitch = P.pitch;
     bool valid = false;
@@ -399,8 +402,7 @@ __device__ __forceinline__ void transport_scatter_body(ScatterTile& sm, Arg<Para
 
 __global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkState in, BkConstants cst, GridPtrs g,
                                                                int32_t* sim_flags) {
-    __shared__ ScatterTile sm;
-    transport_scatter_body(sm, P, in, cst, g, sim_flags, grid_slot());
+    transport_scatter_body(P, in, cst, g, sim_flags, grid_slot());
 }
 
 // ------------------------------------------------------------ grid passes
@@ -440,8 +442,9 @@ struct DiffuseSmem {
 };
 
 template <bool kRef = false>
-__device__ __forceinline__ void diffuse_body(DiffuseSmem& sm, Arg<Params, kRef> P, Arg<GridPtrs, kRef> g, int32_t* errors,
+__device__ __forceinline__ void diffuse_body(Arg<Params, kRef> P, Arg<GridPtrs, kRef> g, int32_t* errors,
                                              Slot sl) {
+    __shared__ DiffuseSmem sm;
     double* s_V = sm.V;
     double* s_T = sm.T;
     double* s_S = sm.S;
@@ -529,8 +532,7 @@ __device__ __forceinline__ void diffuse_body(DiffuseSmem& sm, Arg<Params, kRef> 
 }
 
 __global__ void __launch_bounds__(kDiffThreads) k_diffuse(Params P, GridPtrs g, int32_t* errors) {
-    __shared__ DiffuseSmem sm;
-    diffuse_body(sm, P, g, errors, grid_slot());
+    diffuse_body(P, g, errors, grid_slot());
 }
 
 // Fields scattered ahead for a substep that runs its own scalar P2G instead (the state may have
@@ -650,9 +652,10 @@ __device__ __forceinline__ void copy(uint32_t dst, const void* src, uint32_t byt
 
 // Four 256-thread blocks per SM (64 registers) measured faster than three at 77 registers.
 template <bool kStaged, bool kRef = false>
-__device__ __forceinline__ void p2g_body(P2GSmem& sm, Arg<Params, kRef> P, Arg<BkState, kRef> in, Arg<BkState, kRef> out,
+__device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef> in, Arg<BkState, kRef> out,
                                          Arg<BkConstants, kRef> cst, Arg<GridPtrs, kRef> g, Arg<BkFlags, kRef> flags,
                                          float* max_residuals, Slot sl) {
+    __shared__ P2GSmem sm;
     if (sl.block == 0 && threadIdx.x < 2) max_residuals[threadIdx.x] = 0.0f;
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t i = sl.block * (int64_t)kThreads + tid;
@@ -877,8 +880,7 @@ __device__ __forceinline__ void p2g_body(P2GSmem& sm, Arg<Params, kRef> P, Arg<B
 template <bool kStaged>
 __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
                                                  BkFlags flags, float* max_residuals) {
-    __shared__ P2GSmem sm;
-    p2g_body<kStaged>(sm, P, in, out, cst, g, flags, max_residuals, grid_slot());
+    p2g_body<kStaged>(P, in, out, cst, g, flags, max_residuals, grid_slot());
 }
 
 // ------------------------------------------------------ fused G2P + return
@@ -1136,10 +1138,11 @@ constexpr int kG2PTile = 256;
 using G2PTransportTile = TransportTile<128, kG2PTile>;
 
 template <bool kRef = false>
-__device__ __forceinline__ void g2p_return_body(unsigned char* g2p_smem, Arg<Params, kRef> P, Arg<BkState, kRef> in,
+__device__ __forceinline__ void g2p_return_body(Arg<Params, kRef> P, Arg<BkState, kRef> in,
                                                 Arg<BkState, kRef> out, Arg<BkConstants, kRef> cst, Arg<GridPtrs, kRef> g,
                                                 Arg<BkDiagnostics, kRef> diag, Arg<BkFlags, kRef> flags, Arg<SurrogateDev, kRef> sg,
                                                 Slot sl) {
+    extern __shared__ __align__(16) unsigned char g2p_smem[];
     const int64_t i = sl.block * (int64_t)blockDim.x + threadIdx.x;
     if (sl.block == 0 && threadIdx.x < 6) {
         // This substep's box becomes the box the next substep clears; the active box restarts empty.
@@ -1177,8 +1180,7 @@ __device__ __forceinline__ void g2p_return_body(unsigned char* g2p_smem, Arg<Par
 
 __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
                                                    BkDiagnostics diag, BkFlags flags, SurrogateDev sg) {
-    extern __shared__ __align__(16) unsigned char g2p_smem[];
-    g2p_return_body(g2p_smem, P, in, out, cst, g, diag, flags, sg, grid_slot());
+    g2p_return_body(P, in, out, cst, g, diag, flags, sg, grid_slot());
 }
 
 // G2P + return map with the learned surrogate: a persistent CTA walks 128-particle tiles and
@@ -1590,17 +1592,15 @@ __global__ void __launch_bounds__(kOwnerThreads) kb_surface_owners(BatchArgs b) 
 
 __global__ void __launch_bounds__(kThreads) kb_transport_scatter(BatchArgs b) {
     __shared__ BatchEntry e;
-    __shared__ ScatterTile sm;
     const Slot sl = batch_load(b, kStScatter, e);
     if (e.P.prescattered) return;  // fields scattered ahead by this instance's previous G2P
-    transport_scatter_body<true>(sm, e.P, e.in, e.cst, e.g, e.flags.simulation, sl);
+    transport_scatter_body<true>(e.P, e.in, e.cst, e.g, e.flags.simulation, sl);
 }
 
 __global__ void __launch_bounds__(kDiffThreads) kb_diffuse(BatchArgs b) {
     __shared__ BatchEntry e;
-    __shared__ DiffuseSmem sm;
     const Slot sl = batch_load(b, kStDiffuse, e);
-    diffuse_body<true>(sm, e.P, e.g, e.flags.transport, sl);
+    diffuse_body<true>(e.P, e.g, e.flags.transport, sl);
 }
 
 __global__ void __launch_bounds__(kThreads) kb_clear_previous(BatchArgs b) {
@@ -1612,9 +1612,8 @@ __global__ void __launch_bounds__(kThreads) kb_clear_previous(BatchArgs b) {
 template <bool kStaged>
 __global__ void __launch_bounds__(kThreads, 4) kb_p2g(BatchArgs b) {
     __shared__ BatchEntry e;
-    __shared__ P2GSmem sm;
     const Slot sl = batch_load(b, kStP2G, e);
-    p2g_body<kStaged, true>(sm, e.P, e.in, e.out, e.cst, e.g, e.flags, e.diag.max_residuals, sl);
+    p2g_body<kStaged, true>(e.P, e.in, e.out, e.cst, e.g, e.flags, e.diag.max_residuals, sl);
 }
 
 __global__ void __launch_bounds__(kThreads) kb_grid_update(BatchArgs b) {
@@ -1625,9 +1624,8 @@ __global__ void __launch_bounds__(kThreads) kb_grid_update(BatchArgs b) {
 
 __global__ void __launch_bounds__(128, 8) kb_g2p_return(BatchArgs b) {
     __shared__ BatchEntry e;
-    extern __shared__ __align__(16) unsigned char g2p_smem[];
     const Slot sl = batch_load(b, kStG2P, e);
-    g2p_return_body<true>(g2p_smem, e.P, e.in, e.out, e.cst, e.g, e.diag, e.flags, e.sg, sl);
+    g2p_return_body<true>(e.P, e.in, e.out, e.cst, e.g, e.diag, e.flags, e.sg, sl);
 }
 
 __global__ void __launch_bounds__(128, 4) kb_g2p_return_surrogate(BatchArgs b) {

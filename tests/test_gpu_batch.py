@@ -65,10 +65,10 @@ def test_instance_table_without_graph_and_after_outside_steps():
     assert "p2g" not in kernels
     for sim in batched:
         sim.AdvanceUnchecked(1)
-    batch.Advance(4)
+    batch.Advance(4)   # rebuilds the table and captures (two substeps), then replays twice
     for sim in single:
-        sim.AdvanceUnchecked(9)
-    _compare(batched, single, scs, 9)
+        sim.AdvanceUnchecked(11)
+    _compare(batched, single, scs, 11)
 
 
 def test_instance_table_with_surrogate_on_some_instances():
@@ -86,10 +86,10 @@ def test_instance_table_with_surrogate_on_some_instances():
     for k in (0, 2, 4):
         ReturnMapSurrogate(net).attach(batched[k])
         ReturnMapSurrogate(net).attach(single[k])
-    BatchedSimulators(batched, launch="table").Advance(6)
+    BatchedSimulators(batched, launch="table").Advance(6)   # capture runs two substeps first
     for sim in single:
-        sim.AdvanceUnchecked(6)
-    _compare(batched, single, scs, 6)
+        sim.AdvanceUnchecked(8)
+    _compare(batched, single, scs, 8)
 
 
 def test_snapshot_restore_repeats_a_run():
