@@ -17,6 +17,19 @@ struct M3 { float m[9]; };
 struct M3d { double m[9]; };
 struct V3 { float v[3]; };
 
+// Two independent float32 fused multiply-adds in one instruction (sm_100's packed fma.rn.f32x2):
+// each half is rounded exactly like fmaf, so a loop of paired accumulators gives the bits of the
+// same loop written with fmaf, at half the issue slots.
+BK_DEV float2 ffma2(float2 a, float2 b, float2 c) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\tmov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
 // ------------------------------------------------------------- SoA access
 BK_DEV V3 load_v3(const float* __restrict__ p, int64_t i, int64_t pitch) {
     V3 r;
@@ -938,6 +951,49 @@ BK_DEV float vertex_block(const int* __restrict__ offsets, const int* __restrict
         for (int w = 0; w < kBlock / 32; ++w) sum += s_part[t][w];
         out = anchor[t] + sum;
     }
+    return out;
+}
+
+// The same reconstruction by one warp (lanes stride over the bindings) for vertices binding a few
+// tens of particles (a fine mesh), so that a block can hold several vertices; no block barrier.
+// Lane a < 3 returns coordinate a. The warp's sum is lane 0's butterfly result, as in vertex_block
+// with one warp, so both give the same bits.
+BK_DEV float vertex_warp(const int* __restrict__ offsets, const int* __restrict__ particles,
+                         const float* __restrict__ weights, const float* __restrict__ ref_offsets, int64_t bp,
+                         const float* __restrict__ ref_vertices, int64_t vp, const float* __restrict__ x,
+                         const float* __restrict__ F, int64_t pitch, int vid) {
+    const int b0 = offsets[vid], b1 = offsets[vid + 1];
+    const int lane = threadIdx.x & 31;
+    if (b0 == b1) return lane < 3 ? ref_vertices[lane * vp + vid] : 0.0f;  // the same branch for the warp
+    auto predict = [&](int b, float* r) {
+        const int p = particles[b];
+        const M3 f = load_m3(F, p, pitch);
+        const V3 xp = load_v3(x, p, pitch);
+        const float o[3] = {ref_offsets[b], ref_offsets[bp + b], ref_offsets[2 * bp + b]};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) r[a] = xp.v[a] + (f.m[3 * a] * o[0] + f.m[3 * a + 1] * o[1] + f.m[3 * a + 2] * o[2]);
+    };
+    float anchor[3];
+    predict(b0, anchor);
+    float disp[3] = {0.f, 0.f, 0.f};
+#pragma unroll 4
+    for (int b = b0 + lane; b < b1; b += 32) {
+        float pr[3];
+        predict(b, pr);
+        const float w = weights[b];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) disp[a] += w * (pr[a] - anchor[a]);
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) disp[a] += __shfl_xor_sync(0xffffffffu, disp[a], o);
+        disp[a] = __shfl_sync(0xffffffffu, disp[a], 0);
+    }
+    float out = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        if (lane == a) out = anchor[a] + disp[a];
     return out;
 }
 

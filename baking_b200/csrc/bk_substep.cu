@@ -135,8 +135,6 @@ __device__ __forceinline__ void node_offset(int j, int& ox, int& oy, int& oz) {
     oz = j - 9 * ox - 3 * oy;
 }
 
-// Component o (0, 1, 2) of a float4 holding one axis' three stencil weights.
-__device__ __forceinline__ float pick(const float4& v, int o) { return o == 0 ? v.x : (o == 1 ? v.y : v.z); }
 
 __device__ __forceinline__ long long pack_base(const int* b) {
     return ((long long)b[0] << 42) | ((long long)b[1] << 21) | (long long)b[2];
@@ -152,7 +150,7 @@ struct BlockBox {
 };
 
 // Block-level min/max of valid stencil nodes; also widens the node box `bounds` ([0..2] lo, [3..5]
-// hi). The box is tiled when it holds at most `tile_nodes` nodes. Every thread of the block must
+// hi) unless it is null. The box is tiled when it holds at most `tile_nodes` nodes. Every thread of the block must
 // call this (it synchronises the block).
 __device__ BlockBox block_box(int* bounds, bool valid, const int* b, int tile_nodes = kTileNodes) {
     __shared__ int s_box[6];
@@ -181,7 +179,7 @@ __device__ BlockBox block_box(int* bounds, bool valid, const int* b, int tile_no
         }
         bb.tiled = count <= tile_nodes;
         bb.count = bb.tiled ? (int)count : 0;
-        if (threadIdx.x < 3) {
+        if (bounds != nullptr && threadIdx.x < 3) {
             // The shared box only widens (min of lo, max of hi), so a value read through L2 that is
             // older than the current one is never narrower: a block whose box lies inside it
             // skips the atomics, and thousands of blocks stop contending for six addresses.
@@ -205,61 +203,88 @@ __device__ __forceinline__ int64_t tile_node(const BlockBox& bb, int t, int R) {
 }
 
 // ------------------------------------------------------------------ surface
-// geometry/mesh_tracking.py:13-38 restricted to the vertices of boundary faces; one block per
-// vertex (a vertex binds thousands of particles: a block keeps enough gathers in flight).
+// geometry/mesh_tracking.py:13-38 restricted to the vertices of boundary faces. A vertex of a
+// coarse mesh binds thousands of particles: one block of kBlock = 128 or 256 threads per vertex
+// keeps enough gathers in flight. A vertex of a fine mesh binds tens: kBlock = 32 then means one
+// warp per vertex, kVertexWarps vertices to a block.
+constexpr int kVertexWarps = 8;
+
+// Blocks of the surface vertex launch for `vertices` vertices at block size `threads`.
+inline unsigned vertex_launch_blocks(int64_t vertices, int threads) {
+    return (unsigned)(threads == 32 ? (vertices + kVertexWarps - 1) / kVertexWarps : vertices);
+}
+inline int vertex_launch_threads(int threads) { return threads == 32 ? 32 * kVertexWarps : threads; }
+
 template <int kBlock, bool kRef = false>
 __device__ __forceinline__ void surface_vertices_body(Arg<Params, kRef> P, const float* __restrict__ x,
                                                       const float* __restrict__ F, Arg<BkSurface, kRef> sf, Slot sl) {
-    const int vid = sf.vertex_ids[sl.block];
-    const float v = vertex_block<kBlock>(sf.binding_offsets, sf.binding_particles, sf.binding_weights,
-                                           sf.reference_offsets, sf.binding_pitch, sf.reference_vertices,
-                                           sf.vertex_pitch, x, F, P.pitch, vid);
-    if (threadIdx.x < 3) sf.vertices[threadIdx.x * sf.vertex_pitch + vid] = v;
+    if constexpr (kBlock == 32) {
+        const int64_t k = (int64_t)sl.block * kVertexWarps + (threadIdx.x >> 5);
+        if (k >= sf.vertex_count) return;  // whole warps
+        const int vid = sf.vertex_ids[k];
+        const float v = vertex_warp(sf.binding_offsets, sf.binding_particles, sf.binding_weights,
+                                    sf.reference_offsets, sf.binding_pitch, sf.reference_vertices, sf.vertex_pitch, x,
+                                    F, P.pitch, vid);
+        const int lane = threadIdx.x & 31;
+        if (lane < 3) sf.vertices[lane * sf.vertex_pitch + vid] = v;
+    } else {
+        const int vid = sf.vertex_ids[sl.block];
+        const float v = vertex_block<kBlock>(sf.binding_offsets, sf.binding_particles, sf.binding_weights,
+                                               sf.reference_offsets, sf.binding_pitch, sf.reference_vertices,
+                                               sf.vertex_pitch, x, F, P.pitch, vid);
+        if (threadIdx.x < 3) sf.vertices[threadIdx.x * sf.vertex_pitch + vid] = v;
+    }
 }
 
 template <int kBlock>
-__global__ void __launch_bounds__(kBlock) k_surface_vertices(Params P, const float* __restrict__ x,
+__global__ void __launch_bounds__(kBlock == 32 ? 32 * kVertexWarps : kBlock) k_surface_vertices(Params P, const float* __restrict__ x,
                                                           const float* __restrict__ F, BkSurface sf) {
     surface_vertices_body<kBlock>(P, x, F, sf, grid_slot());
 }
 
-// physics/thermal_water.py:77-92 (face areas, tray contact) and the surface terms of :108-122,
-// one warp per face-owning particle: lane 0 sums the owner's faces in order, every lane forms the
-// owner's rates, lane j < 27 adds stencil node j's share (27 atomics in parallel instead of one
-// thread issuing 81 in turn). With accumulators set in `sf`, lane 0 also advances the owner's
-// water-loss and heat-exchange accumulators (thermal_water.py:225-226), which bk_surface_accumulate
-// does otherwise.
+// ------------------------------------------------------- surface terms
+// physics/thermal_water.py:77-92 (face areas, tray contact) and the surface terms of :108-122 for
+// the face-owning particles, in two layouts chosen by how many particles own faces:
+// * few owners, each with several faces (a coarse voxel mesh: about 3k owners of a 1M-particle
+//   loaf): one warp per owner; lane 0 sums the owner's faces in order, every lane forms the rates,
+//   lane j < 27 adds stencil node j's share (27 atomics in parallel);
+// * many owners (a fine tetrahedral mesh: about a third of a dough ball's particles own faces): one
+//   thread per owner, the node shares summed per stencil run and per block tile like the transport
+//   scatter, so the 81 float64 atomics per owner become a few per node and block.
+// With accumulators set in `sf`, the owner's water-loss and heat-exchange accumulators also advance
+// by one substep (thermal_water.py:225-226), which bk_surface_accumulate does otherwise.
 constexpr int kOwnerThreads = 128;
-template <bool kRef = false>
-__device__ __forceinline__ void surface_owners_body(Arg<Params, kRef> P, Arg<BkState, kRef> in, Arg<BkConstants, kRef> cst,
-                                                    Arg<BkSurface, kRef> sf, Arg<GridPtrs, kRef> g, int32_t* sim_flags, Slot sl) {
-    const int lane = threadIdx.x & 31;
-    const int64_t o = (sl.block * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (o >= sf.owner_count) return;  // whole warps
-    const int64_t vp = sf.vertex_pitch, pitch = P.pitch;
-    const int p = sf.owners[o];
-    double exposed = 0.0, contact = 0.0;
-    if (lane == 0) {
-        for (int f = sf.owner_face_offsets[o]; f < sf.owner_face_offsets[o + 1]; ++f) {
-            double q[3][3];
+
+// Exposed and tray-contact areas of owner o's faces, summed in face order.
+template <class SF>
+__device__ __forceinline__ void owner_areas(const SF& sf, int64_t o, double& exposed, double& contact) {
+    const int64_t vp = sf.vertex_pitch;
+    exposed = 0.0;
+    contact = 0.0;
+    for (int f = sf.owner_face_offsets[o]; f < sf.owner_face_offsets[o + 1]; ++f) {
+        double q[3][3];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                int vid = sf.faces[3 * f + k];
+        for (int k = 0; k < 3; ++k) {
+            int vid = sf.faces[3 * f + k];
 #pragma unroll
-                for (int a = 0; a < 3; ++a) q[k][a] = (double)sf.vertices[a * vp + vid];
-            }
-            double e1[3] = {q[1][0] - q[0][0], q[1][1] - q[0][1], q[1][2] - q[0][2]};
-            double e2[3] = {q[2][0] - q[0][0], q[2][1] - q[0][1], q[2][2] - q[0][2]};
-            double nr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
-            double len = sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]);
-            double area = 0.5 * len;
-            double cy = (q[0][1] + q[1][1] + q[2][1]) / 3.0;
-            if (cy <= (double)(sf.floor_height + sf.contact_distance) && nr[1] < -0.2 * len) contact += area;
-            else exposed += area;
+            for (int a = 0; a < 3; ++a) q[k][a] = (double)sf.vertices[a * vp + vid];
         }
+        double e1[3] = {q[1][0] - q[0][0], q[1][1] - q[0][1], q[1][2] - q[0][2]};
+        double e2[3] = {q[2][0] - q[0][0], q[2][1] - q[0][1], q[2][2] - q[0][2]};
+        double nr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        double len = sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]);
+        double area = 0.5 * len;
+        double cy = (q[0][1] + q[1][1] + q[2][1]) / 3.0;
+        if (cy <= (double)(sf.floor_height + sf.contact_distance) && nr[1] < -0.2 * len) contact += area;
+        else exposed += area;
     }
-    exposed = __shfl_sync(kFull, exposed, 0);
-    contact = __shfl_sync(kFull, contact, 0);
+}
+
+// Heat, loss and exchange rates of owner particle p from its areas; rate[0..2].
+template <class PP, class ST, class CS>
+__device__ __forceinline__ void owner_rates(const PP& P, const ST& in, const CS& cst, int p, double exposed,
+                                            double contact, double* rate) {
+    const int64_t pitch = P.pitch;
     double vol = (double)cst.volume[p] * (double)det3(load_m3(in.F, p, pitch));
     double T = in.temperature[p], W = in.water[p];
     double sat = W / ((double)P.water_density * vol);
@@ -270,15 +295,38 @@ __device__ __forceinline__ void surface_owners_body(Arg<Params, kRef> P, Arg<BkS
                 - (double)P.latent * loss;
     double exch = h * exposed + (double)P.tray_transfer * contact;
     if (P.water_enabled) exch += (double)(P.latent * P.surface_loss) * sat * exposed;
-    if (lane == 0) {
-        sf.owner_heat[o] = heat;
-        sf.owner_loss[o] = loss;
-        if (sf.accumulate_water_losses) {
-            sf.accumulate_water_losses[p] += (double)sf.accumulate_time_step * loss;
-            sf.accumulate_heat_exchanges[p] += (double)sf.accumulate_time_step * heat;
-        }
+    rate[0] = heat;
+    rate[1] = loss;
+    rate[2] = exch;
+}
+
+// Stores owner o's rates and advances its accumulators when `sf` names them.
+template <class SF>
+__device__ __forceinline__ void owner_store(const SF& sf, int64_t o, int p, const double* rate) {
+    sf.owner_heat[o] = rate[0];
+    sf.owner_loss[o] = rate[1];
+    if (sf.accumulate_water_losses) {
+        sf.accumulate_water_losses[p] += (double)sf.accumulate_time_step * rate[1];
+        sf.accumulate_heat_exchanges[p] += (double)sf.accumulate_time_step * rate[0];
     }
-    Stencil st = make_stencil(load_v3(in.x, p, pitch), P.origin, P.dx, P.R);
+}
+
+template <bool kRef = false>
+__device__ __forceinline__ void surface_owners_warp_body(Arg<Params, kRef> P, Arg<BkState, kRef> in,
+                                                         Arg<BkConstants, kRef> cst, Arg<BkSurface, kRef> sf,
+                                                         Arg<GridPtrs, kRef> g, int32_t* sim_flags, Slot sl) {
+    const int lane = threadIdx.x & 31;
+    const int64_t o = (sl.block * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (o >= sf.owner_count) return;  // whole warps
+    const int p = sf.owners[o];
+    double exposed = 0.0, contact = 0.0;
+    if (lane == 0) owner_areas(sf, o, exposed, contact);
+    exposed = __shfl_sync(kFull, exposed, 0);
+    contact = __shfl_sync(kFull, contact, 0);
+    double rate[3];
+    owner_rates(P, in, cst, p, exposed, contact, rate);
+    if (lane == 0) owner_store(sf, o, p, rate);
+    Stencil st = make_stencil(load_v3(in.x, p, P.pitch), P.origin, P.dx, P.R);
     if (!st.valid) {
         if (lane == 0) set_flag(sim_flags, 1);
         return;
@@ -288,14 +336,10 @@ __device__ __forceinline__ void surface_owners_body(Arg<Params, kRef> P, Arg<BkS
         node_offset(lane, ox, oy, oz);
         double w = (double)(st.w[0][ox] * st.w[1][oy] * st.w[2][oz]);
         int64_t node = node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R);
-        atomicAdd(g.f[4] + node, w * heat);
-        atomicAdd(g.f[5] + node, w * loss);
-        atomicAdd(g.f[6] + node, w * exch);
+        atomicAdd(g.f[4] + node, w * rate[0]);
+        atomicAdd(g.f[5] + node, w * rate[1]);
+        atomicAdd(g.f[6] + node, w * rate[2]);
     }
-}
-
-__global__ void k_surface_owners(Params P, BkState in, BkConstants cst, BkSurface sf, GridPtrs g, int32_t* sim_flags) {
-    surface_owners_body(P, in, cst, sf, g, sim_flags, grid_slot());
 }
 
 // ---------------------------------------------------------- transport P2G
@@ -307,19 +351,28 @@ __global__ void k_surface_owners(Params P, BkState in, BkConstants cst, BkSurfac
 // relative, and the node temperature E/C by ~3e-5 K, whose flux over a substep changes
 // temperatures by ~1e-13 K. The run loop then issues float32 multiply-adds and one 16-byte
 // broadcast load per particle instead of float64 ones and a conversion per node.
-template <int kT, int kTile>
+// The routine is shared with the surface terms (heat, loss and exchange of the face owners into
+// node fields 4..6): kF fields starting at node field kFirst, values of invalid threads ignored.
+template <int kT, int kTile, int kF = 4>
 struct TransportTile {
     float w[kT][9];
     float4 val[kT];
-    double tile[4][kTile];
+    double tile[kF][kTile];
 };
 
-template <int kT, int kTile>
-__device__ void transport_scatter_block(TransportTile<kT, kTile>& sm, const Params& P, const GridPtrs& g, int* box,
+template <int kT, int kTile, int kF = 4, int kFirst = 0>
+__device__ void transport_scatter_block(TransportTile<kT, kTile, kF>& sm, const Params& P, const GridPtrs& g, int* box,
                                         bool valid, const Stencil& st, const double* val) {
+    static_assert(kF >= 1 && kF <= 4 && kFirst + kF <= 7, "node fields 0..6, at most four at a time");
     const int tid = threadIdx.x, lane = tid & 31;
-    sm.val[tid] = valid ? make_float4((float)val[0], (float)val[1], (float)val[2], (float)val[3])
-                        : make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 v4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid) {
+        v4.x = (float)val[0];
+        if (kF > 1) v4.y = (float)val[1];
+        if (kF > 2) v4.z = (float)val[2];
+        if (kF > 3) v4.w = (float)val[3];
+    }
+    sm.val[tid] = v4;
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -327,7 +380,7 @@ __device__ void transport_scatter_block(TransportTile<kT, kTile>& sm, const Para
     const BlockBox bb = block_box(box, valid, st.b, kTile);  // synchronises the block
     for (int t = tid; t < bb.count; t += kT)
 #pragma unroll
-        for (int f = 0; f < 4; ++f) sm.tile[f][t] = 0.0;
+        for (int f = 0; f < kF; ++f) sm.tile[f][t] = 0.0;
     __syncthreads();
     long long key = valid ? pack_base(st.b) : -1;
     long long prev = __shfl_up_sync(kFull, key, 1);
@@ -341,33 +394,81 @@ __device__ void transport_scatter_block(TransportTile<kT, kTile>& sm, const Para
         int e = starts ? __ffs(starts) - 1 : 32;
         int b0 = __shfl_sync(kFull, st.b[0], s), b1 = __shfl_sync(kFull, st.b[1], s), b2 = __shfl_sync(kFull, st.b[2], s);
         if (lane < 27) {
-            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            float2 a01 = {0.f, 0.f}, a23 = {0.f, 0.f};
             for (int k = warp_base + s; k < warp_base + e; ++k) {
                 const float w = sm.w[k][ox] * sm.w[k][3 + oy] * sm.w[k][6 + oz];
+                const float2 ww = make_float2(w, w);
                 const float4 v = sm.val[k];
-                acc[0] = fmaf(w, v.x, acc[0]);
-                acc[1] = fmaf(w, v.y, acc[1]);
-                acc[2] = fmaf(w, v.z, acc[2]);
-                acc[3] = fmaf(w, v.w, acc[3]);
+                a01 = ffma2(ww, make_float2(v.x, v.y), a01);
+                if (kF > 2) a23 = ffma2(ww, make_float2(v.z, v.w), a23);
             }
+            const float acc[4] = {a01.x, a01.y, a23.x, a23.y};
             if (bb.tiled) {
                 int t = tile_index(bb, b0 + ox, b1 + oy, b2 + oz);
 #pragma unroll
-                for (int f = 0; f < 4; ++f) atomicAdd(&sm.tile[f][t], (double)acc[f]);
+                for (int f = 0; f < kF; ++f) atomicAdd(&sm.tile[f][t], (double)acc[f]);
             } else {
                 int64_t node = node_index(b0 + ox, b1 + oy, b2 + oz, P.R);
 #pragma unroll
-                for (int f = 0; f < 4; ++f) atomicAdd(g.f[f] + node, (double)acc[f]);
+                for (int f = 0; f < kF; ++f) atomicAdd(g.f[kFirst + f] + node, (double)acc[f]);
             }
         }
     }
     __syncthreads();
     for (int t = tid; t < bb.count; t += kT) {
-        if (sm.tile[1][t] == 0.0 && sm.tile[0][t] == 0.0 && sm.tile[3][t] == 0.0) continue;
+        bool empty = true;
+#pragma unroll
+        for (int f = 0; f < kF; ++f) empty = empty && sm.tile[f][t] == 0.0;
+        if (empty) continue;
         int64_t node = tile_node(bb, t, P.R);
 #pragma unroll
-        for (int f = 0; f < 4; ++f) atomicAdd(g.f[f] + node, sm.tile[f][t]);
+        for (int f = 0; f < kF; ++f) atomicAdd(g.f[kFirst + f] + node, sm.tile[f][t]);
     }
+}
+
+template <bool kRef = false>
+__device__ __forceinline__ void surface_owners_tile_body(Arg<Params, kRef> P, Arg<BkState, kRef> in,
+                                                         Arg<BkConstants, kRef> cst, Arg<BkSurface, kRef> sf,
+                                                         Arg<GridPtrs, kRef> g, int32_t* sim_flags, Slot sl) {
+    __shared__ TransportTile<kOwnerThreads, kTileNodes, 3> sm;
+    const int64_t o = sl.block * (int64_t)kOwnerThreads + threadIdx.x;
+    bool valid = false;
+    Stencil st;
+    st.b[0] = st.b[1] = st.b[2] = 0;
+    double rate[3] = {0.0, 0.0, 0.0};
+    if (o < sf.owner_count) {
+        const int p = sf.owners[o];
+        double exposed, contact;
+        owner_areas(sf, o, exposed, contact);
+        owner_rates(P, in, cst, p, exposed, contact, rate);
+        owner_store(sf, o, p, rate);
+        st = make_stencil(load_v3(in.x, p, P.pitch), P.origin, P.dx, P.R);
+        valid = st.valid;
+        if (!valid) set_flag(sim_flags, 1);
+    }
+    // the owners' nodes lie inside the particles' transport box: no box to widen
+    transport_scatter_block<kOwnerThreads, kTileNodes, 3, 4>(sm, P, g, nullptr, valid, st, rate);
+}
+
+// Many owners take the tiled form (one thread each), few the warp form (one warp each).
+template <bool kRef = false>
+__device__ __forceinline__ void surface_owners_body(Arg<Params, kRef> P, Arg<BkState, kRef> in, Arg<BkConstants, kRef> cst,
+                                                    Arg<BkSurface, kRef> sf, Arg<GridPtrs, kRef> g, int32_t* sim_flags,
+                                                    bool tiled, Slot sl) {
+    if (tiled) surface_owners_tile_body<kRef>(P, in, cst, sf, g, sim_flags, sl);
+    else surface_owners_warp_body<kRef>(P, in, cst, sf, g, sim_flags, sl);
+}
+
+// Whether a body with `owners` face owners among `n` particles takes the tiled form, and its blocks.
+inline bool owners_tiled(int64_t owners, int64_t n) { return owners * 16 >= n; }
+inline unsigned owner_blocks(int64_t owners, int64_t n) {
+    const int64_t threads = owners_tiled(owners, n) ? owners : owners * 32;
+    return (unsigned)((threads + kOwnerThreads - 1) / kOwnerThreads);
+}
+
+__global__ void __launch_bounds__(kOwnerThreads) k_surface_owners(Params P, BkState in, BkConstants cst, BkSurface sf,
+                                                                 GridPtrs g, int32_t* sim_flags, int tiled) {
+    surface_owners_body(P, in, cst, sf, g, sim_flags, tiled != 0, grid_slot());
 }
 
 using ScatterTile = TransportTile<kThreads, kTileNodes>;
@@ -616,8 +717,10 @@ __global__ void k_grid_update(Params P, GridPtrs g) { grid_update_body(P, g, gri
 // Scalar G2P (thermal_water.py:206-229), local gas source (:238-245), gas stress (gas.py:16-35),
 // water stress (thermal_water.py:248-253) and momentum P2G (transfer.py:47-70) for one particle
 // per thread, then the warp-cooperative momentum scatter.
-// One particle's scatter record, six float4 (read as 128-bit broadcasts by the run loop):
-// {wx0 wx1 wx2 m} {wy0 wy1 wy2 q0} {wz0 wz1 wz2 q1} {A0 A1 A2 q2} {A3 A4 A5 -} {A6 A7 A8 -}.
+// One particle's scatter record: its nine stencil weights, axis-major rows of kThreads + 1 floats
+// (a lane reads row 3a + o of its node offset o on axis a; the padding puts the three rows a warp
+// reads in different banks), and four float4 read as 128-bit broadcasts by the run loop:
+// {m q0 q1 q2} {A0 A1 A2 A3} {A4 A5 A6 A7} {A8 - - -}.
 // The staged form first copies the block's particle planes (x, v, C, F and, for Ding, tau: 33
 // planes of 256 floats) into shared memory with bulk copies (cp.async.bulk, the TMA engine's 1-D
 // copy) issued by one thread and counted on an mbarrier, so the loads of a block are in flight
@@ -627,7 +730,10 @@ constexpr int kP2GPlanes = 33;
 struct P2GSmem {
     union {
         float planes[kP2GPlanes][kThreads];  // x 0-2, v 3-5, C 6-14, F 15-23, tau 24-32
-        float4 rec[kThreads][6];
+        struct {
+            float4 val[kThreads][4];
+            float w[9][kThreads + 1];
+        } rec;
     };
     float4 tile[kTileNodes];
     unsigned long long mbar;
@@ -810,17 +916,14 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
     }
     if constexpr (kStaged) __syncthreads();  // every thread has read its planes: the records reuse them
     {
-        float w[3][3];
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
-            for (int o = 0; o < 3; ++o) w[a][o] = valid ? st.w[a][o] : 0.f;
-        sm.rec[tid][0] = make_float4(w[0][0], w[0][1], w[0][2], mass);
-        sm.rec[tid][1] = make_float4(w[1][0], w[1][1], w[1][2], q[0]);
-        sm.rec[tid][2] = make_float4(w[2][0], w[2][1], w[2][2], q[1]);
-        sm.rec[tid][3] = make_float4(A[0], A[1], A[2], q[2]);
-        sm.rec[tid][4] = make_float4(A[3], A[4], A[5], 0.f);
-        sm.rec[tid][5] = make_float4(A[6], A[7], A[8], 0.f);
+            for (int o = 0; o < 3; ++o) sm.rec.w[3 * a + o][tid] = valid ? st.w[a][o] : 0.f;
+        sm.rec.val[tid][0] = make_float4(mass, q[0], q[1], q[2]);
+        sm.rec.val[tid][1] = make_float4(A[0], A[1], A[2], A[3]);
+        sm.rec.val[tid][2] = make_float4(A[4], A[5], A[6], A[7]);
+        sm.rec.val[tid][3] = make_float4(A[8], 0.f, 0.f, 0.f);
     }
     const BlockBox bb = block_box(g.bounds, valid, st.b);  // synchronises the block
     for (int t = tid; t < bb.count; t += kThreads) sm.tile[t] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -838,22 +941,31 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
         int e = starts ? __ffs(starts) - 1 : 32;
         int b0 = __shfl_sync(kFull, st.b[0], s), b1 = __shfl_sync(kFull, st.b[1], s), b2 = __shfl_sync(kFull, st.b[2], s);
         if (lane < 27) {
-            // Node j receives sum_k w_jk (m_k, q_k + A_k o_j): accumulate sum w m, sum w q, sum w A and
-            // apply the node's offset o_j once per run.
-            float am = 0.f, aq[3] = {0.f, 0.f, 0.f}, aA[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            // Node j receives sum_k w_jk (m_k, q_k + A_k o_j): accumulate sum w m, sum w q, sum w A
+            // (paired accumulators, one packed multiply-add per pair) and apply the node's offset
+            // o_j once per run.
+            float2 mq0 = {0.f, 0.f}, q12 = {0.f, 0.f}, A01 = {0.f, 0.f}, A23 = {0.f, 0.f};
+            float2 A45 = {0.f, 0.f}, A67 = {0.f, 0.f};
+            float A8 = 0.f;
+            const float* wx = sm.rec.w[ox];
+            const float* wy = sm.rec.w[3 + oy];
+            const float* wz = sm.rec.w[6 + oz];
 #pragma unroll 2
             for (int k = warp_base + s; k < warp_base + e; ++k) {
-                const float4 r0 = sm.rec[k][0], r1 = sm.rec[k][1], r2 = sm.rec[k][2];
-                const float4 r3 = sm.rec[k][3], r4 = sm.rec[k][4], r5 = sm.rec[k][5];
-                float w = pick(r0, ox) * pick(r1, oy) * pick(r2, oz);
-                am += w * r0.w;
-                aq[0] += w * r1.w;
-                aq[1] += w * r2.w;
-                aq[2] += w * r3.w;
-                aA[0] += w * r3.x; aA[1] += w * r3.y; aA[2] += w * r3.z;
-                aA[3] += w * r4.x; aA[4] += w * r4.y; aA[5] += w * r4.z;
-                aA[6] += w * r5.x; aA[7] += w * r5.y; aA[8] += w * r5.z;
+                const float w = wx[k] * wy[k] * wz[k];
+                const float2 ww = make_float2(w, w);
+                const float4 v0 = sm.rec.val[k][0], v1 = sm.rec.val[k][1], v2 = sm.rec.val[k][2];
+                mq0 = ffma2(ww, make_float2(v0.x, v0.y), mq0);
+                q12 = ffma2(ww, make_float2(v0.z, v0.w), q12);
+                A01 = ffma2(ww, make_float2(v1.x, v1.y), A01);
+                A23 = ffma2(ww, make_float2(v1.z, v1.w), A23);
+                A45 = ffma2(ww, make_float2(v2.x, v2.y), A45);
+                A67 = ffma2(ww, make_float2(v2.z, v2.w), A67);
+                A8 = fmaf(w, sm.rec.val[k][3].x, A8);
             }
+            const float am = mq0.x;
+            const float aq[3] = {mq0.y, q12.x, q12.y};
+            const float aA[9] = {A01.x, A01.y, A23.x, A23.y, A45.x, A45.y, A67.x, A67.y, A8};
             float ap[3];
 #pragma unroll
             for (int r = 0; r < 3; ++r)
@@ -1398,7 +1510,10 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
                 switch (vertex_block_threads(surface->vertex_count, surface->binding_count)) {
                     case 256: k_surface_vertices<256><<<nv, 256, 0, s>>>(P, in->x, in->F, *surface); break;
                     case 128: k_surface_vertices<128><<<nv, 128, 0, s>>>(P, in->x, in->F, *surface); break;
-                    default: k_surface_vertices<32><<<nv, 32, 0, s>>>(P, in->x, in->F, *surface); break;
+                    default:
+                        k_surface_vertices<32><<<vertex_launch_blocks(nv, 32), vertex_launch_threads(32), 0, s>>>(
+                            P, in->x, in->F, *surface);
+                        break;
                 }
                 profile_end(rec, s);
             }
@@ -1407,8 +1522,8 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
         if (surface->owner_count > 0) {
             {
                 int rec = profile_begin("surface_owners", s);
-                k_surface_owners<<<blocks_for(surface->owner_count * 32, kOwnerThreads), kOwnerThreads, 0, s>>>(
-                    P, *in, *constants, *surface, g, flags->simulation);
+                k_surface_owners<<<owner_blocks(surface->owner_count, p.n), kOwnerThreads, 0, s>>>(
+                    P, *in, *constants, *surface, g, flags->simulation, owners_tiled(surface->owner_count, p.n));
                 profile_end(rec, s);
             }
             if (int rc = check_launch("bk_substep/surface_owners")) return rc;
@@ -1536,6 +1651,7 @@ struct BatchEntry {
     BkFlags flags;
     SurrogateDev sg;   // sf carries the surface accumulators of `out`
     int prescatter_ok;  // takes part in the transport prescatter
+    int owners_tiled;   // the surface terms take the tiled form (owners_tiled)
 };
 static_assert(sizeof(BatchEntry) % 4 == 0, "entries are copied as 4-byte words");
 
@@ -1578,7 +1694,7 @@ __device__ __forceinline__ Slot batch_load(const BatchArgs& b, int stage, BatchE
 }
 
 template <int kBlock>
-__global__ void __launch_bounds__(kBlock) kb_surface_vertices(BatchArgs b) {
+__global__ void __launch_bounds__(kBlock == 32 ? 32 * kVertexWarps : kBlock) kb_surface_vertices(BatchArgs b) {
     __shared__ BatchEntry e;
     const Slot sl = batch_load(b, kStVertices, e);
     surface_vertices_body<kBlock, true>(e.P, e.in.x, e.in.F, e.sf, sl);
@@ -1587,7 +1703,7 @@ __global__ void __launch_bounds__(kBlock) kb_surface_vertices(BatchArgs b) {
 __global__ void __launch_bounds__(kOwnerThreads) kb_surface_owners(BatchArgs b) {
     __shared__ BatchEntry e;
     const Slot sl = batch_load(b, kStOwners, e);
-    surface_owners_body<true>(e.P, e.in, e.cst, e.sf, e.g, e.flags.simulation, sl);
+    surface_owners_body<true>(e.P, e.in, e.cst, e.sf, e.g, e.flags.simulation, e.owners_tiled != 0, sl);
 }
 
 __global__ void __launch_bounds__(kThreads) kb_transport_scatter(BatchArgs b) {
@@ -1658,9 +1774,16 @@ int bk_batch_create(const BkBatchInstance* instances, int32_t count, BkBatch** b
     std::vector<BatchEntry> entries(2 * (size_t)count);
     std::vector<uint32_t> first((size_t)kBatchStages * (count + 1), 0);
     int64_t particles = 0, vertices = 0, bindings = 0;
-    for (int k = 0; k < count; ++k) particles += instances[k].params.n;
+    for (int k = 0; k < count; ++k) {
+        particles += instances[k].params.n;
+        if (instances[k].params.transport && instances[k].params.n > 0) {
+            vertices += instances[k].surface.vertex_count;
+            bindings += instances[k].surface.binding_count;
+        }
+    }
     BkBatch host;
     host.count = count;
+    host.vertex_block = vertex_block_threads(vertices, bindings);  // one block size for the whole launch
     for (int k = 0; k < count; ++k) {
         const BkBatchInstance& in = instances[k];
         const BkSubstepParams& p = in.params;
@@ -1690,6 +1813,7 @@ int bk_batch_create(const BkBatchInstance* instances, int32_t count, BkBatch** b
             e.flags = in.flags;
             e.sg = surrogate_dev(surrogate ? p.surrogate : nullptr);
             e.prescatter_ok = p.transport && !p.keep_transport_fields && !surrogate;
+            e.owners_tiled = owners_tiled(in.surface.owner_count, p.n);
             const uintptr_t bases = (uintptr_t)a.x | (uintptr_t)a.v | (uintptr_t)a.C | (uintptr_t)a.F |
                                     (p.material == 1 ? (uintptr_t)a.tau : 0);
             host.staged = host.staged && p.pitch % 4 == 0 && (bases & 15) == 0;
@@ -1700,11 +1824,9 @@ int bk_batch_create(const BkBatchInstance* instances, int32_t count, BkBatch** b
         const int64_t n = p.n;
         if (n > 0) {
             if (p.transport) {
-                blocks[kStVertices] = (uint32_t)in.surface.vertex_count;
-                blocks[kStOwners] = blocks_for(in.surface.owner_count * 32, kOwnerThreads);
+                blocks[kStVertices] = vertex_launch_blocks(in.surface.vertex_count, host.vertex_block);
+                blocks[kStOwners] = owner_blocks(in.surface.owner_count, n);
                 blocks[kStScatter] = blocks_for(n, kThreads);
-                vertices += in.surface.vertex_count;
-                bindings += in.surface.binding_count;
             }
             // node-box passes: about one block per 2048 particles (256 nodes at 8 particles a cell)
             const uint32_t box = (uint32_t)std::min<int64_t>(std::max<int64_t>(1, (n + 2047) / 2048), 4 * sms);
@@ -1727,7 +1849,6 @@ int bk_batch_create(const BkBatchInstance* instances, int32_t count, BkBatch** b
         }
     }
     for (int st = 0; st < kBatchStages; ++st) host.total[st] = first[(size_t)st * (count + 1) + count];
-    host.vertex_block = vertex_block_threads(vertices, bindings);
     BkBatch* out = new BkBatch(host);
     if (cudaMalloc(&out->entries, entries.size() * sizeof(BatchEntry)) != cudaSuccess ||
         cudaMalloc(&out->first, first.size() * sizeof(uint32_t)) != cudaSuccess) {
@@ -1762,7 +1883,7 @@ int bk_batch_substep(BkBatch* batch, int32_t parity, int32_t phases, int32_t pre
             switch (B.vertex_block) {
                 case 256: kb_surface_vertices<256><<<T[kStVertices], 256, 0, s>>>(a); break;
                 case 128: kb_surface_vertices<128><<<T[kStVertices], 128, 0, s>>>(a); break;
-                default: kb_surface_vertices<32><<<T[kStVertices], 32, 0, s>>>(a); break;
+                default: kb_surface_vertices<32><<<T[kStVertices], vertex_launch_threads(32), 0, s>>>(a); break;
             }
             profile_end(rec, s);
             if (int rc = check_launch("bk_batch_substep/surface_vertices")) return rc;
