@@ -5,11 +5,12 @@ temperatures). Two substeps of every instance -- state A -> B and B -> A, which 
 ping-pong states back -- are captured once into a CUDA graph. ``Advance`` replays the graph: one
 host call per two substeps of the whole batch, no per-kernel launch cost.
 
-With ``launch="table"`` (the default) each stage of the substep is ONE launch for the whole batch
-over a device table of the instances (``bk_batch_create``/``bk_batch_substep``): 8-10 launches per
-substep whatever the batch size, each filling the GPU with the blocks of every instance. With
-``launch="streams"`` every instance launches its own kernels, spread over several streams so that
-the kernels of small bodies run side by side.
+With ``launch="table"`` (the default) each stage of the substep is one launch per group of
+instances over a device table of them (``bk_batch_create``/``bk_batch_substep``): 8-10 launches per
+substep and group whatever the batch size, each filling the GPU with the blocks of its instances,
+and the groups on their own streams so that different stages (the latency-bound return map of one
+group, the scatter of another) share the GPU. With ``launch="streams"`` every instance launches its
+own kernels, spread over several streams so that the kernels of small bodies run side by side.
 """
 from __future__ import annotations
 
@@ -22,7 +23,12 @@ from .physics.substep import PHASE_MECHANICS, PHASE_TRANSPORT, BkBatchInstance
 
 
 class BatchedSimulators:
-    def __init__(self, simulators, streams=8, launch="table"):
+    """``launch="table"``: ``groups`` instance tables (instances dealt out by particle count so the
+    groups weigh about the same), each stepped by one launch per stage on a stream of its own, so
+    that the stages of different groups overlap on the GPU. ``launch="streams"``: every instance
+    launches its own kernels, instances spread over ``streams`` streams."""
+
+    def __init__(self, simulators, streams=8, launch="table", groups=2):
         self.sims = list(simulators)
         if not self.sims:
             raise ValueError("no simulators")
@@ -37,8 +43,12 @@ class BatchedSimulators:
         self.device = self.sims[0].device
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(max(1, int(streams)))]
         self.graph = None
-        self._table = None      # bk_batch_create handle
-        self._layout = None     # the state pairs (and surrogates) the table and the graph were made for
+        self.groups = max(1, min(int(groups), len(self.sims)))
+        if launch == "table":
+            self.streams = self.streams[:self.groups] + [torch.cuda.Stream(device=self.device)
+                                                         for _ in range(self.groups - len(self.streams))]
+        self._tables = []       # bk_batch_create handles, one per group
+        self._layout = None     # the state pairs (and surrogates) the tables and the graph were made for
         self.particle_count = sum(s.particle_data.particle_count for s in self.sims)
 
     @staticmethod
@@ -60,41 +70,56 @@ class BatchedSimulators:
         if layout == self._layout:
             return
         self.graph = None
-        self._free_table()
+        self._free_tables()
         if self.launch == "table":
             lib = self.sims[0]._engine.lib
-            table = (BkBatchInstance * len(self.sims))()
-            for k, sim in enumerate(self.sims):
-                table[k] = sim._engine.batch_instance(sim._current, sim.next_state)
-            handle = ctypes.c_void_p()
-            _lib.call_raw(lib.bk_batch_create, "bk_batch_create", table, len(self.sims), ctypes.byref(handle))
-            self._table = handle
+            # largest first, each to the lightest group so far
+            order = sorted(range(len(self.sims)), key=lambda k: -self.sims[k].particle_data.particle_count)
+            members, weight = [[] for _ in range(self.groups)], [0] * self.groups
+            for k in order:
+                g = weight.index(min(weight))
+                members[g].append(k)
+                weight[g] += self.sims[k].particle_data.particle_count
+            for group in members:
+                table = (BkBatchInstance * len(group))()
+                for j, k in enumerate(group):
+                    sim = self.sims[k]
+                    table[j] = sim._engine.batch_instance(sim._current, sim.next_state)
+                handle = ctypes.c_void_p()
+                _lib.call_raw(lib.bk_batch_create, "bk_batch_create", table, len(group), ctypes.byref(handle))
+                self._tables.append(handle)
         self._layout = layout
 
-    def _free_table(self):
-        if self._table is not None and self._table.value:
-            self.sims[0]._engine.lib.bk_batch_destroy(self._table)
-        self._table = None
+    def _free_tables(self):
+        for handle in self._tables:
+            if handle.value:
+                self.sims[0]._engine.lib.bk_batch_destroy(handle)
+        self._tables = []
 
     def __del__(self):
         try:
-            self._free_table()
+            self._free_tables()
         except Exception:
             pass
 
     def _record(self):
         self._ensure_layout()
+        main = torch.cuda.current_stream()
         if self.launch == "table":
             # parity 0 steps every instance A -> B and scatters B's transport fields ahead;
             # parity 1 steps B -> A on them
             lib = self.sims[0]._engine.lib
-            stream = _lib.stream_handle()
             phases = PHASE_TRANSPORT | PHASE_MECHANICS
-            for parity, prescattered, ahead in ((0, 0, 1), (1, 1, 0)):
-                _lib.call_raw(lib.bk_batch_substep, "bk_batch_substep", self._table, parity, phases, prescattered,
-                              ahead, stream)
+            for table, s in zip(self._tables, self.streams):
+                s.wait_stream(main)
+                with torch.cuda.stream(s):
+                    stream = _lib.stream_handle()
+                    for parity, prescattered, ahead in ((0, 0, 1), (1, 1, 0)):
+                        _lib.call_raw(lib.bk_batch_substep, "bk_batch_substep", table, parity, phases, prescattered,
+                                      ahead, stream)
+            for s in self.streams[:len(self._tables)]:
+                main.wait_stream(s)
             return
-        main = torch.cuda.current_stream()
         for k, sim in enumerate(self.sims):
             s = self.streams[k % len(self.streams)]
             s.wait_stream(main)

@@ -346,17 +346,15 @@ __device__ __forceinline__ void surface_owners_warp_body(Arg<Params, kRef> P, Ar
 // physics/thermal_water.py:108-137 (volume, capacity, energy, water), warp-cooperative per stencil run.
 // The block routine scatters its threads' particles; each thread passes its stencil, whether it is
 // valid, and its four values (V0 det F, capacity, capacity T, W). Every thread of the block calls it.
-// A run's sums are formed in float32 and added to the float64 node fields (the reference adds each
-// particle's float64 term): within a run of at most 32 particles that moves a node sum by ~1e-7
-// relative, and the node temperature E/C by ~3e-5 K, whose flux over a substep changes
-// temperatures by ~1e-13 K. The run loop then issues float32 multiply-adds and one 16-byte
-// broadcast load per particle instead of float64 ones and a conversion per node.
+// The run sums are float64, as the reference's float64 atomics: float32 partial sums moved the
+// node temperature E/C by ~3e-5 K, harmless to the trajectory but enough to make finite
+// differences of the loss in the initial temperatures disagree with the adjoint by several percent.
 // The routine is shared with the surface terms (heat, loss and exchange of the face owners into
 // node fields 4..6): kF fields starting at node field kFirst, values of invalid threads ignored.
 template <int kT, int kTile, int kF = 4>
 struct TransportTile {
     float w[kT][9];
-    float4 val[kT];
+    double val[kT][kF];
     double tile[kF][kTile];
 };
 
@@ -365,14 +363,8 @@ __device__ void transport_scatter_block(TransportTile<kT, kTile, kF>& sm, const 
                                         bool valid, const Stencil& st, const double* val) {
     static_assert(kF >= 1 && kF <= 4 && kFirst + kF <= 7, "node fields 0..6, at most four at a time");
     const int tid = threadIdx.x, lane = tid & 31;
-    float4 v4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (valid) {
-        v4.x = (float)val[0];
-        if (kF > 1) v4.y = (float)val[1];
-        if (kF > 2) v4.z = (float)val[2];
-        if (kF > 3) v4.w = (float)val[3];
-    }
-    sm.val[tid] = v4;
+#pragma unroll
+    for (int f = 0; f < kF; ++f) sm.val[tid][f] = valid ? val[f] : 0.0;
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -394,23 +386,22 @@ __device__ void transport_scatter_block(TransportTile<kT, kTile, kF>& sm, const 
         int e = starts ? __ffs(starts) - 1 : 32;
         int b0 = __shfl_sync(kFull, st.b[0], s), b1 = __shfl_sync(kFull, st.b[1], s), b2 = __shfl_sync(kFull, st.b[2], s);
         if (lane < 27) {
-            float2 a01 = {0.f, 0.f}, a23 = {0.f, 0.f};
+            double acc[kF];
+#pragma unroll
+            for (int f = 0; f < kF; ++f) acc[f] = 0.0;
             for (int k = warp_base + s; k < warp_base + e; ++k) {
-                const float w = sm.w[k][ox] * sm.w[k][3 + oy] * sm.w[k][6 + oz];
-                const float2 ww = make_float2(w, w);
-                const float4 v = sm.val[k];
-                a01 = ffma2(ww, make_float2(v.x, v.y), a01);
-                if (kF > 2) a23 = ffma2(ww, make_float2(v.z, v.w), a23);
+                const double w = (double)(sm.w[k][ox] * sm.w[k][3 + oy] * sm.w[k][6 + oz]);
+#pragma unroll
+                for (int f = 0; f < kF; ++f) acc[f] += w * sm.val[k][f];
             }
-            const float acc[4] = {a01.x, a01.y, a23.x, a23.y};
             if (bb.tiled) {
                 int t = tile_index(bb, b0 + ox, b1 + oy, b2 + oz);
 #pragma unroll
-                for (int f = 0; f < kF; ++f) atomicAdd(&sm.tile[f][t], (double)acc[f]);
+                for (int f = 0; f < kF; ++f) atomicAdd(&sm.tile[f][t], acc[f]);
             } else {
                 int64_t node = node_index(b0 + ox, b1 + oy, b2 + oz, P.R);
 #pragma unroll
-                for (int f = 0; f < kF; ++f) atomicAdd(g.f[kFirst + f] + node, (double)acc[f]);
+                for (int f = 0; f < kF; ++f) atomicAdd(g.f[kFirst + f] + node, acc[f]);
             }
         }
     }

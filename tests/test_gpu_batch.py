@@ -29,15 +29,15 @@ def _compare(batched, single, scs, steps):
                                    s.current_state.material_state.porosities.cpu().numpy(), rtol=0, atol=1e-6)
 
 
-@pytest.mark.parametrize("launch", ["table", "streams"])
+@pytest.mark.parametrize("launch,groups", [("table", 2), ("table", 1), ("streams", 1)])
 @pytest.mark.parametrize("prestrain", [(0.0, 0.0), (0.04, 0.1)])
-def test_graph_replay_matches_individual_advance(prestrain, launch):
+def test_graph_replay_matches_individual_advance(prestrain, launch, groups):
     from baking_b200 import scenes
     from baking_b200.batch import BatchedSimulators
     scs = bodies(prestrain)
     batched = [scenes.make_simulator(s, diagnostics="lean") for s in scs]
     single = [scenes.make_simulator(s, diagnostics="lean") for s in scs]
-    batch = BatchedSimulators(batched, streams=4, launch=launch).capture()   # capture runs two substeps
+    batch = BatchedSimulators(batched, streams=4, launch=launch, groups=groups).capture()   # capture runs two substeps
     batch.Advance(10)
     for sim in single:
         sim.AdvanceUnchecked(12)
