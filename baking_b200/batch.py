@@ -5,12 +5,10 @@ temperatures). Two substeps of every instance -- state A -> B and B -> A, which 
 ping-pong states back -- are captured once into a CUDA graph. ``Advance`` replays the graph: one
 host call per two substeps of the whole batch, no per-kernel launch cost.
 
-With ``launch="table"`` (the default) each stage of the substep is one launch per group of
-instances over a device table of them (``bk_batch_create``/``bk_batch_substep``): 8-10 launches per
-substep and group whatever the batch size, each filling the GPU with the blocks of its instances,
-and the groups on their own streams so that different stages (the latency-bound return map of one
-group, the scatter of another) share the GPU. With ``launch="streams"`` every instance launches its
-own kernels, spread over several streams so that the kernels of small bodies run side by side.
+Small bodies go through device tables of instances (``bk_batch_create``/``bk_batch_substep``):
+each stage of the substep is one launch per table, 8-10 launches per substep whatever the number
+of bodies. Large bodies launch their own kernels on several streams, so that their kernels and
+stages interleave on the GPU (``BatchedSimulators`` below says which body goes where).
 """
 from __future__ import annotations
 
@@ -23,12 +21,20 @@ from .physics.substep import PHASE_MECHANICS, PHASE_TRANSPORT, BkBatchInstance
 
 
 class BatchedSimulators:
-    """``launch="table"``: ``groups`` instance tables (instances dealt out by particle count so the
-    groups weigh about the same), each stepped by one launch per stage on a stream of its own, so
-    that the stages of different groups overlap on the GPU. ``launch="streams"``: every instance
-    launches its own kernels, instances spread over ``streams`` streams."""
+    """Where each instance's kernels come from:
 
-    def __init__(self, simulators, streams=8, launch="table", groups=2):
+    * ``launch="auto"`` (default): bodies below ``table_particles`` particles go through instance
+      tables, larger ones launch their own kernels. Small bodies are launch-bound, and a table steps
+      any number of them in 8-10 launches per substep; a large body fills the GPU with its own
+      launches, and on separate streams the kernels of different bodies and stages interleave
+      (a table launch holds one stage of all its instances, 10-15% slower per kernel than a plain
+      launch because every block first copies its instance entry into shared memory).
+    * ``launch="table"``: every body through ``groups`` tables (dealt out by particle count so the
+      groups weigh about the same), each on a stream of its own.
+    * ``launch="streams"``: every body launches its own kernels, spread over ``streams`` streams.
+    """
+
+    def __init__(self, simulators, streams=8, launch="auto", groups=2, table_particles=50_000):
         self.sims = list(simulators)
         if not self.sims:
             raise ValueError("no simulators")
@@ -37,16 +43,22 @@ class BatchedSimulators:
                 raise ValueError("batched simulators must be past settling (settling_duration_s = 0)")
             if sim.retain_history:
                 raise ValueError("batched simulators keep no history")
-        if launch not in ("table", "streams"):
-            raise ValueError(f"launch must be 'table' or 'streams', not {launch!r}")
+        if launch not in ("auto", "table", "streams"):
+            raise ValueError(f"launch must be 'auto', 'table' or 'streams', not {launch!r}")
         self.launch = launch
         self.device = self.sims[0].device
-        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(max(1, int(streams)))]
-        self.graph = None
-        self.groups = max(1, min(int(groups), len(self.sims)))
         if launch == "table":
-            self.streams = self.streams[:self.groups] + [torch.cuda.Stream(device=self.device)
-                                                         for _ in range(self.groups - len(self.streams))]
+            self.table_sims = list(self.sims)
+        elif launch == "streams":
+            self.table_sims = []
+        else:
+            self.table_sims = [s for s in self.sims if s.particle_data.particle_count < table_particles]
+        tabled = {id(s) for s in self.table_sims}
+        self.stream_sims = [s for s in self.sims if id(s) not in tabled]
+        self.groups = max(1, min(int(groups), len(self.table_sims))) if self.table_sims else 0
+        count = self.groups + (max(1, int(streams)) if self.stream_sims else 0)
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(count)]
+        self.graph = None
         self._tables = []       # bk_batch_create handles, one per group
         self._layout = None     # the state pairs (and surrogates) the tables and the graph were made for
         self.particle_count = sum(s.particle_data.particle_count for s in self.sims)
@@ -71,19 +83,20 @@ class BatchedSimulators:
             return
         self.graph = None
         self._free_tables()
-        if self.launch == "table":
+        if self.table_sims:
             lib = self.sims[0]._engine.lib
+            sims = self.table_sims
             # largest first, each to the lightest group so far
-            order = sorted(range(len(self.sims)), key=lambda k: -self.sims[k].particle_data.particle_count)
+            order = sorted(range(len(sims)), key=lambda k: -sims[k].particle_data.particle_count)
             members, weight = [[] for _ in range(self.groups)], [0] * self.groups
             for k in order:
                 g = weight.index(min(weight))
                 members[g].append(k)
-                weight[g] += self.sims[k].particle_data.particle_count
+                weight[g] += sims[k].particle_data.particle_count
             for group in members:
                 table = (BkBatchInstance * len(group))()
                 for j, k in enumerate(group):
-                    sim = self.sims[k]
+                    sim = sims[k]
                     table[j] = sim._engine.batch_instance(sim._current, sim.next_state)
                 handle = ctypes.c_void_p()
                 _lib.call_raw(lib.bk_batch_create, "bk_batch_create", table, len(group), ctypes.byref(handle))
@@ -105,23 +118,20 @@ class BatchedSimulators:
     def _record(self):
         self._ensure_layout()
         main = torch.cuda.current_stream()
-        if self.launch == "table":
-            # parity 0 steps every instance A -> B and scatters B's transport fields ahead;
-            # parity 1 steps B -> A on them
-            lib = self.sims[0]._engine.lib
-            phases = PHASE_TRANSPORT | PHASE_MECHANICS
-            for table, s in zip(self._tables, self.streams):
-                s.wait_stream(main)
-                with torch.cuda.stream(s):
-                    stream = _lib.stream_handle()
-                    for parity, prescattered, ahead in ((0, 0, 1), (1, 1, 0)):
-                        _lib.call_raw(lib.bk_batch_substep, "bk_batch_substep", table, parity, phases, prescattered,
-                                      ahead, stream)
-            for s in self.streams[:len(self._tables)]:
-                main.wait_stream(s)
-            return
-        for k, sim in enumerate(self.sims):
-            s = self.streams[k % len(self.streams)]
+        # parity 0 steps every instance A -> B and scatters B's transport fields ahead; parity 1
+        # steps B -> A on them
+        lib = self.sims[0]._engine.lib
+        phases = PHASE_TRANSPORT | PHASE_MECHANICS
+        for table, s in zip(self._tables, self.streams):
+            s.wait_stream(main)
+            with torch.cuda.stream(s):
+                stream = _lib.stream_handle()
+                for parity, prescattered, ahead in ((0, 0, 1), (1, 1, 0)):
+                    _lib.call_raw(lib.bk_batch_substep, "bk_batch_substep", table, parity, phases, prescattered,
+                                  ahead, stream)
+        own = self.streams[self.groups:]
+        for k, sim in enumerate(self.stream_sims):
+            s = own[k % len(own)]
             s.wait_stream(main)
             with torch.cuda.stream(s):
                 a, b = sim._current, sim.next_state

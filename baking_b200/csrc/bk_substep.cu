@@ -1649,20 +1649,17 @@ static_assert(sizeof(BatchEntry) % 4 == 0, "entries are copied as 4-byte words")
 struct BatchArgs {
     const BatchEntry* entries;  // [2][count]: parity 0 steps states[0] -> states[1], parity 1 back
     const uint32_t* first;      // [kBatchStages][count + 1]: first block of each instance per stage
+    const int32_t* owner;       // the instance of every block of every stage, stage by stage
+    uint32_t owner_offset[kBatchStages];  // where each stage's blocks start in `owner`
     int count, parity, prescattered, prescatter_next;
 };
 
-// The instance that owns this block in `stage` (the last one whose first block is at or below
-// blockIdx.x, which skips instances given no blocks) and the block's slot within it.
+// The instance that owns this block in `stage` (one load from the block map) and the block's slot
+// within it.
 __device__ __forceinline__ Slot batch_find(const BatchArgs& b, int stage, int& k) {
+    k = __ldg(b.owner + b.owner_offset[stage] + blockIdx.x);
     const uint32_t* f = b.first + (size_t)stage * (b.count + 1);
-    int lo = 0, hi = b.count - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(f + mid) <= blockIdx.x) lo = mid; else hi = mid - 1;
-    }
-    k = lo;
-    const uint32_t f0 = __ldg(f + lo), f1 = __ldg(f + lo + 1);
+    const uint32_t f0 = __ldg(f + k), f1 = __ldg(f + k + 1);
     return Slot{(int)(blockIdx.x - f0), (int)(f1 - f0)};
 }
 
@@ -1747,6 +1744,8 @@ struct BkBatch {
     int count = 0;
     BatchEntry* entries = nullptr;  // device [2][count]
     uint32_t* first = nullptr;      // device [kBatchStages][count + 1]
+    int32_t* owner = nullptr;       // device: instance of each block, stage by stage
+    uint32_t owner_offset[kBatchStages] = {};
     uint32_t total[kBatchStages] = {};
     int vertex_block = 32;
     bool staged = true;             // every instance allows the bulk-staged P2G
@@ -1839,19 +1838,30 @@ int bk_batch_create(const BkBatchInstance* instances, int32_t count, BkBatch** b
             f[k + 1] = f[k] + blocks[st];
         }
     }
-    for (int st = 0; st < kBatchStages; ++st) host.total[st] = first[(size_t)st * (count + 1) + count];
+    std::vector<int32_t> owner;
+    for (int st = 0; st < kBatchStages; ++st) {
+        host.total[st] = first[(size_t)st * (count + 1) + count];
+        host.owner_offset[st] = (uint32_t)owner.size();
+        for (int k = 0; k < count; ++k)
+            owner.insert(owner.end(), first[(size_t)st * (count + 1) + k + 1] - first[(size_t)st * (count + 1) + k], k);
+    }
+    BK_REQUIRE(owner.size() < (1ull << 31), "bk_batch_create: too many blocks");
+    if (owner.empty()) owner.push_back(0);
     BkBatch* out = new BkBatch(host);
     if (cudaMalloc(&out->entries, entries.size() * sizeof(BatchEntry)) != cudaSuccess ||
-        cudaMalloc(&out->first, first.size() * sizeof(uint32_t)) != cudaSuccess) {
+        cudaMalloc(&out->first, first.size() * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMalloc(&out->owner, owner.size() * sizeof(int32_t)) != cudaSuccess) {
         cudaFree(out->entries);
         cudaFree(out->first);
+        cudaFree(out->owner);
         delete out;
         cudaGetLastError();
         return fail(BK_ERR_LAUNCH, "bk_batch_create: device allocation failed");
     }
     if (cudaMemcpy(out->entries, entries.data(), entries.size() * sizeof(BatchEntry), cudaMemcpyHostToDevice) !=
             cudaSuccess ||
-        cudaMemcpy(out->first, first.data(), first.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaMemcpy(out->first, first.data(), first.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(out->owner, owner.data(), owner.size() * sizeof(int32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
         bk_batch_destroy(out);
         return fail(BK_ERR_LAUNCH, "bk_batch_create: table upload failed");
     }
@@ -1865,7 +1875,15 @@ int bk_batch_substep(BkBatch* batch, int32_t parity, int32_t phases, int32_t pre
     BK_REQUIRE(!prescatter_next || (phases & BK_PHASE_MECHANICS),
                "bk_batch_substep: the transport prescatter runs in the G2P kernel of a mechanics phase");
     const BkBatch& B = *batch;
-    const BatchArgs a{B.entries, B.first, B.count, parity, prescattered ? 1 : 0, prescatter_next ? 1 : 0};
+    BatchArgs a{};
+    a.entries = B.entries;
+    a.first = B.first;
+    a.owner = B.owner;
+    for (int st = 0; st < kBatchStages; ++st) a.owner_offset[st] = B.owner_offset[st];
+    a.count = B.count;
+    a.parity = parity;
+    a.prescattered = prescattered ? 1 : 0;
+    a.prescatter_next = prescatter_next ? 1 : 0;
     const uint32_t* T = B.total;
     cudaStream_t s = S(stream);
     if ((phases & BK_PHASE_TRANSPORT) && B.any_transport) {
@@ -1939,6 +1957,7 @@ int bk_batch_destroy(BkBatch* batch) {
     if (!batch) return BK_OK;
     cudaFree(batch->entries);
     cudaFree(batch->first);
+    cudaFree(batch->owner);
     delete batch;
     return BK_OK;
 }

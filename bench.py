@@ -518,10 +518,12 @@ def _timed(fn, dist, stream):
 def batched(args, rank, dist, net, count=64, steps=200):
     """64 independent dough balls (particles ~ U[5k, 200k], grids from {32, 48, 64, 96}^3, oven
     ~ U[150, 220] C, prestrain ~ U[0.04, 0.1] so that they yield), advanced together under one
-    captured CUDA graph of batched launches (one launch per stage for all 64, over the instance
-    table): exact return map, then the surrogate from the same initial states; also the exact map
-    with every instance launching its own kernels on 8 streams under a graph, and the batched
-    launches without the graph."""
+    captured CUDA graph (BatchedSimulators' default: bodies under 50k particles through instance
+    tables, one launch per stage for all of them, larger bodies with their own launches on 8
+    streams): exact return map, then the surrogate from the same initial states; also the exact
+    map with every body in a table and with every body on its own launches, the default launched
+    without the graph, and 128 small bodies (4-6k particles, 32-48^3) through tables against
+    their own launches."""
     import torch
     from baking_b200.batch import BatchedSimulators, RestoreStates, SnapshotStates
     from baking_b200.scenes import dough_batch, make_simulator
@@ -540,11 +542,13 @@ def batched(args, rank, dist, net, count=64, steps=200):
     exact.CheckState()
     del exact
     RestoreStates(sims, saved)
-    streams = BatchedSimulators(sims, launch="streams").capture()
-    RestoreStates(sims, saved)
-    t_streams, _ = _timed(lambda: streams.Advance(steps), dist, stream)
-    del streams
-    RestoreStates(sims, saved)
+    alt = {}
+    for launch in ("streams", "table"):
+        other = BatchedSimulators(sims, launch=launch).capture()
+        RestoreStates(sims, saved)
+        alt[launch], _ = _timed(lambda: other.Advance(steps), dist, stream)
+        del other
+        RestoreStates(sims, saved)
     surs = [ReturnMapSurrogate(net).attach(s) for s in sims]
     fast = BatchedSimulators(sims).capture()
     RestoreStates(sims, saved)
@@ -554,13 +558,35 @@ def batched(args, rank, dist, net, count=64, steps=200):
     fast.CheckState()
     paths = [sum(s.statistics()[k] for s in surs) for k in ("elastic", "surrogate", "exact_yielding")]
     return {"value": world * n * steps / t_exact, "unit": UNIT, "surrogate": world * n * steps / t_sur,
-            "without_graph": world * n * 20 / t_launch, "per_instance_launches": world * n * steps / t_streams,
+            "without_graph": world * n * 20 / t_launch,
+            "all_own_launches": world * n * steps / alt["streams"], "all_tables": world * n * steps / alt["table"],
+            "small_bodies": small_bodies(dist, stream, world, rank),
             "instances": count, "particles": n, "steps": steps,
             "surrogate_paths": dict(zip(("elastic", "surrogate", "exact_yielding"), paths)),
             "roofline": step_roofline(n, active, steps, t_exact),
             "surrogate_roofline": step_roofline(n, active, steps, t_sur),
             "scene": "dough balls (loaf dough: Ding + gas + thermal-water), dt 5e-5, one CUDA graph per 2 substeps",
-            "launch": "one launch per stage for all instances over a device instance table"}
+            "launch": "bodies under 50k particles: one launch per stage per instance table; larger: own launches"}
+
+
+def small_bodies(dist, stream, world, rank, count=128, steps=40):
+    """128 dough balls of 4-6k particles on 32^3-48^3 grids: launch-bound bodies, through instance
+    tables (BatchedSimulators' default for them) against their own launches on 8 streams."""
+    from baking_b200.batch import BatchedSimulators, RestoreStates, SnapshotStates
+    from baking_b200.scenes import dough_batch, make_simulator
+    bodies = dough_batch(count, seed=rank + 1, particles=(4000, 6000), resolutions=(32, 48), prestrain=(0.04, 0.1))
+    sims = [make_simulator(b, diagnostics="lean") for b in bodies]
+    n = sum(s.particle_data.particle_count for s in sims)
+    saved = SnapshotStates(sims)
+    out = {"instances": count, "particles": n, "steps": steps, "unit": UNIT}
+    for name, launch in (("tables", "auto"), ("own_launches", "streams")):
+        batch = BatchedSimulators(sims, launch=launch).capture()
+        RestoreStates(sims, saved)
+        t, _ = _timed(lambda: batch.Advance(steps), dist, stream)
+        out[name] = world * n * steps / t
+        del batch
+        RestoreStates(sims, saved)
+    return out
 
 
 def rollout_variant(sim, dist, stream, world, scene, fb_steps=64, every=FWD_BWD_CHECKPOINT_EVERY):

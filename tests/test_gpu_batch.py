@@ -30,15 +30,19 @@ def _compare(batched, single, scs, steps, porosity_atol=1e-6):
                                    atol=porosity_atol)
 
 
-@pytest.mark.parametrize("launch,groups", [("table", 2), ("table", 1), ("streams", 1)])
+@pytest.mark.parametrize("launch,groups,table_particles",
+                         [("table", 2, 0), ("table", 1, 0), ("streams", 1, 0), ("auto", 2, 12_000)])
 @pytest.mark.parametrize("prestrain", [(0.0, 0.0), (0.04, 0.1)])
-def test_graph_replay_matches_individual_advance(prestrain, launch, groups):
+def test_graph_replay_matches_individual_advance(prestrain, launch, groups, table_particles):
     from baking_b200 import scenes
     from baking_b200.batch import BatchedSimulators
     scs = bodies(prestrain)
     batched = [scenes.make_simulator(s, diagnostics="lean") for s in scs]
     single = [scenes.make_simulator(s, diagnostics="lean") for s in scs]
-    batch = BatchedSimulators(batched, streams=4, launch=launch, groups=groups).capture()   # capture runs two substeps
+    batch = BatchedSimulators(batched, streams=4, launch=launch, groups=groups, table_particles=table_particles)
+    if launch == "auto":  # bodies of 5k-20k particles: some through a table, some on their own
+        assert batch.table_sims and batch.stream_sims
+    batch.capture()   # capture runs two substeps
     batch.Advance(10)
     for sim in single:
         sim.AdvanceUnchecked(12)
