@@ -658,13 +658,14 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
 // atomic per tile node. Each particle also gathers the weight gradients of x (reads only).
 constexpr int kTileNodes = 512;
 
+// A particle's record: stencil weights as padded axis rows (a lane reads row 3a + o of its node
+// offsets without selects), and {q0 q1 q2 A0} {A1 A2 A3 A4} {A5 A6 A7 A8} as 128-bit broadcasts.
 struct ScatterSmem {
-    float4 rec[kThreads][6];  // {wx0 wx1 wx2 -} {wy0 wy1 wy2 q0} {wz0 wz1 wz2 q1} {A0 A1 A2 q2} {A3 A4 A5 -} {A6 A7 A8 -}
+    float4 val[kThreads][3];
+    float w[9][kThreads + 1];
     float4 tile[kTileNodes];
     int box[6];
 };
-
-__device__ __forceinline__ float pick3(const float4& v, int o) { return o == 0 ? v.x : (o == 1 ? v.y : v.z); }
 
 __global__ void __launch_bounds__(kThreads) k_adj_g2p_scatter(AdjParams P, BkState in, const float4* __restrict__ grid_v,
                                                             AdjState out_adj, AdjState in_adj,
@@ -730,17 +731,13 @@ __global__ void __launch_bounds__(kThreads) k_adj_g2p_scatter(AdjParams P, BkSta
         for (int c = 0; c < 3; ++c) in_adj.x[c * pitch + i] = 0.f;
     }
     {
-        float w[3][3];
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
-            for (int o = 0; o < 3; ++o) w[a][o] = valid ? st.w[a][o] : 0.f;
-        sm.rec[tid][0] = make_float4(w[0][0], w[0][1], w[0][2], 0.f);
-        sm.rec[tid][1] = make_float4(w[1][0], w[1][1], w[1][2], q[0]);
-        sm.rec[tid][2] = make_float4(w[2][0], w[2][1], w[2][2], q[1]);
-        sm.rec[tid][3] = make_float4(A[0], A[1], A[2], q[2]);
-        sm.rec[tid][4] = make_float4(A[3], A[4], A[5], 0.f);
-        sm.rec[tid][5] = make_float4(A[6], A[7], A[8], 0.f);
+            for (int o = 0; o < 3; ++o) sm.w[3 * a + o][tid] = valid ? st.w[a][o] : 0.f;
+        sm.val[tid][0] = make_float4(q[0], q[1], q[2], A[0]);
+        sm.val[tid][1] = make_float4(A[1], A[2], A[3], A[4]);
+        sm.val[tid][2] = make_float4(A[5], A[6], A[7], A[8]);
     }
     if (tid < 6) sm.box[tid] = tid < 3 ? INT_MAX : INT_MIN;
     __syncthreads();
@@ -783,19 +780,26 @@ __global__ void __launch_bounds__(kThreads) k_adj_g2p_scatter(AdjParams P, BkSta
         const int b0 = __shfl_sync(0xffffffffu, st.b[0], s0), b1 = __shfl_sync(0xffffffffu, st.b[1], s0),
                   b2 = __shfl_sync(0xffffffffu, st.b[2], s0);
         if (lane < 27) {
-            float aq[3] = {0.f, 0.f, 0.f}, aA[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            // paired accumulators, one packed multiply-add per pair (ffma2)
+            float2 q01 = {0.f, 0.f}, q2A0 = {0.f, 0.f}, A12 = {0.f, 0.f}, A34 = {0.f, 0.f};
+            float2 A56 = {0.f, 0.f}, A78 = {0.f, 0.f};
+            const float* wx = sm.w[ox];
+            const float* wy = sm.w[3 + oy];
+            const float* wz = sm.w[6 + oz];
 #pragma unroll 2
             for (int k = warp_base + s0; k < warp_base + e; ++k) {
-                const float4 r0 = sm.rec[k][0], r1 = sm.rec[k][1], r2 = sm.rec[k][2];
-                const float4 r3 = sm.rec[k][3], r4 = sm.rec[k][4], r5 = sm.rec[k][5];
-                const float w = pick3(r0, ox) * pick3(r1, oy) * pick3(r2, oz);
-                aq[0] += w * r1.w;
-                aq[1] += w * r2.w;
-                aq[2] += w * r3.w;
-                aA[0] += w * r3.x; aA[1] += w * r3.y; aA[2] += w * r3.z;
-                aA[3] += w * r4.x; aA[4] += w * r4.y; aA[5] += w * r4.z;
-                aA[6] += w * r5.x; aA[7] += w * r5.y; aA[8] += w * r5.z;
+                const float w = wx[k] * wy[k] * wz[k];
+                const float2 ww = make_float2(w, w);
+                const float4 v0 = sm.val[k][0], v1 = sm.val[k][1], v2 = sm.val[k][2];
+                q01 = ffma2(ww, make_float2(v0.x, v0.y), q01);
+                q2A0 = ffma2(ww, make_float2(v0.z, v0.w), q2A0);
+                A12 = ffma2(ww, make_float2(v1.x, v1.y), A12);
+                A34 = ffma2(ww, make_float2(v1.z, v1.w), A34);
+                A56 = ffma2(ww, make_float2(v2.x, v2.y), A56);
+                A78 = ffma2(ww, make_float2(v2.z, v2.w), A78);
             }
+            const float aq[3] = {q01.x, q01.y, q2A0.x};
+            const float aA[9] = {q2A0.y, A12.x, A12.y, A34.x, A34.y, A56.x, A56.y, A78.x, A78.y};
             float ap[3];
 #pragma unroll
             for (int r = 0; r < 3; ++r) ap[r] = aq[r] + (aA[3 * r] * fo[0] + aA[3 * r + 1] * fo[1] + aA[3 * r + 2] * fo[2]);
