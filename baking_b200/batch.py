@@ -122,8 +122,10 @@ class BatchedSimulators:
         # steps B -> A on them
         lib = self.sims[0]._engine.lib
         phases = PHASE_TRANSPORT | PHASE_MECHANICS
+        used = []  # only streams forked from `main` join it again (under capture, no other may)
         for table, s in zip(self._tables, self.streams):
             s.wait_stream(main)
+            used.append(s)
             with torch.cuda.stream(s):
                 stream = _lib.stream_handle()
                 for parity, prescattered, ahead in ((0, 0, 1), (1, 1, 0)):
@@ -132,13 +134,15 @@ class BatchedSimulators:
         own = self.streams[self.groups:]
         for k, sim in enumerate(self.stream_sims):
             s = own[k % len(own)]
-            s.wait_stream(main)
+            if k < len(own):
+                s.wait_stream(main)
+                used.append(s)
             with torch.cuda.stream(s):
                 a, b = sim._current, sim.next_state
                 # the second substep of the pair finds its transport fields scattered by the first
                 self._substep(sim, a, b, prescatter_next=True)
                 self._substep(sim, b, a, prescattered=True)
-        for s in self.streams:
+        for s in used:
             main.wait_stream(s)
 
     def capture(self):
