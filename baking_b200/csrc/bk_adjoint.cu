@@ -467,7 +467,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkS
                 float cg = 1.f, target = 1.f;
                 if (coupled) {
                     target = (float)(1.0 - (double)D.initial_porosity + (double)n_ret);
-                    cg = (float)cbrt((double)detFn / ((double)target * ((double)pr.g[0] * pr.g[1] * pr.g[2])));
+                    cg = cbrt_near_one((double)detFn / ((double)target * ((double)pr.g[0] * pr.g[1] * pr.g[2])));
 #pragma unroll
                     for (int k = 0; k < 3; ++k) gv[k] *= cg;
                     if (porosity_free) nret_b += por_b;  // porosity' = n_ret

@@ -797,6 +797,17 @@ struct FStored {
     }
 };
 
+// The float32 rounding of the cube root of v, for the volume corrections, whose ratios lie within
+// ~1e-6 of 1 (they undo spectral reconstruction roundoff). Near 1 it sums the binomial series
+// (1 + d)^(1/3) = 1 + d/3 - d^2/9 + 5 d^3/81 - 10 d^4/243 + ...; for |d| < 2^-10 the omitted terms
+// are below 3e-17, so the rounded result is that of the float64 cube root unless the root lies
+// within ~2e-16 (relative) of a float32 rounding boundary. Elsewhere it calls cbrt.
+BK_DEV float cbrt_near_one(double v) {
+    const double d = v - 1.0;
+    if (fabs(d) < 0x1p-10) return (float)(1.0 + d * (1.0 / 3.0 + d * (-1.0 / 9.0 + d * (5.0 / 81.0 - d * (10.0 / 243.0)))));
+    return (float)cbrt(v);
+}
+
 // Volume correction (gas mode), plastic gradient and porosity update shared by the exact and the
 // surrogate returns (ding.py:200-221).
 template <class FSrc>
@@ -810,7 +821,7 @@ BK_DEV void ding_close(const DingParamsDev& P, float por, const FSrc& F_src, flo
 #pragma unroll
         for (int e = 0; e < 9; ++e) { Fd.m[e] = (double)F_tot.m[e]; Fed.m[e] = (double)Fe.m[e]; }
         double vs = det3(Fd) / (target * det3(Fed));
-        float scale = (float)cbrt(vs);  // pow(vs, 1/3) in the reference
+        float scale = cbrt_near_one(vs);  // pow(vs, 1/3) in the reference
 #pragma unroll
         for (int e = 0; e < 9; ++e) Fe.m[e] *= scale;
     }

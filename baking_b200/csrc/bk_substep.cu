@@ -29,6 +29,7 @@
 #include <climits>
 #include <cstdio>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "baking_b200.h"
@@ -120,6 +121,43 @@ struct Slot {
     int block, blocks;
 };
 __device__ __forceinline__ Slot grid_slot() { return Slot{(int)blockIdx.x, (int)gridDim.x}; }
+
+// Programmatic dependent launch between the kernels of a substep: each is launched with
+// programmatic stream serialisation (launch_chained), so the launch of the next kernel and the
+// placement of its blocks overlap the tail of the one before it. Every such kernel first waits
+// until the kernel before it in the stream has completed and its memory is visible (which makes
+// the chain transitive), then lets the next kernel launch; its blocks only take SM slots left free
+// by blocks already running. A kernel without a programmatic predecessor returns from the wait at
+// once.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// The status of a launch_chained call, as check_launch reports a launch's.
+int check_chained(cudaError_t e, const char* name) {
+    if (e == cudaSuccess) return check_launch(name);
+    cudaGetLastError();
+    char msg[256];
+    snprintf(msg, sizeof msg, "%s: %s", name, cudaGetErrorString(e));
+    return fail(BK_ERR_LAUNCH, msg);
+}
+
+template <class... KArgs, class... Args>
+cudaError_t launch_chained(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t s,
+                           Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // How a kernel body takes its parameter structs: by value from a plain launch's parameter space
 // (a reference to a kernel parameter would make the compiler copy it to local memory), by
@@ -239,6 +277,7 @@ __device__ __forceinline__ void surface_vertices_body(Arg<Params, kRef> P, const
 template <int kBlock>
 __global__ void __launch_bounds__(kBlock == 32 ? 32 * kVertexWarps : kBlock) k_surface_vertices(Params P, const float* __restrict__ x,
                                                           const float* __restrict__ F, BkSurface sf) {
+    pdl_enter();
     surface_vertices_body<kBlock>(P, x, F, sf, grid_slot());
 }
 
@@ -351,24 +390,61 @@ __device__ __forceinline__ void surface_owners_warp_body(Arg<Params, kRef> P, Ar
 // differences of the loss in the initial temperatures disagree with the adjoint by several percent.
 // The routine is shared with the surface terms (heat, loss and exchange of the face owners into
 // node fields 4..6): kF fields starting at node field kFirst, values of invalid threads ignored.
-template <int kT, int kTile, int kF = 4>
-struct TransportTile {
+// Stencil weights of the block's particles, in one of two forms:
+// * kNodeWeights: each particle's 27 weights (w_x w_y) w_z, formed once by its own thread as the
+//   reference rounds them, in node-major rows of kT + 1 floats; lane j of a run reads row j at the
+//   particle's column, one conflict-free load in place of three loads and two multiplies per node;
+// * otherwise the nine axis weights per particle (3 loads and 2 multiplies per node), a third of
+//   the space: the form of the scatter inside the G2P kernel, whose eight blocks per SM leave the
+//   rest of the SM's shared memory to L1 for its spilled registers (the 27-weight rows there made
+//   that kernel 4 us slower at 1M particles while the standalone scatter gained 4 us).
+template <int kT, bool kNodeWeights>
+struct ScatterWeights;
+template <int kT>
+struct ScatterWeights<kT, true> {
+    float w[27][kT + 1];
+    __device__ __forceinline__ void put(int tid, bool valid, const Stencil& st) {
+#pragma unroll
+        for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+            for (int oy = 0; oy < 3; ++oy) {
+                const float wxy = st.w[0][ox] * st.w[1][oy];
+#pragma unroll
+                for (int oz = 0; oz < 3; ++oz) w[9 * ox + 3 * oy + oz][tid] = valid ? wxy * st.w[2][oz] : 0.f;
+            }
+    }
+    // weight of node (ox, oy, oz) = lane j for particle k
+    __device__ __forceinline__ float get(int k, int j, int, int, int) const { return w[j][k]; }
+};
+template <int kT>
+struct ScatterWeights<kT, false> {
     float w[kT][9];
+    __device__ __forceinline__ void put(int tid, bool valid, const Stencil& st) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int o = 0; o < 3; ++o) w[tid][3 * a + o] = valid ? st.w[a][o] : 0.f;
+    }
+    __device__ __forceinline__ float get(int k, int, int ox, int oy, int oz) const {
+        return w[k][ox] * w[k][3 + oy] * w[k][6 + oz];
+    }
+};
+
+template <int kT, int kTile, int kF = 4, bool kNodeWeights = true>
+struct TransportTile {
+    ScatterWeights<kT, kNodeWeights> w;
     double val[kT][kF];
     double tile[kF][kTile];
 };
 
-template <int kT, int kTile, int kF = 4, int kFirst = 0>
-__device__ void transport_scatter_block(TransportTile<kT, kTile, kF>& sm, const Params& P, const GridPtrs& g, int* box,
+template <int kT, int kTile, int kF = 4, int kFirst = 0, bool kNodeWeights = true>
+__device__ void transport_scatter_block(TransportTile<kT, kTile, kF, kNodeWeights>& sm, const Params& P, const GridPtrs& g, int* box,
                                         bool valid, const Stencil& st, const double* val) {
     static_assert(kF >= 1 && kF <= 4 && kFirst + kF <= 7, "node fields 0..6, at most four at a time");
     const int tid = threadIdx.x, lane = tid & 31;
 #pragma unroll
     for (int f = 0; f < kF; ++f) sm.val[tid][f] = valid ? val[f] : 0.0;
-#pragma unroll
-    for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int o = 0; o < 3; ++o) sm.w[tid][3 * a + o] = valid ? st.w[a][o] : 0.f;
+    sm.w.put(tid, valid, st);
     const BlockBox bb = block_box(box, valid, st.b, kTile);  // synchronises the block
     for (int t = tid; t < bb.count; t += kT)
 #pragma unroll
@@ -390,7 +466,7 @@ __device__ void transport_scatter_block(TransportTile<kT, kTile, kF>& sm, const 
 #pragma unroll
             for (int f = 0; f < kF; ++f) acc[f] = 0.0;
             for (int k = warp_base + s; k < warp_base + e; ++k) {
-                const double w = (double)(sm.w[k][ox] * sm.w[k][3 + oy] * sm.w[k][6 + oz]);
+                const double w = (double)sm.w.get(k, lane, ox, oy, oz);
 #pragma unroll
                 for (int f = 0; f < kF; ++f) acc[f] += w * sm.val[k][f];
             }
@@ -459,10 +535,12 @@ inline unsigned owner_blocks(int64_t owners, int64_t n) {
 
 __global__ void __launch_bounds__(kOwnerThreads) k_surface_owners(Params P, BkState in, BkConstants cst, BkSurface sf,
                                                                  GridPtrs g, int32_t* sim_flags, int tiled) {
+    pdl_enter();
     surface_owners_body(P, in, cst, sf, g, sim_flags, tiled != 0, grid_slot());
 }
 
-using ScatterTile = TransportTile<kThreads, kTileNodes>;
+// 256 nodes: the 27 weight rows of 256 particles leave room for no larger tile in 48 KB of static shared memory.
+using ScatterTile = TransportTile<kThreads, 256>;
 
 template <bool kRef = false>
 __device__ __forceinline__ void transport_scatter_body(Arg<Params, kRef> P, Arg<BkState, kRef> in,
@@ -489,11 +567,12 @@ __device__ __forceinline__ void transport_scatter_body(Arg<Params, kRef> P, Arg<
         val[2] = cap * in.temperature[i];
         val[3] = in.water[i];
     }
-    transport_scatter_block<kThreads, kTileNodes>(sm, P, g, g.bounds, valid, st, val);
+    transport_scatter_block<kThreads, 256>(sm, P, g, g.bounds, valid, st, val);
 }
 
 __global__ void __launch_bounds__(kThreads) k_transport_scatter(Params P, BkState in, BkConstants cst, GridPtrs g,
                                                                int32_t* sim_flags) {
+    pdl_enter();
     transport_scatter_body(P, in, cst, g, sim_flags, grid_slot());
 }
 
@@ -624,6 +703,7 @@ __device__ __forceinline__ void diffuse_body(Arg<Params, kRef> P, Arg<GridPtrs, 
 }
 
 __global__ void __launch_bounds__(kDiffThreads) k_diffuse(Params P, GridPtrs g, int32_t* errors) {
+    pdl_enter();
     diffuse_body(P, g, errors, grid_slot());
 }
 
@@ -644,7 +724,10 @@ __device__ __forceinline__ void clear_prescatter_body(Arg<Params, kRef> P, Arg<G
     }
 }
 
-__global__ void k_clear_prescatter(Params P, GridPtrs g) { clear_prescatter_body(P, g, grid_slot()); }
+__global__ void k_clear_prescatter(Params P, GridPtrs g) {
+    pdl_enter();
+    clear_prescatter_body(P, g, grid_slot());
+}
 
 // GridState.Clear (physics/grid.py:14-17) restricted to the previous substep's active box, the only
 // nodes holding nonzero momentum, mass or velocity; the grid of the last substep stays readable
@@ -664,7 +747,10 @@ __device__ __forceinline__ void clear_previous_body(Arg<Params, kRef> P, Arg<Gri
     }
 }
 
-__global__ void k_clear_previous(Params P, GridPtrs g) { clear_previous_body(P, g, grid_slot()); }
+__global__ void k_clear_previous(Params P, GridPtrs g) {
+    pdl_enter();
+    clear_previous_body(P, g, grid_slot());
+}
 
 // physics/grid.py:20-38 over the active box; clears the transport scatter fields behind it.
 template <bool kRef = false>
@@ -702,16 +788,19 @@ __device__ __forceinline__ void grid_update_body(Arg<Params, kRef> P, Arg<GridPt
     }
 }
 
-__global__ void k_grid_update(Params P, GridPtrs g) { grid_update_body(P, g, grid_slot()); }
+__global__ void k_grid_update(Params P, GridPtrs g) {
+    pdl_enter();
+    grid_update_body(P, g, grid_slot());
+}
 
 // ------------------------------------------------------------- fused P2G
 // Scalar G2P (thermal_water.py:206-229), local gas source (:238-245), gas stress (gas.py:16-35),
 // water stress (thermal_water.py:248-253) and momentum P2G (transfer.py:47-70) for one particle
 // per thread, then the warp-cooperative momentum scatter.
-// One particle's scatter record: its nine stencil weights, axis-major rows of kThreads + 1 floats
-// (a lane reads row 3a + o of its node offset o on axis a; the padding puts the three rows a warp
-// reads in different banks), and four float4 read as 128-bit broadcasts by the run loop:
-// {m q0 q1 q2} {A0 A1 A2 A3} {A4 A5 A6 A7} {A8 - - -}.
+// One particle's scatter record: its 27 stencil weights (w_x w_y) w_z, formed once by its own
+// thread, in node-major rows of kThreads + 1 floats (lane j of a run reads row j at the particle's
+// column: one conflict-free load per node in place of three loads and two multiplies), and
+// {m q0 q1 q2} {A0 A1 A2 A3} {A4 A5 A6 A7} read as 128-bit broadcasts plus A8.
 // The staged form first copies the block's particle planes (x, v, C, F and, for Ding, tau: 33
 // planes of 256 floats) into shared memory with bulk copies (cp.async.bulk, the TMA engine's 1-D
 // copy) issued by one thread and counted on an mbarrier, so the loads of a block are in flight
@@ -722,13 +811,25 @@ struct P2GSmem {
     union {
         float planes[kP2GPlanes][kThreads];  // x 0-2, v 3-5, C 6-14, F 15-23, tau 24-32
         struct {
-            float4 val[kThreads][4];
-            float w[9][kThreads + 1];
+            float4 val[kThreads][3];
+            float a8[kThreads];
+            float w[27][kThreads + 1];
         } rec;
     };
     float4 tile[kTileNodes];
     unsigned long long mbar;
 };
+// Above the 48 KB of static shared memory: the kernels take it as dynamic shared memory, opted in
+// per device before their first launch there.
+constexpr size_t kP2GSmemBytes = sizeof(P2GSmem);
+
+// Opts `kernel` into `bytes` of dynamic shared memory on the current device. Set on every launch:
+// a host call without device work, and correct after a device reset or in another context.
+int allow_smem(const void* kernel, size_t bytes, const char* what) {
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+        return check_launch(what);
+    return 0;
+}
 
 namespace stage {
 // Polls of a bulk copy's mbarrier before a block gives up (far beyond any copy's latency).
@@ -752,7 +853,8 @@ template <bool kStaged, bool kRef = false>
 __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef> in, Arg<BkState, kRef> out,
                                          Arg<BkConstants, kRef> cst, Arg<GridPtrs, kRef> g, Arg<BkFlags, kRef> flags,
                                          float* max_residuals, Slot sl) {
-    __shared__ P2GSmem sm;
+    extern __shared__ __align__(16) unsigned char p2g_smem[];
+    P2GSmem& sm = *reinterpret_cast<P2GSmem*>(p2g_smem);
     if (sl.block == 0 && threadIdx.x < 2) max_residuals[threadIdx.x] = 0.0f;
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t i = sl.block * (int64_t)kThreads + tid;
@@ -908,13 +1010,17 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
     if constexpr (kStaged) __syncthreads();  // every thread has read its planes: the records reuse them
     {
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+        for (int ox = 0; ox < 3; ++ox)
 #pragma unroll
-            for (int o = 0; o < 3; ++o) sm.rec.w[3 * a + o][tid] = valid ? st.w[a][o] : 0.f;
+            for (int oy = 0; oy < 3; ++oy) {
+                const float wxy = st.w[0][ox] * st.w[1][oy];
+#pragma unroll
+                for (int oz = 0; oz < 3; ++oz) sm.rec.w[9 * ox + 3 * oy + oz][tid] = valid ? wxy * st.w[2][oz] : 0.f;
+            }
         sm.rec.val[tid][0] = make_float4(mass, q[0], q[1], q[2]);
         sm.rec.val[tid][1] = make_float4(A[0], A[1], A[2], A[3]);
         sm.rec.val[tid][2] = make_float4(A[4], A[5], A[6], A[7]);
-        sm.rec.val[tid][3] = make_float4(A[8], 0.f, 0.f, 0.f);
+        sm.rec.a8[tid] = A[8];
     }
     const BlockBox bb = block_box(g.bounds, valid, st.b);  // synchronises the block
     for (int t = tid; t < bb.count; t += kThreads) sm.tile[t] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -938,12 +1044,10 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
             float2 mq0 = {0.f, 0.f}, q12 = {0.f, 0.f}, A01 = {0.f, 0.f}, A23 = {0.f, 0.f};
             float2 A45 = {0.f, 0.f}, A67 = {0.f, 0.f};
             float A8 = 0.f;
-            const float* wx = sm.rec.w[ox];
-            const float* wy = sm.rec.w[3 + oy];
-            const float* wz = sm.rec.w[6 + oz];
+            const float* wj = sm.rec.w[lane];
 #pragma unroll 2
             for (int k = warp_base + s; k < warp_base + e; ++k) {
-                const float w = wx[k] * wy[k] * wz[k];
+                const float w = wj[k];
                 const float2 ww = make_float2(w, w);
                 const float4 v0 = sm.rec.val[k][0], v1 = sm.rec.val[k][1], v2 = sm.rec.val[k][2];
                 mq0 = ffma2(ww, make_float2(v0.x, v0.y), mq0);
@@ -952,7 +1056,7 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
                 A23 = ffma2(ww, make_float2(v1.z, v1.w), A23);
                 A45 = ffma2(ww, make_float2(v2.x, v2.y), A45);
                 A67 = ffma2(ww, make_float2(v2.z, v2.w), A67);
-                A8 = fmaf(w, sm.rec.val[k][3].x, A8);
+                A8 = fmaf(w, sm.rec.a8[k], A8);
             }
             const float am = mq0.x;
             const float aq[3] = {mq0.y, q12.x, q12.y};
@@ -983,6 +1087,7 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
 template <bool kStaged>
 __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
                                                  BkFlags flags, float* max_residuals) {
+    pdl_enter();
     p2g_body<kStaged>(P, in, out, cst, g, flags, max_residuals, grid_slot());
 }
 
@@ -1238,7 +1343,7 @@ __device__ __forceinline__ void g2p_return_particle(const Params& P, const BkSta
 
 // Shared-memory node tile of the transport prescatter in k_g2p_return (128 particles per block).
 constexpr int kG2PTile = 256;
-using G2PTransportTile = TransportTile<128, kG2PTile>;
+using G2PTransportTile = TransportTile<128, kG2PTile, 4, false>;
 
 template <bool kRef = false>
 __device__ __forceinline__ void g2p_return_body(Arg<Params, kRef> P, Arg<BkState, kRef> in,
@@ -1277,12 +1382,13 @@ __device__ __forceinline__ void g2p_return_body(Arg<Params, kRef> P, Arg<BkState
                 val[3] = out.water[i];
             }
         }
-        transport_scatter_block<128, kG2PTile>(sm, P, g, g.bounds + 12, valid, st, val);
+        transport_scatter_block<128, kG2PTile, 4, 0, false>(sm, P, g, g.bounds + 12, valid, st, val);
     }
 }
 
 __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
                                                    BkDiagnostics diag, BkFlags flags, SurrogateDev sg) {
+    pdl_enter();
     g2p_return_body(P, in, out, cst, g, diag, flags, sg, grid_slot());
 }
 
@@ -1379,6 +1485,7 @@ __device__ __forceinline__ void g2p_return_surrogate_body(Arg<Params, kRef> P, A
 __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkState in, BkState out, BkConstants cst,
                                                              GridPtrs g, BkDiagnostics diag, BkFlags flags,
                                                              SurrogateDev sg) {
+    pdl_enter();
     g2p_return_surrogate_body(P, in, out, cst, g, diag, flags, sg, grid_slot());
 }
 
@@ -1493,94 +1600,98 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
     cudaGetDevice(&device);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const unsigned box_blocks = (unsigned)sms * 4;
+    cudaError_t e = cudaSuccess;
     if ((phases & BK_PHASE_TRANSPORT) && p.transport) {
         if (surface->vertex_count > 0) {
             {
                 int rec = profile_begin("surface_vertices", s);
                 const unsigned nv = (unsigned)surface->vertex_count;
                 switch (vertex_block_threads(surface->vertex_count, surface->binding_count)) {
-                    case 256: k_surface_vertices<256><<<nv, 256, 0, s>>>(P, in->x, in->F, *surface); break;
-                    case 128: k_surface_vertices<128><<<nv, 128, 0, s>>>(P, in->x, in->F, *surface); break;
+                    case 256: e = launch_chained(k_surface_vertices<256>, nv, 256, 0, s, P, in->x, in->F, *surface); break;
+                    case 128: e = launch_chained(k_surface_vertices<128>, nv, 128, 0, s, P, in->x, in->F, *surface); break;
                     default:
-                        k_surface_vertices<32><<<vertex_launch_blocks(nv, 32), vertex_launch_threads(32), 0, s>>>(
-                            P, in->x, in->F, *surface);
+                        e = launch_chained(k_surface_vertices<32>, vertex_launch_blocks(nv, 32), vertex_launch_threads(32),
+                                           0, s, P, in->x, in->F, *surface);
                         break;
                 }
                 profile_end(rec, s);
             }
-            if (int rc = check_launch("bk_substep/surface_vertices")) return rc;
+            if (int rc = check_chained(e, "bk_substep/surface_vertices")) return rc;
         }
         if (surface->owner_count > 0) {
             {
                 int rec = profile_begin("surface_owners", s);
-                k_surface_owners<<<owner_blocks(surface->owner_count, p.n), kOwnerThreads, 0, s>>>(
-                    P, *in, *constants, *surface, g, flags->simulation, owners_tiled(surface->owner_count, p.n));
+                e = launch_chained(k_surface_owners, owner_blocks(surface->owner_count, p.n), kOwnerThreads, 0, s, P,
+                                   *in, *constants, *surface, g, flags->simulation,
+                                   (int)owners_tiled(surface->owner_count, p.n));
                 profile_end(rec, s);
             }
-            if (int rc = check_launch("bk_substep/surface_owners")) return rc;
+            if (int rc = check_chained(e, "bk_substep/surface_owners")) return rc;
         }
         if (!p.transport_prescattered) {
             if (p.transport_prescatter_stale) {
-                k_clear_prescatter<<<box_blocks, kThreads, 0, s>>>(P, g);
-                if (int rc = check_launch("bk_substep/clear_prescatter")) return rc;
+                e = launch_chained(k_clear_prescatter, box_blocks, kThreads, 0, s, P, g);
+                if (int rc = check_chained(e, "bk_substep/clear_prescatter")) return rc;
             }
             {
                 int rec = profile_begin("transport_scatter", s);
-                k_transport_scatter<<<particle_blocks, kThreads, 0, s>>>(P, *in, *constants, g, flags->simulation);
+                e = launch_chained(k_transport_scatter, particle_blocks, kThreads, 0, s, P, *in, *constants, g,
+                                   flags->simulation);
                 profile_end(rec, s);
             }
-            if (int rc = check_launch("bk_substep/transport_scatter")) return rc;
+            if (int rc = check_chained(e, "bk_substep/transport_scatter")) return rc;
         }
         {
             int rec = profile_begin("diffuse", s);
-            k_diffuse<<<box_blocks, kDiffThreads, 0, s>>>(P, g, flags->transport);
+            e = launch_chained(k_diffuse, box_blocks, kDiffThreads, 0, s, P, g, flags->transport);
             profile_end(rec, s);
         }
-        if (int rc = check_launch("bk_substep/diffuse")) return rc;
+        if (int rc = check_chained(e, "bk_substep/diffuse")) return rc;
     }
     if (phases & BK_PHASE_MECHANICS) {
         {
             int rec = profile_begin("clear_previous", s);
-            k_clear_previous<<<box_blocks, kThreads, 0, s>>>(P, g);
+            e = launch_chained(k_clear_previous, box_blocks, kThreads, 0, s, P, g);
             profile_end(rec, s);
         }
-        if (int rc = check_launch("bk_substep/clear_previous")) return rc;
+        if (int rc = check_chained(e, "bk_substep/clear_previous")) return rc;
         {
             int rec = profile_begin("p2g", s);
             // Bulk staging needs 16-byte aligned plane starts: a pitch that is a multiple of 4 floats
             // and 16-byte aligned array bases.
             const uintptr_t bases = (uintptr_t)in->x | (uintptr_t)in->v | (uintptr_t)in->C | (uintptr_t)in->F |
                                     (p.material == 1 ? (uintptr_t)in->tau : 0);
-            if (p.pitch % 4 == 0 && (bases & 15) == 0)
-                k_p2g<true><<<particle_blocks, kThreads, 0, s>>>(P, *in, *out, *constants, g, *flags,
-                                                                 diagnostics->max_residuals);
-            else
-                k_p2g<false><<<particle_blocks, kThreads, 0, s>>>(P, *in, *out, *constants, g, *flags,
-                                                                  diagnostics->max_residuals);
+            const bool staged = p.pitch % 4 == 0 && (bases & 15) == 0;
+            if (int rc = allow_smem(staged ? (const void*)k_p2g<true> : (const void*)k_p2g<false>, kP2GSmemBytes,
+                                    "bk_substep/p2g"))
+                return rc;
+            e = launch_chained(staged ? k_p2g<true> : k_p2g<false>, particle_blocks, kThreads, kP2GSmemBytes, s, P,
+                               *in, *out, *constants, g, *flags, diagnostics->max_residuals);
             profile_end(rec, s);
         }
-        if (int rc = check_launch("bk_substep/p2g")) return rc;
+        if (int rc = check_chained(e, "bk_substep/p2g")) return rc;
         {
             int rec = profile_begin("grid_update", s);
-            k_grid_update<<<box_blocks, kThreads, 0, s>>>(P, g);
+            e = launch_chained(k_grid_update, box_blocks, kThreads, 0, s, P, g);
             profile_end(rec, s);
         }
-        if (int rc = check_launch("bk_substep/grid_update")) return rc;
+        if (int rc = check_chained(e, "bk_substep/grid_update")) return rc;
         const SurrogateDev sg = surrogate_dev(p.surrogate);
         if (sg.blob && p.material == 1) {
             int rec = profile_begin("g2p_return_surrogate", s);
             const unsigned tiles = blocks_for(p.n, 128);
             const unsigned persistent = (unsigned)sms * 4;
-            k_g2p_return_surrogate<<<tiles < persistent ? tiles : persistent, 128, 0, s>>>(
-                P, *in, *out, *constants, g, *diagnostics, *flags, sg);
+            e = launch_chained(k_g2p_return_surrogate, tiles < persistent ? tiles : persistent, 128, 0, s, P, *in,
+                               *out, *constants, g, *diagnostics, *flags, sg);
             profile_end(rec, s);
         } else {
             int rec = profile_begin("g2p_return", s);
             const size_t smem = p.transport_prescatter_next ? sizeof(G2PTransportTile) : 0;
-            k_g2p_return<<<blocks_for(p.n, 128), 128, smem, s>>>(P, *in, *out, *constants, g, *diagnostics, *flags, sg);
+            e = launch_chained(k_g2p_return, blocks_for(p.n, 128), 128, smem, s, P, *in, *out, *constants, g,
+                               *diagnostics, *flags, sg);
             profile_end(rec, s);
         }
-        if (int rc = check_launch("bk_substep/g2p_return")) return rc;
+        if (int rc = check_chained(e, "bk_substep/g2p_return")) return rc;
     }
     return BK_OK;
 }
@@ -1925,8 +2036,11 @@ int bk_batch_substep(BkBatch* batch, int32_t parity, int32_t phases, int32_t pre
         }
         if (T[kStP2G]) {
             int rec = profile_begin("batch_p2g", s);
-            if (B.staged) kb_p2g<true><<<T[kStP2G], kThreads, 0, s>>>(a);
-            else kb_p2g<false><<<T[kStP2G], kThreads, 0, s>>>(a);
+            if (int rc = allow_smem(B.staged ? (const void*)kb_p2g<true> : (const void*)kb_p2g<false>,
+                                    kP2GSmemBytes, "bk_batch_substep/p2g"))
+                return rc;
+            if (B.staged) kb_p2g<true><<<T[kStP2G], kThreads, kP2GSmemBytes, s>>>(a);
+            else kb_p2g<false><<<T[kStP2G], kThreads, kP2GSmemBytes, s>>>(a);
             profile_end(rec, s);
             if (int rc = check_launch("bk_batch_substep/p2g")) return rc;
         }
