@@ -462,14 +462,29 @@ __device__ void transport_scatter_block(TransportTile<kT, kTile, kF, kNodeWeight
         int e = starts ? __ffs(starts) - 1 : 32;
         int b0 = __shfl_sync(kFull, st.b[0], s), b1 = __shfl_sync(kFull, st.b[1], s), b2 = __shfl_sync(kFull, st.b[2], s);
         if (lane < 27) {
-            double acc[kF];
+            // Even and odd particles of the run into separate sums: two independent chains of
+            // float64 multiply-adds per field, so consecutive particles' loads and conversions overlap.
+            double acc[kF], acc_odd[kF];
 #pragma unroll
-            for (int f = 0; f < kF; ++f) acc[f] = 0.0;
-            for (int k = warp_base + s; k < warp_base + e; ++k) {
-                const double w = (double)sm.w.get(k, lane, ox, oy, oz);
+            for (int f = 0; f < kF; ++f) acc[f] = acc_odd[f] = 0.0;
+            int k = warp_base + s;
+            const int k_end = warp_base + e;
+            for (; k + 1 < k_end; k += 2) {
+                const double w0 = (double)sm.w.get(k, lane, ox, oy, oz);
+                const double w1 = (double)sm.w.get(k + 1, lane, ox, oy, oz);
 #pragma unroll
-                for (int f = 0; f < kF; ++f) acc[f] += w * sm.val[k][f];
+                for (int f = 0; f < kF; ++f) {
+                    acc[f] = fma(w0, sm.val[k][f], acc[f]);
+                    acc_odd[f] = fma(w1, sm.val[k + 1][f], acc_odd[f]);
+                }
             }
+            if (k < k_end) {
+                const double w0 = (double)sm.w.get(k, lane, ox, oy, oz);
+#pragma unroll
+                for (int f = 0; f < kF; ++f) acc[f] = fma(w0, sm.val[k][f], acc[f]);
+            }
+#pragma unroll
+            for (int f = 0; f < kF; ++f) acc[f] += acc_odd[f];
             if (bb.tiled) {
                 int t = tile_index(bb, b0 + ox, b1 + oy, b2 + oz);
 #pragma unroll
