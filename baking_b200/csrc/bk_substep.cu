@@ -821,10 +821,17 @@ __global__ void k_grid_update(Params P, GridPtrs g) {
 // copy) issued by one thread and counted on an mbarrier, so the loads of a block are in flight
 // together and each thread then reads its particle's 33 values from shared memory; the scatter
 // records reuse that space once every thread has read it.
+// A full block (256 particles) also stages its per-particle scalars: temperature, water, dry mass
+// and gas content (float64), reference volume, gas source rate and porosity (float32), those the
+// substep reads; the last, partial block loads them directly (the arrays need not extend past n).
 constexpr int kP2GPlanes = 33;
 struct P2GSmem {
     union {
-        float planes[kP2GPlanes][kThreads];  // x 0-2, v 3-5, C 6-14, F 15-23, tau 24-32
+        struct {
+            float planes[kP2GPlanes][kThreads];  // x 0-2, v 3-5, C 6-14, F 15-23, tau 24-32
+            double d[4][kThreads];               // temperature, water, dry mass, gas moles
+            float f[3][kThreads];                // reference volume, gas source rate, porosity
+        } in;
         struct {
             float4 val[kThreads][3];
             float a8[kThreads];
@@ -837,6 +844,30 @@ struct P2GSmem {
 // Above the 48 KB of static shared memory: the kernels take it as dynamic shared memory, opted in
 // per device before their first launch there.
 constexpr size_t kP2GSmemBytes = sizeof(P2GSmem);
+
+// Which per-particle scalars a full P2G block stages (bit k of d[k], bit 4 + k of f[k]).
+__host__ __device__ inline unsigned p2g_staged_scalars(int transport, int gas, int material, int rate_per_particle) {
+    unsigned m = 0;
+    if (transport) m |= 1u | 2u | 4u | 16u;
+    if (transport && gas) m |= 8u | (rate_per_particle ? 32u : 0u);
+    if (material == 1 && gas) m |= 64u;
+    return m;
+}
+
+// OR of the base addresses the bulk-staged P2G copies from (each must be 16-byte aligned).
+inline uintptr_t p2g_stage_bases(const BkSubstepParams& p, const BkState& in, const BkConstants& c) {
+    uintptr_t b = (uintptr_t)in.x | (uintptr_t)in.v | (uintptr_t)in.C | (uintptr_t)in.F |
+                  (p.material == 1 ? (uintptr_t)in.tau : 0);
+    const unsigned m = p2g_staged_scalars(p.transport, p.gas, p.material, c.gas_rate_per_particle);
+    if (m & 1u) b |= (uintptr_t)in.temperature;
+    if (m & 2u) b |= (uintptr_t)in.water;
+    if (m & 4u) b |= (uintptr_t)c.dry_mass;
+    if (m & 8u) b |= (uintptr_t)in.gas_moles;
+    if (m & 16u) b |= (uintptr_t)c.volume;
+    if (m & 32u) b |= (uintptr_t)c.gas_rate;
+    if (m & 64u) b |= (uintptr_t)in.porosity;
+    return b;
+}
 
 // Opts `kernel` into `bytes` of dynamic shared memory on the current device. Set on every launch:
 // a host call without device work, and correct after a device reset or in another context.
@@ -874,6 +905,11 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t i = sl.block * (int64_t)kThreads + tid;
     const int64_t pitch = P.pitch;
+    // Scalars this block reads from shared memory (full blocks of the staged form), by bit as in
+    // p2g_staged_scalars; the others are loaded directly.
+    const unsigned staged_scalars =
+        kStaged && P.n - (int64_t)sl.block * kThreads >= kThreads
+            ? p2g_staged_scalars(P.transport, P.gas, P.material, cst.gas_rate_per_particle) : 0u;
     if constexpr (kStaged) {
         // Planes are pitch-long with a pitch that is a multiple of 4 and 16-byte aligned bases (the
         // host checks), so the block's range rounded up to 16 bytes stays inside each plane.
@@ -887,11 +923,22 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
             const int arrays = P.material == 1 ? 5 : 4;
             const float* src[5] = {in.x, in.v, in.C, in.F, in.tau};
             const int planes[5] = {3, 3, 9, 9, 9};
-            stage::arrive_expect_tx(mbar, bytes * (uint32_t)(P.material == 1 ? kP2GPlanes : kP2GPlanes - 9));
+            const unsigned m = count == kThreads ? staged_scalars : 0u;
+            uint32_t total = bytes * (uint32_t)(P.material == 1 ? kP2GPlanes : kP2GPlanes - 9);
+#pragma unroll
+            for (int k = 0; k < 7; ++k)
+                if (m & (1u << k)) total += k < 4 ? kThreads * 8 : kThreads * 4;
+            stage::arrive_expect_tx(mbar, total);
             int k = 0;
             for (int a = 0; a < arrays; ++a)
                 for (int c = 0; c < planes[a]; ++c, ++k)
-                    stage::copy(mlp::smem_addr(&sm.planes[k][0]), src[a] + c * pitch + start, bytes, mbar);
+                    stage::copy(mlp::smem_addr(&sm.in.planes[k][0]), src[a] + c * pitch + start, bytes, mbar);
+            const double* dsrc[4] = {in.temperature, in.water, cst.dry_mass, in.gas_moles};
+            const float* fsrc[3] = {cst.volume, cst.gas_rate, in.porosity};
+            for (int k = 0; k < 4; ++k)
+                if (m & (1u << k)) stage::copy(mlp::smem_addr(&sm.in.d[k][0]), dsrc[k] + start, kThreads * 8, mbar);
+            for (int k = 0; k < 3; ++k)
+                if (m & (16u << k)) stage::copy(mlp::smem_addr(&sm.in.f[k][0]), fsrc[k] + start, kThreads * 4, mbar);
         }
         const bool arrived = __syncthreads_and(mlp::mbar_wait(mbar, 0, stage::kWaitPolls)) != 0;
         if (!arrived) {
@@ -904,14 +951,14 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
     }
     // This particle's plane arrays: from the staged copies or from global memory.
     auto ld_v3 = [&](const float* src, int plane0) {
-        if constexpr (kStaged) return V3{{sm.planes[plane0][tid], sm.planes[plane0 + 1][tid], sm.planes[plane0 + 2][tid]}};
+        if constexpr (kStaged) return V3{{sm.in.planes[plane0][tid], sm.in.planes[plane0 + 1][tid], sm.in.planes[plane0 + 2][tid]}};
         else return load_v3(src, i, pitch);
     };
     auto ld_m3 = [&](const float* src, int plane0) {
         if constexpr (kStaged) {
             M3 r;
 #pragma unroll
-            for (int c = 0; c < 9; ++c) r.m[c] = sm.planes[plane0 + c][tid];
+            for (int c = 0; c < 9; ++c) r.m[c] = sm.in.planes[plane0 + c][tid];
             return r;
         } else {
             return load_m3(src, i, pitch);
@@ -947,11 +994,11 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
                         dTp += w * d.x;
                         ratio += w * d.y;
                     }
-            double T_old = in.temperature[i];
+            double T_old = (staged_scalars & 1u) ? sm.in.d[0][tid] : in.temperature[i];
             double Tn = T_old + dTp;
-            double Wn = in.water[i] * (1.0 + ratio);
-            double dry = cst.dry_mass[i];
-            float V0 = cst.volume[i];
+            double Wn = ((staged_scalars & 2u) ? sm.in.d[1][tid] : in.water[i]) * (1.0 + ratio);
+            double dry = (staged_scalars & 4u) ? sm.in.d[2][tid] : cst.dry_mass[i];
+            float V0 = (staged_scalars & 16u) ? sm.in.f[0][tid] : cst.volume[i];
             out.temperature[i] = Tn;
             out.water[i] = Wn;
             mass = (float)(dry + Wn);
@@ -959,12 +1006,13 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
             sat = Wn / ((double)P.water_density * (double)V0 * (double)J);
             T_mat = (float)Tn;
             if (P.gas) {
-                double N = in.gas_moles[i];
+                double N = (staged_scalars & 8u) ? sm.in.d[3][tid] : in.gas_moles[i];
                 if (!P.settling) {
                     double Tm = 0.5 * (T_old + Tn);
                     double z = (Tm - (double)P.peak) / (double)P.width;
-                    N += (double)(P.dt * P.density) * (double)cst.gas_rate[cst.gas_rate_per_particle ? i : 0] *
-                         exp(-(z * z));
+                    const float rate = (staged_scalars & 32u) ? sm.in.f[1][tid]
+                                                              : cst.gas_rate[cst.gas_rate_per_particle ? i : 0];
+                    N += (double)(P.dt * P.density) * (double)rate * exp(-(z * z));
                 }
                 out.gas_moles[i] = N;
             }
@@ -975,7 +1023,7 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
         if (P.material == 1) {
             tau = ld_m3(in.tau, 24);
             if (P.gas) {
-                float n = in.porosity[i];
+                float n = (staged_scalars & 64u) ? sm.in.f[2][tid] : in.porosity[i];
                 if (n <= 0.0f || n >= 1.0f || !isfinite(n) || J <= 0.0f) {
                     set_flag(flags.ding, 0);
                 } else {
@@ -1010,7 +1058,7 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
 #pragma unroll
             for (int e = 0; e < 9; ++e) tau.m[e] -= (e % 4) == 0 ? iso : iso * 0.0f;
         }
-        float scale = P.dt * cst.volume[i] * 4.0f / (P.dx * P.dx);
+        float scale = P.dt * ((staged_scalars & 16u) ? sm.in.f[0][tid] : cst.volume[i]) * 4.0f / (P.dx * P.dx);
         M3 Cm = ld_m3(in.C, 6);
         V3 vel = ld_v3(in.v, 3);
 #pragma unroll
@@ -1674,9 +1722,7 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
             int rec = profile_begin("p2g", s);
             // Bulk staging needs 16-byte aligned plane starts: a pitch that is a multiple of 4 floats
             // and 16-byte aligned array bases.
-            const uintptr_t bases = (uintptr_t)in->x | (uintptr_t)in->v | (uintptr_t)in->C | (uintptr_t)in->F |
-                                    (p.material == 1 ? (uintptr_t)in->tau : 0);
-            const bool staged = p.pitch % 4 == 0 && (bases & 15) == 0;
+            const bool staged = p.pitch % 4 == 0 && (p2g_stage_bases(p, *in, *constants) & 15) == 0;
             if (int rc = allow_smem(staged ? (const void*)k_p2g<true> : (const void*)k_p2g<false>, kP2GSmemBytes,
                                     "bk_substep/p2g"))
                 return rc;
@@ -1930,9 +1976,7 @@ int bk_batch_create(const BkBatchInstance* instances, int32_t count, BkBatch** b
             e.sg = surrogate_dev(surrogate ? p.surrogate : nullptr);
             e.prescatter_ok = p.transport && !p.keep_transport_fields && !surrogate;
             e.owners_tiled = owners_tiled(in.surface.owner_count, p.n);
-            const uintptr_t bases = (uintptr_t)a.x | (uintptr_t)a.v | (uintptr_t)a.C | (uintptr_t)a.F |
-                                    (p.material == 1 ? (uintptr_t)a.tau : 0);
-            host.staged = host.staged && p.pitch % 4 == 0 && (bases & 15) == 0;
+            host.staged = host.staged && p.pitch % 4 == 0 && (p2g_stage_bases(p, a, in.constants) & 15) == 0;
         }
         host.any_transport = host.any_transport || p.transport;
         if (p.transport && (p.keep_transport_fields || surrogate)) host.all_prescatter = false;
