@@ -96,6 +96,23 @@ Params to_params(const BkSubstepParams& p) {
     return k;
 }
 
+// The configuration of the loaf and dough bodies: Ding with temperature-dependent parameters, gas
+// with the coupled porosity solve, thermal-water transport, no per-particle diagnostics and no
+// harvest. The particle kernels have an instance for it in which these flags are compile-time
+// constants, so the branches of the other configurations fold away (same arithmetic, less code).
+bool loaf_mode(const BkSubstepParams& p, const BkDiagnostics& d) {
+    return p.material == 1 && p.transport && p.gas && p.ding.coupled_porosity && p.ding.temperature_enabled &&
+           !d.plastic_gradients && !d.return_residuals && !d.porosity_residuals &&
+           !(p.surrogate && p.surrogate->samples);
+}
+__device__ __forceinline__ void fix_loaf_mode(Params& P) {
+    P.material = 1;
+    P.transport = 1;
+    P.gas = 1;
+    P.ding.coupled_porosity = 1;
+    P.ding.temperature_enabled = 1;
+}
+
 struct GridPtrs {
     float4* pm;
     float4* v;
@@ -1147,10 +1164,11 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
     }
 }
 
-template <bool kStaged>
+template <bool kStaged, bool kLoaf = false>
 __global__ void __launch_bounds__(kThreads, 4) k_p2g(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
                                                  BkFlags flags, float* max_residuals) {
     pdl_enter();
+    if constexpr (kLoaf) fix_loaf_mode(P);
     p2g_body<kStaged>(P, in, out, cst, g, flags, max_residuals, grid_slot());
 }
 
@@ -1449,9 +1467,15 @@ __device__ __forceinline__ void g2p_return_body(Arg<Params, kRef> P, Arg<BkState
     }
 }
 
+template <bool kLoaf = false>
 __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
                                                    BkDiagnostics diag, BkFlags flags, SurrogateDev sg) {
     pdl_enter();
+    if constexpr (kLoaf) {
+        fix_loaf_mode(P);
+        diag.plastic_gradients = diag.return_residuals = diag.porosity_residuals = nullptr;
+        sg.samples = nullptr;
+    }
     g2p_return_body(P, in, out, cst, g, diag, flags, sg, grid_slot());
 }
 
@@ -1723,11 +1747,14 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
             // Bulk staging needs 16-byte aligned plane starts: a pitch that is a multiple of 4 floats
             // and 16-byte aligned array bases.
             const bool staged = p.pitch % 4 == 0 && (p2g_stage_bases(p, *in, *constants) & 15) == 0;
-            if (int rc = allow_smem(staged ? (const void*)k_p2g<true> : (const void*)k_p2g<false>, kP2GSmemBytes,
-                                    "bk_substep/p2g"))
+            if (int rc = allow_smem(staged ? (loaf_mode(p, *diagnostics) ? (const void*)k_p2g<true, true> : (const void*)k_p2g<true>)
+                                           : (loaf_mode(p, *diagnostics) ? (const void*)k_p2g<false, true> : (const void*)k_p2g<false>),
+                                    kP2GSmemBytes, "bk_substep/p2g"))
                 return rc;
-            e = launch_chained(staged ? k_p2g<true> : k_p2g<false>, particle_blocks, kThreads, kP2GSmemBytes, s, P,
-                               *in, *out, *constants, g, *flags, diagnostics->max_residuals);
+            const bool loaf = loaf_mode(p, *diagnostics);
+            auto* kernel = staged ? (loaf ? k_p2g<true, true> : k_p2g<true>) : (loaf ? k_p2g<false, true> : k_p2g<false>);
+            e = launch_chained(kernel, particle_blocks, kThreads, kP2GSmemBytes, s, P, *in, *out, *constants, g, *flags,
+                               diagnostics->max_residuals);
             profile_end(rec, s);
         }
         if (int rc = check_chained(e, "bk_substep/p2g")) return rc;
@@ -1748,8 +1775,8 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
         } else {
             int rec = profile_begin("g2p_return", s);
             const size_t smem = p.transport_prescatter_next ? sizeof(G2PTransportTile) : 0;
-            e = launch_chained(k_g2p_return, blocks_for(p.n, 128), 128, smem, s, P, *in, *out, *constants, g,
-                               *diagnostics, *flags, sg);
+            e = launch_chained(loaf_mode(p, *diagnostics) ? k_g2p_return<true> : k_g2p_return<false>,
+                               blocks_for(p.n, 128), 128, smem, s, P, *in, *out, *constants, g, *diagnostics, *flags, sg);
             profile_end(rec, s);
         }
         if (int rc = check_chained(e, "bk_substep/g2p_return")) return rc;
