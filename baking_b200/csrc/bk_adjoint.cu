@@ -47,6 +47,17 @@ struct AdjParams {
     DingParamsDev ding;
 };
 
+// The loaf and dough configuration (Ding with temperature-dependent parameters, thermal-water
+// transport): kernel instances for it take these flags as compile-time constants.
+__device__ __forceinline__ void fix_loaf_mode(AdjParams& P) {
+    P.material = 1;
+    P.transport = 1;
+    P.ding.temperature_enabled = 1;
+}
+bool adj_loaf_mode(const BkSubstepParams& p) {
+    return p.material == 1 && p.transport && p.ding.temperature_enabled;
+}
+
 // Adjoint of a particle state: same planes as BkState.
 struct AdjState {
     float *x, *v, *C, *F, *Fe, *tau, *porosity, *temperature, *mass;
@@ -368,10 +379,12 @@ __device__ __forceinline__ float qweight_grad(float l, int o) {
 // ------------------------------------------------------------ G2P + return
 // params_adj: float64 [0] mu, [1] lambda, [2] viscosity parameter.
 // kCoupled: gas mode's coupled porosity (a separate instance, so the other modes keep their registers).
-template <bool kCoupled>
+// kLoaf: the loaf configuration (Ding with temperature, transport) as compile-time constants.
+template <bool kCoupled, bool kLoaf = false>
 __global__ void __launch_bounds__(kThreads, 4) k_adj_g2p_return(AdjParams P, BkState in, const float4* __restrict__ grid_v,
                                                           const float* __restrict__ eta_param, AdjState out_adj,
                                                           AdjState in_adj, double* __restrict__ params_adj) {
+    if constexpr (kLoaf) fix_loaf_mode(P);
     const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
     float acc_mu = 0.f, acc_lam = 0.f, acc_eta = 0.f;
     if (i < P.n) {
@@ -667,9 +680,11 @@ struct ScatterSmem {
     int box[6];
 };
 
+template <bool kLoaf = false>
 __global__ void __launch_bounds__(kThreads) k_adj_g2p_scatter(AdjParams P, BkState in, const float4* __restrict__ grid_v,
                                                             AdjState out_adj, AdjState in_adj,
                                                             float4* __restrict__ grid_v_adj) {
+    if constexpr (kLoaf) fix_loaf_mode(P);
     __shared__ ScatterSmem sm;
     const int tid = threadIdx.x, lane = tid & 31;
     const int64_t i = blockIdx.x * (int64_t)kThreads + tid;
@@ -882,9 +897,11 @@ __global__ void k_adj_grid_box(AdjParams P, const int32_t* __restrict__ box, con
 
 // ---------------------------------------------------------------- P2G
 // tau is the Ding state stress, or the neo-Hookean stress of F.
+template <bool kLoaf = false>
 __global__ void __launch_bounds__(kThreads) k_adj_p2g(AdjParams P, BkState in, const float* __restrict__ mass,
                                                    const float* __restrict__ volume, const float4* __restrict__ pm_adj,
                                                    AdjState in_adj, double* __restrict__ params_adj) {
+    if constexpr (kLoaf) fix_loaf_mode(P);
     const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
     float acc_mu = 0.f, acc_lam = 0.f;
     if (i < P.n) {
@@ -1073,18 +1090,17 @@ int bk_substep_adjoint(const BkSubstepParams* params, const BkState* in, const B
     const int64_t nodes = (int64_t)p.resolution * p.resolution * p.resolution;
     if (!node_box) cudaMemsetAsync(node_v_adjoint, 0, nodes * sizeof(float4), s);
     unsigned blocks = (unsigned)((p.n + kThreads - 1) / kThreads);
-    if (p.material == 1 && p.ding.coupled_porosity)
-        k_adj_g2p_return<true><<<blocks, kThreads, 0, s>>>(a, *in, reinterpret_cast<const float4*>(node_v),
-                                                         constants->viscosity_parameter, adj_state(*out_adjoint),
-                                                         adj_state(*in_adjoint), parameter_adjoint);
-    else
-        k_adj_g2p_return<false><<<blocks, kThreads, 0, s>>>(a, *in, reinterpret_cast<const float4*>(node_v),
-                                                          constants->viscosity_parameter, adj_state(*out_adjoint),
-                                                          adj_state(*in_adjoint), parameter_adjoint);
+    const bool loaf = adj_loaf_mode(p);
+    const bool coupled = p.material == 1 && p.ding.coupled_porosity;
+    auto* g2p_return = coupled ? (loaf ? k_adj_g2p_return<true, true> : k_adj_g2p_return<true>)
+                               : (loaf ? k_adj_g2p_return<false, true> : k_adj_g2p_return<false>);
+    g2p_return<<<blocks, kThreads, 0, s>>>(a, *in, reinterpret_cast<const float4*>(node_v),
+                                           constants->viscosity_parameter, adj_state(*out_adjoint),
+                                           adj_state(*in_adjoint), parameter_adjoint);
     if (int rc = bk::check_launch("bk_substep_adjoint/g2p_return")) return rc;
-    k_adj_g2p_scatter<<<blocks, kThreads, 0, s>>>(a, *in, reinterpret_cast<const float4*>(node_v),
-                                                  adj_state(*out_adjoint), adj_state(*in_adjoint),
-                                                  reinterpret_cast<float4*>(node_v_adjoint));
+    (loaf ? k_adj_g2p_scatter<true> : k_adj_g2p_scatter<false>)<<<blocks, kThreads, 0, s>>>(
+        a, *in, reinterpret_cast<const float4*>(node_v), adj_state(*out_adjoint), adj_state(*in_adjoint),
+        reinterpret_cast<float4*>(node_v_adjoint));
     if (int rc = bk::check_launch("bk_substep_adjoint/g2p_scatter")) return rc;
     if (node_box) {
         int device = 0, sms = 148;
@@ -1099,7 +1115,7 @@ int bk_substep_adjoint(const BkSubstepParams* params, const BkState* in, const B
                                                                   reinterpret_cast<float4*>(node_pm_adjoint), nodes);
     }
     if (int rc = bk::check_launch("bk_substep_adjoint/grid")) return rc;
-    k_adj_p2g<<<blocks, kThreads, 0, s>>>(a, *in, constants->mass, constants->volume,
+    (loaf ? k_adj_p2g<true> : k_adj_p2g<false>)<<<blocks, kThreads, 0, s>>>(a, *in, constants->mass, constants->volume,
                                           reinterpret_cast<const float4*>(node_pm_adjoint), adj_state(*in_adjoint),
                                           parameter_adjoint);
     return bk::check_launch("bk_substep_adjoint/p2g");

@@ -1467,12 +1467,14 @@ __device__ __forceinline__ void g2p_return_body(Arg<Params, kRef> P, Arg<BkState
     }
 }
 
-template <bool kLoaf = false>
+// kLoaf instances also fix whether the next substep's transport fields are scattered (kPrescatter).
+template <bool kLoaf = false, bool kPrescatter = false>
 __global__ void __launch_bounds__(128, 8) k_g2p_return(Params P, BkState in, BkState out, BkConstants cst, GridPtrs g,
                                                    BkDiagnostics diag, BkFlags flags, SurrogateDev sg) {
     pdl_enter();
     if constexpr (kLoaf) {
         fix_loaf_mode(P);
+        P.prescatter_next = kPrescatter;
         diag.plastic_gradients = diag.return_residuals = diag.porosity_residuals = nullptr;
         sg.samples = nullptr;
     }
@@ -1569,10 +1571,16 @@ __device__ __forceinline__ void g2p_return_surrogate_body(Arg<Params, kRef> P, A
     if (sg.path_counts && threadIdx.x < 3 && s_counts[threadIdx.x]) atomicAdd(sg.path_counts + threadIdx.x, s_counts[threadIdx.x]);
 }
 
+template <bool kLoaf = false>
 __global__ void __launch_bounds__(128, 4) k_g2p_return_surrogate(Params P, BkState in, BkState out, BkConstants cst,
                                                              GridPtrs g, BkDiagnostics diag, BkFlags flags,
                                                              SurrogateDev sg) {
     pdl_enter();
+    if constexpr (kLoaf) {
+        fix_loaf_mode(P);
+        diag.plastic_gradients = diag.return_residuals = diag.porosity_residuals = nullptr;
+        sg.samples = nullptr;
+    }
     g2p_return_surrogate_body(P, in, out, cst, g, diag, flags, sg, grid_slot());
 }
 
@@ -1769,14 +1777,18 @@ int bk_substep(const BkSubstepParams* params, const BkState* in, BkState* out, c
             int rec = profile_begin("g2p_return_surrogate", s);
             const unsigned tiles = blocks_for(p.n, 128);
             const unsigned persistent = (unsigned)sms * 4;
-            e = launch_chained(k_g2p_return_surrogate, tiles < persistent ? tiles : persistent, 128, 0, s, P, *in,
-                               *out, *constants, g, *diagnostics, *flags, sg);
+            e = launch_chained(loaf_mode(p, *diagnostics) ? k_g2p_return_surrogate<true> : k_g2p_return_surrogate<false>,
+                               tiles < persistent ? tiles : persistent, 128, 0, s, P, *in, *out, *constants, g,
+                               *diagnostics, *flags, sg);
             profile_end(rec, s);
         } else {
             int rec = profile_begin("g2p_return", s);
             const size_t smem = p.transport_prescatter_next ? sizeof(G2PTransportTile) : 0;
-            e = launch_chained(loaf_mode(p, *diagnostics) ? k_g2p_return<true> : k_g2p_return<false>,
-                               blocks_for(p.n, 128), 128, smem, s, P, *in, *out, *constants, g, *diagnostics, *flags, sg);
+            auto* kernel = !loaf_mode(p, *diagnostics)       ? k_g2p_return<false>
+                           : p.transport_prescatter_next ? k_g2p_return<true, true>
+                                                         : k_g2p_return<true, false>;
+            e = launch_chained(kernel, blocks_for(p.n, 128), 128, smem, s, P, *in, *out, *constants, g, *diagnostics,
+                               *flags, sg);
             profile_end(rec, s);
         }
         if (int rc = check_chained(e, "bk_substep/g2p_return")) return rc;
