@@ -206,7 +206,10 @@ class _MappedDoubles:
 
     def __del__(self):
         if getattr(self, "_host_ptr", None):
-            self._cudart.cudaFreeHost(self._host_ptr)
+            try:
+                self._cudart.cudaFreeHost(self._host_ptr)
+            except (TypeError, AttributeError):
+                pass  # interpreter shutdown: the runtime bindings are already torn down
             self._host_ptr = None
 
 

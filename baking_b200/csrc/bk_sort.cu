@@ -8,6 +8,7 @@
 // the largest key) and a stable least-significant-digit radix sort over 3 x ceil(log2 R) key bits
 // (CUB's DeviceRadixSort::SortPairs), particle index as the value: particles of one cell keep
 // their relative order.
+#include <algorithm>
 #include <cstdint>
 #include <cub/device/device_radix_sort.cuh>
 
@@ -73,15 +74,42 @@ size_t cub_bytes(int64_t n, int end_bit) {
     return bytes;
 }
 
-// scratch[p * n + k] = data[p * pitch + order[k]] over planes x n elements.
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_gather_planes(int64_t n, const int32_t* __restrict__ order,
-                                                            int64_t total, const T* __restrict__ data, int64_t pitch,
-                                                            T* __restrict__ scratch) {
-    const int64_t e = blockIdx.x * (int64_t)kThreads + threadIdx.x;
-    if (e >= total) return;
-    const int64_t p = e / n, k = e - p * n;
-    scratch[e] = data[p * pitch + order[k]];
+// A group of per-particle arrays permuted together: each array's planes gathered into its slice of
+// the scratch buffer (element k of plane p <- element order[k]), then copied back in order. One
+// launch per pass for the whole group; block row y is the array, block column x a range of
+// particles, each thread one particle and every plane of the array (order[k] read once).
+constexpr int kPermuteGroupMax = 64;
+struct PermuteEntry {
+    void* data;
+    int64_t pitch;
+    int64_t offset;  // bytes into the scratch buffer (256-byte aligned)
+    int32_t planes, bytes;
+};
+struct PermuteGroup {
+    PermuteEntry e[kPermuteGroupMax];
+};
+
+template <bool kBack, class T>
+__device__ __forceinline__ void permute_planes(int64_t n, int64_t k, int64_t src, const PermuteEntry& E,
+                                               unsigned char* scratch) {
+    T* d = static_cast<T*>(E.data);
+    T* sc = reinterpret_cast<T*>(scratch + E.offset);
+    for (int p = 0; p < E.planes; ++p) {
+        if constexpr (kBack) d[p * E.pitch + k] = sc[p * n + k];
+        else sc[p * n + k] = d[p * E.pitch + src];
+    }
+}
+
+template <bool kBack>
+__global__ void __launch_bounds__(kThreads) k_permute_group(int64_t n, const int32_t* __restrict__ order,
+                                                            const __grid_constant__ PermuteGroup g,
+                                                            unsigned char* __restrict__ scratch) {
+    const PermuteEntry& E = g.e[blockIdx.y];
+    for (int64_t k = blockIdx.x * (int64_t)kThreads + threadIdx.x; k < n; k += (int64_t)gridDim.x * kThreads) {
+        const int64_t src = kBack ? k : (int64_t)order[k];
+        if (E.bytes == 4) permute_planes<kBack, uint32_t>(n, k, src, E, scratch);
+        else permute_planes<kBack, uint64_t>(n, k, src, E, scratch);
+    }
 }
 
 }  // namespace
@@ -149,21 +177,29 @@ int bk_permute_particles(int64_t n, const int32_t* order, int32_t array_count, c
             return fail(BK_ERR_ARGUMENT, "bk_permute_particles: scratch smaller than the largest array");
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    for (int32_t a = 0; a < array_count; ++a) {
-        const BkParticleArray& arr = arrays[a];
-        const int64_t total = (int64_t)arr.planes * n;
-        const unsigned blocks = (unsigned)((total + kThreads - 1) / kThreads);
-        if (arr.element_bytes == 4)
-            k_gather_planes<uint32_t><<<blocks, kThreads, 0, s>>>(n, order, total, static_cast<const uint32_t*>(arr.data),
-                                                                  arr.pitch, static_cast<uint32_t*>(scratch));
-        else
-            k_gather_planes<uint64_t><<<blocks, kThreads, 0, s>>>(n, order, total, static_cast<const uint64_t*>(arr.data),
-                                                                  arr.pitch, static_cast<uint64_t*>(scratch));
+    unsigned char* base = static_cast<unsigned char*>(scratch);
+    const unsigned blocks = (unsigned)std::min<int64_t>((n + kThreads - 1) / kThreads, 2048);
+    // Groups of consecutive arrays whose slices (each rounded up to 256 bytes) fit the scratch
+    // buffer and the launch table; a group is gathered, then copied back, before the next starts.
+    int32_t a = 0;
+    while (a < array_count) {
+        PermuteGroup g;
+        int count = 0;
+        int64_t used = 0;
+        while (a < array_count && count < kPermuteGroupMax) {
+            const BkParticleArray& arr = arrays[a];
+            const int64_t bytes = ((int64_t)arr.planes * n * arr.element_bytes + 255) & ~(int64_t)255;
+            if (count > 0 && used + bytes > scratch_bytes) break;
+            g.e[count] = PermuteEntry{arr.data, arr.pitch, used, arr.planes, arr.element_bytes};
+            used += bytes;
+            ++count;
+            ++a;
+        }
+        const dim3 grid(blocks, (unsigned)count);
+        k_permute_group<false><<<grid, kThreads, 0, s>>>(n, order, g, base);
         if (int rc = check_launch("bk_permute_particles/gather")) return rc;
-        const size_t row = (size_t)n * arr.element_bytes;
-        cudaError_t e = cudaMemcpy2DAsync(arr.data, (size_t)arr.pitch * arr.element_bytes, scratch, row, row,
-                                          (size_t)arr.planes, cudaMemcpyDeviceToDevice, s);
-        if (e != cudaSuccess) return fail(BK_ERR_LAUNCH, cudaGetErrorString(e));
+        k_permute_group<true><<<grid, kThreads, 0, s>>>(n, order, g, base);
+        if (int rc = check_launch("bk_permute_particles/copy_back")) return rc;
     }
     return BK_OK;
 }

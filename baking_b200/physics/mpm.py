@@ -242,10 +242,11 @@ class MpmSimulator:
         return out
 
     def _permute_arrays(self, order):
-        """Every per-particle array in place through bk_permute_particles (one gather kernel and
-        one 2-D copy per array); arrays not in plane layout go through torch."""
+        """Every per-particle array in place through bk_permute_particles (arrays gathered in groups
+        that fit a scratch buffer of up to 256 MB, or the largest array, two launches per group);
+        arrays not in plane layout go through torch."""
         n = self.particle_data.particle_count
-        table, largest = [], 0
+        table, largest, total = [], 0, 0
         for t in self._particle_arrays():
             planes = t.numel() // n if n else 0
             pitch = n if t.dim() == 1 else arrays.layout_pitch(t) if _plane_layout(t) else None
@@ -254,13 +255,15 @@ class MpmSimulator:
                 continue
             table.append(_lib.BkParticleArray(t.data_ptr(), pitch, planes, t.element_size()))
             largest = max(largest, planes * n * t.element_size())
+            total += (planes * n * t.element_size() + 255) // 256 * 256
         if not table:
             return
-        scratch = torch.empty(largest, dtype=torch.uint8, device=self.device)
+        size = min(total, max(largest, 256 << 20))
+        scratch = torch.empty(size, dtype=torch.uint8, device=self.device)
         order32 = order.to(torch.int32)
         entries = (_lib.BkParticleArray * len(table))(*table)
         _lib.call("bk_permute_particles", n, order32.data_ptr(), len(table), _lib.C.addressof(entries),
-                  scratch.data_ptr(), largest, _lib.stream_handle())
+                  scratch.data_ptr(), size, _lib.stream_handle())
 
     def SortParticles(self, order=None):
         """Reorder the particles in place by grid cell (``CellOrder``, or a given permutation), so

@@ -641,7 +641,10 @@ typedef struct {
 /* In place, for every array: element k of each plane becomes the element order[k] had. `arrays`
    is a HOST table of `array_count` entries, each array aligned to its element size; order: n
    int32 (device), a permutation, so n <= INT32_MAX; scratch: device, 256-byte aligned, at least
-   planes * n * element_bytes bytes of the largest array. Arrays must not overlap one another. One gather kernel and one 2-D copy per array, in order on `stream`. */
+   planes * n * element_bytes bytes of the largest array. Arrays must not overlap one another.
+   Consecutive arrays are permuted in groups whose slices (each rounded up to 256 bytes) fit the
+   scratch buffer: one gather launch and one copy-back launch per group, in order on `stream`, so
+   a scratch buffer as large as all the arrays together takes two launches in all. */
 BK_API int bk_permute_particles(int64_t n, const int32_t *order, int32_t array_count, const BkParticleArray *arrays,
                                 void *scratch, int64_t scratch_bytes, void *stream);
 

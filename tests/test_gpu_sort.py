@@ -186,7 +186,8 @@ def test_rollout_gradients_follow_the_order():
 
 def test_permute_particles_planes_and_element_sizes():
     """bk_permute_particles on float32 planes (1, 3 and 9 planes, pitch above n), float64 and int32
-    arrays against numpy indexing; a scratch smaller than the largest array is refused."""
+    arrays against numpy indexing, with a scratch buffer of the largest array (three groups) and
+    one for all arrays (one group); a scratch smaller than the largest array is refused."""
     import ctypes
     import torch
     from baking_b200 import _lib, arrays
@@ -216,6 +217,17 @@ def test_permute_particles_planes_and_element_sizes():
     np.testing.assert_array_equal(arrays.to_numpy(dev_arrays[1]), host[1][order])
     np.testing.assert_array_equal(dev_arrays[2].cpu().numpy(), host[2][order])
     np.testing.assert_array_equal(dev_arrays[3].cpu().numpy(), host[3][order])
+    # again with a scratch buffer for all four arrays at once: one group, two launches
+    order2 = rng.permutation(n)
+    order2_d = torch.as_tensor(order2, dtype=torch.int32, device=dev)
+    big = torch.empty(64 * 1024, dtype=torch.uint8, device=dev)
+    _lib.call("bk_permute_particles", n, order2_d.data_ptr(), 4, ctypes.addressof(table), big.data_ptr(),
+              big.numel(), _lib.stream_handle())
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(arrays.to_numpy(dev_arrays[0]), host[0][order][order2])
+    np.testing.assert_array_equal(arrays.to_numpy(dev_arrays[1]), host[1][order][order2])
+    np.testing.assert_array_equal(dev_arrays[2].cpu().numpy(), host[2][order][order2])
+    np.testing.assert_array_equal(dev_arrays[3].cpu().numpy(), host[3][order][order2])
 
 
 def test_sort_interval_sorts_during_advance():
