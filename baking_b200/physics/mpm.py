@@ -100,6 +100,10 @@ class MpmSimulator:
         # particle_order[k]: index in the constructor's samples of the particle at position k
         self.particle_order = torch.arange(len(particle_samples.particle_positions), device=self.device)
         self.sort_count = 0
+        # Within one Advance/AdvanceUnchecked call, let each substep's G2P kernel also scatter the
+        # next substep's transport fields (one particle pass fewer). Off by default: on the 1M loaf
+        # the separate scatter kernel measured 1% faster per substep (2.77e9 against 2.74e9).
+        self.scatter_ahead = False
         self.Reset()
 
     # --------------------------------------------------------------- state
@@ -480,7 +484,7 @@ class MpmSimulator:
         if step_count < 1:
             raise ValueError("step_count must be positive")
         start = self.step_count
-        ahead = self._engine.prescatter_allowed()
+        ahead = self.scatter_ahead and self._engine.prescatter_allowed()
         for k in range(step_count):
             self._substep(check=self.IsSettling, prescattered=ahead and k > 0,
                           prescatter_next=ahead and k + 1 < step_count)
@@ -500,8 +504,9 @@ class MpmSimulator:
 
     def AdvanceUnchecked(self, step_count):
         """Run substeps with no host synchronisation; flags stay on the device until CheckState/Advance.
-        Within the call each substep's G2P scatters the next substep's transport fields ahead."""
-        ahead = self._engine.prescatter_allowed()
+        With ``scatter_ahead`` set, each substep's G2P within the call scatters the next substep's
+        transport fields ahead."""
+        ahead = self.scatter_ahead and self._engine.prescatter_allowed()
         for k in range(step_count):
             self._substep(check=False, prescattered=ahead and k > 0, prescatter_next=ahead and k + 1 < step_count)
 

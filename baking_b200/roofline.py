@@ -42,8 +42,9 @@ PER_KERNEL = {
 }
 
 
-def fused_bytes(kernel, engine, active_nodes):
-    """Bytes per launch of the kernels inside ``bk_substep`` for the engine's mode."""
+def fused_bytes(kernel, engine, active_nodes, scatter_ahead=False):
+    """Bytes per launch of the kernels inside ``bk_substep`` for the engine's mode; ``scatter_ahead``:
+    the G2P kernel also scatters the next substep's transport fields."""
     n, tr, gas = engine.n, engine.transport, engine.gas
     ding = engine.is_ding
     if kernel == "surface_vertices":
@@ -72,7 +73,7 @@ def fused_bytes(kernel, engine, active_nodes):
             per += 36 + 4 + 4 + (8 if tr else 4)    # Fe, porosity, gelled, temperature read
             per += 36 + 36 + 4 + 4                  # Fe, tau, porosity, gelled written
         node = 16
-        if engine.prescatter_allowed():
+        if scatter_ahead and engine.prescatter_allowed():
             # Inside an Advance call the kernel also scatters the next substep's transport fields:
             # V0 4, capacity 8, water 8 read (temperature counted above); 4 node fields written.
             per += 4 + 8 + 8
@@ -85,7 +86,7 @@ def algorithmic_bytes(kernel, simulator, active_nodes):
     n = simulator.particle_data.particle_count
     engine = getattr(simulator, "_engine", None)
     if engine is not None:
-        fused = fused_bytes(kernel, engine, active_nodes)
+        fused = fused_bytes(kernel, engine, active_nodes, getattr(simulator, "scatter_ahead", False))
         if fused is not None:
             return fused
     if kernel in PER_KERNEL:

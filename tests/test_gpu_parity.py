@@ -104,6 +104,7 @@ def test_prescattered_transport_matches_substep_by_substep():
     scene = box_loaf(resolution=48, particle_count=20000, seed=4, time_step=1e-4)
     a = make_simulator(scene)
     b = make_simulator(scene)
+    b.scatter_ahead = True
     for _ in range(12):
         a.Step()
     b.AdvanceUnchecked(12)

@@ -9,6 +9,7 @@ def test_kernel_timer_all_and_selected():
     from baking_b200 import _lib
     from tests.scenes import build_transport
     sim = build_transport("cuda", gas=True)
+    sim.scatter_ahead = True
     sim.AdvanceUnchecked(1)
     every = _lib.KernelTimer()
     with every:
