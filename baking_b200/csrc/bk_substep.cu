@@ -845,7 +845,7 @@ constexpr int kP2GPlanes = 33;
 struct P2GSmem {
     union {
         struct {
-            float planes[kP2GPlanes][kThreads];  // x 0-2, v 3-5, C 6-14, F 15-23, tau 24-32
+            float planes[kP2GPlanes][kThreads];  // x 0-2 (unused: x is read directly), v 3-5, C 6-14, F 15-23, tau 24-32
             double d[4][kThreads];               // temperature, water, dry mass, gas moles
             float f[3][kThreads];                // reference volume, gas source rate, porosity
         } in;
@@ -927,9 +927,36 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
     const unsigned staged_scalars =
         kStaged && P.n - (int64_t)sl.block * kThreads >= kThreads
             ? p2g_staged_scalars(P.transport, P.gas, P.material, cst.gas_rate_per_particle) : 0u;
+    // The particle's stencil and its scalar G2P of the diffused node fields (thermal_water.py:206-215)
+    // read only x and the grid: the staged form runs them while its bulk copies are in flight.
+    bool valid = false;
+    Stencil st;
+    st.b[0] = st.b[1] = st.b[2] = 0;
+    double dTp = 0.0, ratio = 0.0;
+    auto stencil_and_gather = [&]() {
+        if (i < P.n) {
+            st = make_stencil(load_v3(in.x, i, pitch), P.origin, P.dx, P.R);
+            valid = st.valid;
+            if (!valid) set_flag(flags.simulation, 1);
+        }
+        if (valid && P.transport) {
+#pragma unroll
+            for (int ox = 0; ox < 3; ++ox)
+#pragma unroll
+                for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+                    for (int oz = 0; oz < 3; ++oz) {
+                        double w = (double)(st.w[0][ox] * st.w[1][oy] * st.w[2][oz]);
+                        double2 d = __ldg(g.dTr + node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R));
+                        dTp += w * d.x;
+                        ratio += w * d.y;
+                    }
+        }
+    };
     if constexpr (kStaged) {
         // Planes are pitch-long with a pitch that is a multiple of 4 and 16-byte aligned bases (the
-        // host checks), so the block's range rounded up to 16 bytes stays inside each plane.
+        // host checks), so the block's range rounded up to 16 bytes stays inside each plane. The x
+        // planes are not copied: x is read directly, before the wait.
         const uint32_t mbar = mlp::smem_addr(&sm.mbar);
         if (tid == 0) mlp::mbar_init(mbar, 1);
         __syncthreads();
@@ -941,13 +968,13 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
             const float* src[5] = {in.x, in.v, in.C, in.F, in.tau};
             const int planes[5] = {3, 3, 9, 9, 9};
             const unsigned m = count == kThreads ? staged_scalars : 0u;
-            uint32_t total = bytes * (uint32_t)(P.material == 1 ? kP2GPlanes : kP2GPlanes - 9);
+            uint32_t total = bytes * (uint32_t)(P.material == 1 ? kP2GPlanes - 3 : kP2GPlanes - 12);
 #pragma unroll
             for (int k = 0; k < 7; ++k)
                 if (m & (1u << k)) total += k < 4 ? kThreads * 8 : kThreads * 4;
             stage::arrive_expect_tx(mbar, total);
-            int k = 0;
-            for (int a = 0; a < arrays; ++a)
+            int k = 3;
+            for (int a = 1; a < arrays; ++a)
                 for (int c = 0; c < planes[a]; ++c, ++k)
                     stage::copy(mlp::smem_addr(&sm.in.planes[k][0]), src[a] + c * pitch + start, bytes, mbar);
             const double* dsrc[4] = {in.temperature, in.water, cst.dry_mass, in.gas_moles};
@@ -957,6 +984,7 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
             for (int k = 0; k < 3; ++k)
                 if (m & (16u << k)) stage::copy(mlp::smem_addr(&sm.in.f[k][0]), fsrc[k] + start, kThreads * 4, mbar);
         }
+        stencil_and_gather();
         const bool arrived = __syncthreads_and(mlp::mbar_wait(mbar, 0, stage::kWaitPolls)) != 0;
         if (!arrived) {
             // Leave this block's particles unprocessed and report it; wait (bounded) for the copies
@@ -965,6 +993,8 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
             mlp::mbar_wait(mbar, 0, stage::kWaitPolls);
             return;
         }
+    } else {
+        stencil_and_gather();
     }
     // This particle's plane arrays: from the staged copies or from global memory.
     auto ld_v3 = [&](const float* src, int plane0) {
@@ -981,16 +1011,7 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
             return load_m3(src, i, pitch);
         }
     };
-    bool valid = false;
-    Stencil st;
-    st.b[0] = st.b[1] = st.b[2] = 0;
     float mass = 0.f, q[3] = {0.f, 0.f, 0.f}, A[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (i < P.n) {
-        V3 x = ld_v3(in.x, 0);
-        st = make_stencil(x, P.origin, P.dx, P.R);
-        valid = st.valid;
-        if (!valid) set_flag(flags.simulation, 1);
-    }
     if (valid) {
         M3 F = ld_m3(in.F, 15);
         float J = det3(F);
@@ -999,18 +1020,6 @@ __device__ __forceinline__ void p2g_body(Arg<Params, kRef> P, Arg<BkState, kRef>
         float rho_ref = P.density;
         double sat = 0.0;
         if (P.transport) {
-            double dTp = 0.0, ratio = 0.0;
-#pragma unroll
-            for (int ox = 0; ox < 3; ++ox)
-#pragma unroll
-                for (int oy = 0; oy < 3; ++oy)
-#pragma unroll
-                    for (int oz = 0; oz < 3; ++oz) {
-                        double w = (double)(st.w[0][ox] * st.w[1][oy] * st.w[2][oz]);
-                        double2 d = __ldg(g.dTr + node_index(st.b[0] + ox, st.b[1] + oy, st.b[2] + oz, P.R));
-                        dTp += w * d.x;
-                        ratio += w * d.y;
-                    }
             double T_old = (staged_scalars & 1u) ? sm.in.d[0][tid] : in.temperature[i];
             double Tn = T_old + dTp;
             double Wn = ((staged_scalars & 2u) ? sm.in.d[1][tid] : in.water[i]) * (1.0 + ratio);
